@@ -1,0 +1,100 @@
+/*
+ * ssol_b200.h - B200 extensions of the ssol_* C API.
+ *
+ * None of these entry points has a counterpart in the reference; they expose
+ * what a GPU solver adds around `ssol_solve` (src/ssol.h:1216-1223):
+ *  - solve options: arithmetic precision of geometry/sampling/BSDFs (FP32 or
+ *    all-FP64; tallies are FP64 in both), launch shape, BVH leaf size;
+ *  - plans: a scene snapshot resident in device memory that can be launched
+ *    many times on a caller's CUDA stream and read back once, which is how
+ *    `ssol_solve` itself is built (create, reset, launch, finish);
+ *  - per-solve device timing and work counters for roofline reporting.
+ * Plain C: CUDA streams travel as `void*` (a cudaStream_t).
+ */
+#ifndef SSOL_B200_H
+#define SSOL_B200_H
+
+#include "ssol.h"
+#include "ssp.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum ssol_b200_precision {
+  SSOL_B200_FP32 = 0, /* FP32 geometry, sampling and BSDFs; FP64 tallies */
+  SSOL_B200_FP64 = 1 /* everything in FP64 on identical random numbers */
+};
+
+struct ssol_b200_options {
+  enum ssol_b200_precision precision;
+  int block_size; /* threads per block, <= 256; 0 => 256 */
+  int grid_blocks; /* 0 => one persistent wave sized from occupancy */
+  int waves; /* persistent grid multiplier when grid_blocks == 0 */
+  int bvh_leaf_size; /* primitives per BVH leaf; 0 => 4 */
+  unsigned long long max_segments; /* path segment budget; 0 => 1e6 */
+};
+#define SSOL_B200_OPTIONS_DEFAULT__ { SSOL_B200_FP32, 256, 0, 1, 4, 0 }
+static const struct ssol_b200_options SSOL_B200_OPTIONS_DEFAULT =
+  SSOL_B200_OPTIONS_DEFAULT__;
+
+/* Device work of the last solve (or of a plan's launches since its reset) */
+struct ssol_b200_stats {
+  double kernel_ms; /* CUDA-event time of the realisation launches */
+  unsigned long long rays; /* rays cast (shadow + scattered) */
+  unsigned long long node_visits; /* BVH nodes fetched */
+  unsigned long long triangle_tests;
+  unsigned long long quadric_tests;
+  unsigned long long bounces; /* surface interactions that were shaded */
+  unsigned long long paths;
+  unsigned long long killed; /* paths ended by the Russian roulette */
+  unsigned long long scene_bytes; /* host -> device bytes of the snapshot */
+  unsigned long long tally_bytes; /* device -> host bytes of the tallies */
+};
+
+/* ssol_solve with explicit options (NULL => defaults) */
+SSOL_API res_T ssol_solve_ex
+  (struct ssol_scene* scn,
+   const struct ssp_rng* rng,
+   const size_t realisations_count,
+   const size_t max_failed_count,
+   const struct ssol_path_tracker* tracker,
+   const struct ssol_b200_options* options,
+   struct ssol_estimator** estimator);
+
+SSOL_API res_T ssol_estimator_get_b200_stats
+  (const struct ssol_estimator* estimator, struct ssol_b200_stats* stats);
+
+/* Plans */
+struct ssol_b200_plan;
+
+/* Snapshot `scn` (flatten, build the BVH, upload); device memory stays
+ * allocated until the last reference is released */
+SSOL_API res_T ssol_b200_plan_create
+  (struct ssol_scene* scn, const struct ssol_b200_options* options,
+   struct ssol_b200_plan** plan);
+SSOL_API res_T ssol_b200_plan_ref_get(struct ssol_b200_plan* plan);
+SSOL_API res_T ssol_b200_plan_ref_put(struct ssol_b200_plan* plan);
+/* Zero the device tallies, asynchronously on `stream` (NULL => the plan's
+ * own stream) */
+SSOL_API res_T ssol_b200_plan_reset
+  (struct ssol_b200_plan* plan, void* stream);
+/* Enqueue realisations [first, first + count) of the streams keyed by `rng`;
+ * tallies accumulate. Asynchronous. */
+SSOL_API res_T ssol_b200_plan_launch
+  (struct ssol_b200_plan* plan, const struct ssp_rng* rng,
+   const uint64_t first, const uint64_t count, void* stream);
+/* Wait for `stream`, read the tallies back and build an estimator for
+ * `realisations_count` realisations; same failure rule as ssol_solve */
+SSOL_API res_T ssol_b200_plan_finish
+  (struct ssol_b200_plan* plan, const struct ssp_rng* rng,
+   const uint64_t realisations_count, const size_t max_failed_count,
+   void* stream, struct ssol_estimator** estimator);
+SSOL_API res_T ssol_b200_plan_get_stats
+  (const struct ssol_b200_plan* plan, struct ssol_b200_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SSOL_B200_H */

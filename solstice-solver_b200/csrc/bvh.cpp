@@ -1,0 +1,250 @@
+/*
+ * bvh.cpp - top-down binned SAH builder (Wald, "On fast construction of
+ * SAH-based bounding volume hierarchies", 2007) with a median-split fallback
+ * that bounds the depth for the device's fixed traversal stack.
+ */
+#include "bvh.h"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+
+namespace ssolb {
+
+namespace {
+
+struct Box {
+  double lo[3], hi[3];
+  void reset()
+  {
+    for(int c = 0; c < 3; ++c) {
+      lo[c] = std::numeric_limits<double>::max();
+      hi[c] = -std::numeric_limits<double>::max();
+    }
+  }
+  void grow(const double* l, const double* h)
+  {
+    for(int c = 0; c < 3; ++c) {
+      lo[c] = std::min(lo[c], l[c]);
+      hi[c] = std::max(hi[c], h[c]);
+    }
+  }
+  double area() const
+  {
+    const double d[3] = {std::max(0.0, hi[0] - lo[0]),
+                         std::max(0.0, hi[1] - lo[1]),
+                         std::max(0.0, hi[2] - lo[2])};
+    return 2 * (d[0] * d[1] + d[1] * d[2] + d[2] * d[0]);
+  }
+};
+
+struct Task {
+  int begin, end; /* range of prims */
+  int node, slot; /* parent slot to fill: node*2 + k */
+  int depth;
+};
+
+Box bounds(const std::vector<PrimBox>& p, int b, int e)
+{
+  Box box;
+  box.reset();
+  for(int i = b; i < e; ++i) box.grow(p[i].lo, p[i].hi);
+  return box;
+}
+
+double centroid(const PrimBox& p, int axis)
+{ return 0.5 * (p.lo[axis] + p.hi[axis]); }
+
+/* Returns the split position in [b, e) or -1 to make a leaf */
+int split(std::vector<PrimBox>& p, int b, int e, const BvhBuildParams& prm,
+          int depth)
+{
+  const int n = e - b;
+  if(n <= prm.max_leaf) return -1;
+  Box cb;
+  cb.reset();
+  for(int i = b; i < e; ++i) {
+    double c[3];
+    for(int k = 0; k < 3; ++k) c[k] = centroid(p[i], k);
+    cb.grow(c, c);
+  }
+  const bool force_median = depth >= prm.max_depth - 8;
+  double best_cost = std::numeric_limits<double>::max();
+  int best_axis = -1, best_bin = -1;
+  const int nb = prm.bins;
+  if(!force_median) {
+    for(int axis = 0; axis < 3; ++axis) {
+      const double ext = cb.hi[axis] - cb.lo[axis];
+      if(!(ext > 0)) continue;
+      std::vector<Box> bin(nb);
+      std::vector<int> cnt(nb, 0);
+      for(Box& x : bin) x.reset();
+      for(int i = b; i < e; ++i) {
+        int k = (int)((centroid(p[i], axis) - cb.lo[axis]) / ext * nb);
+        k = std::min(std::max(k, 0), nb - 1);
+        bin[k].grow(p[i].lo, p[i].hi);
+        ++cnt[k];
+      }
+      std::vector<double> right_area(nb, 0);
+      std::vector<int> right_cnt(nb, 0);
+      Box acc;
+      acc.reset();
+      int c = 0;
+      for(int k = nb - 1; k > 0; --k) {
+        acc.grow(bin[k].lo, bin[k].hi);
+        c += cnt[k];
+        right_area[k] = acc.area();
+        right_cnt[k] = c;
+      }
+      acc.reset();
+      c = 0;
+      for(int k = 0; k < nb - 1; ++k) {
+        acc.grow(bin[k].lo, bin[k].hi);
+        c += cnt[k];
+        if(!c || !right_cnt[k + 1]) continue;
+        const double cost = acc.area() * c + right_area[k + 1] * right_cnt[k + 1];
+        if(cost < best_cost) {
+          best_cost = cost;
+          best_axis = axis;
+          best_bin = k;
+        }
+      }
+    }
+  }
+  if(best_axis >= 0) {
+    const double ext = cb.hi[best_axis] - cb.lo[best_axis];
+    auto mid = std::partition(p.begin() + b, p.begin() + e,
+      [&](const PrimBox& x) {
+        int k = (int)((centroid(x, best_axis) - cb.lo[best_axis]) / ext * nb);
+        k = std::min(std::max(k, 0), nb - 1);
+        return k <= best_bin;
+      });
+    const int m = (int)(mid - p.begin());
+    if(m > b && m < e) return m;
+  }
+  /* Median split along the largest centroid extent */
+  int axis = 0;
+  double ext = -1;
+  for(int k = 0; k < 3; ++k) {
+    if(cb.hi[k] - cb.lo[k] > ext) { ext = cb.hi[k] - cb.lo[k]; axis = k; }
+  }
+  const int m = b + n / 2;
+  std::nth_element(p.begin() + b, p.begin() + m, p.begin() + e,
+    [&](const PrimBox& x, const PrimBox& y) {
+      return centroid(x, axis) < centroid(y, axis);
+    });
+  return m;
+}
+
+} /* namespace */
+
+void build_bvh(std::vector<PrimBox> prims, const BvhBuildParams& prm,
+               BvhResult& out)
+{
+  out = BvhResult();
+  /* Node 0 is the root; its two slots hold the two top-level children */
+  auto new_node = [&]() {
+    const int id = (int)(out.child.size() / 2);
+    out.lo.resize(out.lo.size() + 6, 0);
+    out.hi.resize(out.hi.size() + 6, 0);
+    out.child.resize(out.child.size() + 2, 0);
+    out.count.resize(out.count.size() + 2, 0);
+    return id;
+  };
+  auto set_slot = [&](int slot, const Box& b, int child, int count) {
+    for(int c = 0; c < 3; ++c) {
+      out.lo[(size_t)slot * 3 + c] = b.lo[c];
+      out.hi[(size_t)slot * 3 + c] = b.hi[c];
+    }
+    out.child[slot] = child;
+    out.count[slot] = count;
+  };
+
+  const int root = new_node();
+  const int n = (int)prims.size();
+  if(n == 0) {
+    Box empty;
+    empty.reset();
+    set_slot(root * 2 + 0, empty, 0, -1);
+    set_slot(root * 2 + 1, empty, 0, -1);
+    out.primrefs.push_back(0);
+    return;
+  }
+  std::vector<Task> stack;
+  int m = split(prims, 0, n, prm, 0);
+  if(m < 0) {
+    /* Whole scene in one leaf; the second slot is an empty box */
+    Box empty;
+    empty.reset();
+    for(int i = 0; i < n; ++i) out.primrefs.push_back(prims[i].ref);
+    set_slot(root * 2 + 0, bounds(prims, 0, n), 0, n);
+    set_slot(root * 2 + 1, empty, 0, -1);
+    out.depth = 1;
+    return;
+  }
+  stack.push_back({0, m, root, 0, 1});
+  stack.push_back({m, n, root, 1, 1});
+  /* Leaves are emitted in build order into `primrefs` */
+  std::vector<uint32_t> refs;
+  refs.reserve(n);
+  while(!stack.empty()) {
+    const Task t = stack.back();
+    stack.pop_back();
+    out.depth = std::max(out.depth, t.depth + 1);
+    const Box b = bounds(prims, t.begin, t.end);
+    const int s = split(prims, t.begin, t.end, prm, t.depth);
+    if(s < 0) {
+      const int first = (int)refs.size();
+      for(int i = t.begin; i < t.end; ++i) refs.push_back(prims[i].ref);
+      set_slot(t.node * 2 + t.slot, b, first, t.end - t.begin);
+    } else {
+      const int id = new_node();
+      set_slot(t.node * 2 + t.slot, b, id, 0);
+      stack.push_back({t.begin, s, id, 0, t.depth + 1});
+      stack.push_back({s, t.end, id, 1, t.depth + 1});
+    }
+  }
+  out.primrefs = std::move(refs);
+}
+
+template<class R> static R round_down(double x)
+{
+  R r = (R)x;
+  if((double)r > x) r = std::nextafter(r, -std::numeric_limits<R>::max());
+  return r;
+}
+template<class R> static R round_up(double x)
+{
+  R r = (R)x;
+  if((double)r < x) r = std::nextafter(r, std::numeric_limits<R>::max());
+  return r;
+}
+
+template<class R> std::vector<DNode<R>> bvh_nodes(const BvhResult& b)
+{
+  const size_t nnodes = b.child.size() / 2;
+  std::vector<DNode<R>> nodes(nnodes);
+  for(size_t i = 0; i < nnodes; ++i) {
+    for(int k = 0; k < 2; ++k) {
+      const size_t s = i * 2 + k;
+      for(int c = 0; c < 3; ++c) {
+        const double lo = b.lo[s * 3 + c], hi = b.hi[s * 3 + c];
+        if(lo > hi) { /* empty slot (count < 0): never entered */
+          nodes[i].lo[k][c] = R(0);
+          nodes[i].hi[k][c] = R(0);
+        } else {
+          nodes[i].lo[k][c] = round_down<R>(lo);
+          nodes[i].hi[k][c] = round_up<R>(hi);
+        }
+      }
+      nodes[i].child[k] = b.child[s];
+      nodes[i].count[k] = b.count[s];
+    }
+  }
+  return nodes;
+}
+
+template std::vector<DNode<float>> bvh_nodes<float>(const BvhResult&);
+template std::vector<DNode<double>> bvh_nodes<double>(const BvhResult&);
+
+} /* namespace ssolb */

@@ -1,0 +1,612 @@
+/*
+ * flatten.cpp - ssol_scene -> FlatScene<R> (see flatten.h).
+ */
+#include "flatten.h"
+#include "tessellate.h"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <map>
+
+namespace ssolb {
+
+namespace {
+
+/* 3x4 column-major affine helpers (the ssol_instance / ssol_quadric
+ * transform convention: R in [0..8] column major, T in [9..11]) */
+void compose(double out[12], const double a[12], const double b[12])
+{
+  double r[12];
+  for(int c = 0; c < 3; ++c)
+    for(int row = 0; row < 3; ++row)
+      r[c * 3 + row] = a[row] * b[c * 3] + a[3 + row] * b[c * 3 + 1]
+                     + a[6 + row] * b[c * 3 + 2];
+  for(int row = 0; row < 3; ++row)
+    r[9 + row] = a[row] * b[9] + a[3 + row] * b[10] + a[6 + row] * b[11]
+               + a[9 + row];
+  for(int i = 0; i < 12; ++i) out[i] = r[i];
+}
+
+bool invert(double out[12], const double m[12])
+{
+  const double a = m[0], b = m[3], c = m[6];
+  const double d = m[1], e = m[4], f = m[7];
+  const double g = m[2], h = m[5], k = m[8];
+  const double A = e * k - f * h, B = -(d * k - f * g), C = d * h - e * g;
+  const double det = a * A + b * B + c * C;
+  if(det == 0) return false;
+  const double inv = 1.0 / det;
+  /* row-major inverse entries */
+  const double i00 = A * inv, i01 = -(b * k - c * h) * inv, i02 = (b * f - c * e) * inv;
+  const double i10 = B * inv, i11 = (a * k - c * g) * inv, i12 = -(a * f - c * d) * inv;
+  const double i20 = C * inv, i21 = -(a * h - b * g) * inv, i22 = (a * e - b * d) * inv;
+  out[0] = i00; out[3] = i01; out[6] = i02;
+  out[1] = i10; out[4] = i11; out[7] = i12;
+  out[2] = i20; out[5] = i21; out[8] = i22;
+  for(int row = 0; row < 3; ++row)
+    out[9 + row] = -(out[row] * m[9] + out[3 + row] * m[10]
+                   + out[6 + row] * m[11]);
+  return true;
+}
+
+void apply(const double m[12], const double p[3], double out[3])
+{
+  for(int r = 0; r < 3; ++r)
+    out[r] = m[r] * p[0] + m[3 + r] * p[1] + m[6 + r] * p[2] + m[9 + r];
+}
+
+/* Column-major 3x4 -> row-major 3x4 of precision R */
+template<class R> void to_rows(R out[12], const double m[12])
+{
+  for(int r = 0; r < 3; ++r) {
+    for(int c = 0; c < 3; ++c) out[r * 4 + c] = (R)m[c * 3 + r];
+    out[r * 4 + 3] = (R)m[9 + r];
+  }
+}
+
+/* Buie sunshape constants (src/ssol_ranst_sun_dir.c:82-222): the Buie et al.
+ * (2003) circumsolar profile with its published CSR calibration */
+double buie_chi(double csr)
+{
+  if(csr > 0.145)
+    return -0.04419909985804843 + csr * (1.401323894233574
+      + csr * (-0.3639746714505299 + csr * (-0.9579768560161194
+      + 1.1550475450828657 * csr)));
+  if(csr > 0.035)
+    return 0.022652077593662934 + csr * (0.5252380349996234
+      + csr * (2.5484334534423887 - 0.8763755326550412 * csr));
+  return 0.004733749294807862 + csr * (4.716738065192151
+    + csr * (-463.506669149804 + csr * (24745.88727411664
+    + csr * (-606122.7511711778 + 5521693.445014727 * csr))));
+}
+
+void buie_state(double csr, double out[8])
+{
+  const double thetaSD = 0.00465, thetaCS = 0.0436;
+  const double integralA = 9.224724736098827E-6;
+  const double chi = buie_chi(csr);
+  const double k = 0.9 * std::log(13.5 * chi) * std::pow(chi, -0.3);
+  const double gamma = 2.2 * std::log(0.52 * chi) * std::pow(chi, 0.43) - 0.1;
+  const double ek1000g = std::exp(k) * std::pow(1000, gamma);
+  const double g2 = gamma + 2.0;
+  const double integralB = ek1000g / g2
+    * (std::pow(thetaCS, g2) - std::pow(thetaSD, g2));
+  const double alpha = 1 / (integralA + integralB);
+  auto pdf = [&](double t) {
+    const double phi = t < thetaSD ? std::cos(326 * t) / std::cos(308 * t)
+                                   : ek1000g * std::pow(t, gamma);
+    return alpha * phi * std::sin(t);
+  };
+  const double h1 = 1.001 * pdf(0.0038915695846209047);
+  const double h2 = pdf(thetaSD);
+  const double d = thetaCS - thetaSD;
+  out[0] = thetaSD;
+  out[1] = d;
+  out[2] = gamma;
+  out[3] = ek1000g;
+  out[4] = alpha;
+  out[5] = h1;
+  out[6] = h2;
+  out[7] = (thetaSD * h1) / (thetaSD * h1 + d * h2);
+}
+
+/* Orthonormal basis, same construction as the device (Duff et al. 2017) */
+void basis(const double n[3], double out[9])
+{
+  const double sgn = n[2] >= 0 ? 1.0 : -1.0;
+  const double a = -1.0 / (sgn + n[2]);
+  const double b = n[0] * n[1] * a;
+  const double b1[3] = {1 + sgn * n[0] * n[0] * a, sgn * b, -sgn * n[0]};
+  const double b2[3] = {b, sgn + n[1] * n[1] * a, -n[1]};
+  for(int c = 0; c < 3; ++c) {
+    out[c] = b1[c];
+    out[3 + c] = b2[c];
+    out[6 + c] = n[c];
+  }
+}
+
+struct Interner {
+  std::vector<ssol_medium> media;
+  std::map<const ssol_spectrum*, int> spectra;
+};
+
+template<class R>
+int intern_spectrum(FlatScene<R>& out, Interner& in, const ssol_spectrum* s)
+{
+  auto it = in.spectra.find(s);
+  if(it != in.spectra.end()) return it->second;
+  DSpectrum d;
+  d.first = (int32_t)out.spec_wl.size();
+  d.count = (int32_t)s->wavelengths.size();
+  out.spec_wl.insert(out.spec_wl.end(), s->wavelengths.begin(),
+                     s->wavelengths.end());
+  out.spec_val.insert(out.spec_val.end(), s->intensities.begin(),
+                      s->intensities.end());
+  const int id = (int)out.spectra.size();
+  out.spectra.push_back(d);
+  in.spectra.emplace(s, id);
+  return id;
+}
+
+template<class R>
+DData to_ddata(FlatScene<R>& out, Interner& in, const ssol_data& d)
+{
+  DData r;
+  r.pad = 0;
+  if(d.type == SSOL_DATA_SPECTRUM) {
+    r.spectrum = intern_spectrum(out, in, d.value.spectrum);
+    r.real = 0;
+  } else {
+    r.spectrum = -1;
+    r.real = d.value.real;
+  }
+  return r;
+}
+
+/* Media compare by value (media_ceq, src/ssol_material.c:730-736) */
+template<class R>
+int intern_medium(FlatScene<R>& out, Interner& in, const ssol_medium& m)
+{
+  for(size_t i = 0; i < in.media.size(); ++i)
+    if(ssolb_media_ceq(in.media[i], m)) return (int)i;
+  DMedium d;
+  d.extinction = to_ddata(out, in, m.extinction);
+  d.refractive_index = to_ddata(out, in, m.refractive_index);
+  out.media.push_back(d);
+  in.media.push_back(m);
+  return (int)in.media.size() - 1;
+}
+
+/* Evaluate shader callbacks once per sun wavelength node on a canonical
+ * fragment; shaders may vary with the wavelength, not with the position */
+template<class R>
+void tabulate_shaders(FlatScene<R>& out, ssol_material* m, ssol_device* dev)
+{
+  ssol_surface_fragment frag = SSOL_SURFACE_FRAGMENT_NULL;
+  frag.dir[2] = -1;
+  frag.Ng[2] = 1;
+  frag.Ns[2] = 1;
+  frag.dPdu[0] = 1;
+  frag.dPdv[1] = 1;
+  for(double wl : out.shader_wl) {
+    double refl = 0, rough = 0;
+    if(m->reflectivity) m->reflectivity(dev, m->buf, wl, &frag, &refl);
+    if(m->roughness) m->roughness(dev, m->buf, wl, &frag, &rough);
+    out.shader_tab.push_back((R)refl);
+    out.shader_tab.push_back((R)rough);
+  }
+  if(m->normal) {
+    double n[3] = {0, 0, 0};
+    m->normal(dev, m->buf, out.shader_wl[0], &frag, n);
+    if(n[0] != 0 || n[1] != 0 || n[2] != 1)
+      dev->log_warning("normal shaders other than the shading normal are "
+                       "not supported on the device; using Ns.\n");
+  }
+}
+
+/* Quadric patch bounds: local z range over the carving AABB */
+void quadric_z_range(const ssol_shape* s, double& zlo, double& zhi)
+{
+  const double* lo = s->carve_lo;
+  const double* hi = s->carve_hi;
+  const int t = s->quadric.type;
+  if(t == SSOL_QUADRIC_PLANE) { zlo = zhi = 0; return; }
+  /* All supported heights are monotonic in |x| and |y| */
+  const double xmin = (lo[0] <= 0 && hi[0] >= 0) ? 0
+                    : std::min(std::fabs(lo[0]), std::fabs(hi[0]));
+  const double ymin = (lo[1] <= 0 && hi[1] >= 0) ? 0
+                    : std::min(std::fabs(lo[1]), std::fabs(hi[1]));
+  const double xmax = std::max(std::fabs(lo[0]), std::fabs(hi[0]));
+  const double ymax = std::max(std::fabs(lo[1]), std::fabs(hi[1]));
+  zlo = ssolb_quadric_z(t, s->qparam, xmin, ymin);
+  zhi = ssolb_quadric_z(t, s->qparam, xmax, ymax);
+  if(zlo > zhi) std::swap(zlo, zhi);
+}
+
+} /* namespace */
+
+void build_alias(const std::vector<double>& w, std::vector<float>& prob,
+                 std::vector<int32_t>& alias)
+{
+  const size_t n = w.size();
+  prob.assign(n, 1.0f);
+  alias.resize(n);
+  double total = 0;
+  for(double x : w) total += x;
+  std::vector<double> p(n);
+  std::vector<int32_t> small, large;
+  for(size_t i = 0; i < n; ++i) {
+    alias[i] = (int32_t)i;
+    p[i] = total > 0 ? w[i] * (double)n / total : 1.0;
+    if(p[i] < 1.0) small.push_back((int32_t)i);
+    else large.push_back((int32_t)i);
+  }
+  while(!small.empty() && !large.empty()) {
+    const int32_t s = small.back(); small.pop_back();
+    const int32_t l = large.back(); large.pop_back();
+    prob[s] = (float)p[s];
+    alias[s] = l;
+    p[l] = (p[l] + p[s]) - 1.0;
+    if(p[l] < 1.0) small.push_back(l); else large.push_back(l);
+  }
+  for(int32_t i : small) prob[i] = 1.0f;
+  for(int32_t i : large) prob[i] = 1.0f;
+}
+
+template<class R>
+static res_T flatten_impl
+  (ssol_scene* scn, const BvhBuildParams& bvh_params, FlatScene<R>& out)
+{
+  ssol_device* dev = scn->dev;
+  out = FlatScene<R>();
+
+  /* scene_check (src/ssol_scene.c:539-558) */
+  if(!scn->sun) { dev->log_error("no sun attached.\n"); return RES_BAD_ARG; }
+  const ssol_sun* sun = scn->sun;
+  if(!sun->spectrum || sun->spectrum->wavelengths.empty()) {
+    dev->log_error("sun's spectrum undefined.\n");
+    return RES_BAD_ARG;
+  }
+  if(sun->dni <= 0) {
+    dev->log_error("sun's DNI undefined.\n");
+    return RES_BAD_ARG;
+  }
+
+  Interner in;
+  /* Air: vacuum with the atmosphere's extinction (src/ssol_solver.c:1180) */
+  ssol_medium air = SSOL_MEDIUM_VACUUM;
+  if(scn->atmosphere) air.extinction = scn->atmosphere->extinction;
+  out.air_medium = intern_medium(out, in, air);
+
+  /* Sun */
+  for(int c = 0; c < 3; ++c) out.sun_dir[c] = (R)sun->direction[c];
+  double B[9];
+  basis(sun->direction, B);
+  for(int c = 0; c < 9; ++c) out.sun_basis[c] = (R)B[c];
+  out.dni = sun->dni;
+  switch(sun->kind) {
+    case SUNK_DIRECTIONAL: out.sun_type = SUN_DIRAC; break;
+    case SUNK_PILLBOX: {
+      if(!(sun->half_angle > 0)) {
+        dev->log_error("pillbox half angle undefined.\n");
+        return RES_BAD_ARG;
+      }
+      out.sun_type = SUN_PILLBOX;
+      const double s = std::sin(sun->half_angle);
+      out.sun_param = (R)(s * s);
+      break;
+    }
+    case SUNK_GAUSSIAN:
+      if(!(sun->std_dev > 0)) return RES_BAD_ARG;
+      out.sun_type = SUN_GAUSSIAN;
+      out.sun_param = (R)sun->std_dev;
+      break;
+    case SUNK_BUIE:
+      /* ranst_sun_dir_buie_setup accepts CSR in [1e-6, 0.849] */
+      if(sun->csr < 1e-6 || sun->csr > 0.849) return RES_BAD_ARG;
+      out.sun_type = SUN_BUIE;
+      buie_state(sun->csr, out.buie);
+      break;
+  }
+  /* Wavelength distribution (src/ssol_ranst_sun_wl.c:154-188) */
+  out.wl_nodes = sun->spectrum->wavelengths;
+  out.wl_pdf = sun->spectrum->intensities;
+  {
+    const size_t n = out.wl_nodes.size();
+    out.wl_cdf.assign(n, 0.0);
+    for(size_t i = 1; i < n; ++i)
+      out.wl_cdf[i] = out.wl_cdf[i - 1] + 0.5 * (out.wl_pdf[i] + out.wl_pdf[i - 1])
+                    * (out.wl_nodes[i] - out.wl_nodes[i - 1]);
+    if(n > 1) {
+      const double total = out.wl_cdf[n - 1];
+      if(!(total > 0)) return RES_BAD_ARG;
+      for(double& c : out.wl_cdf) c /= total;
+      out.wl_cdf[n - 1] = 1.0;
+    }
+  }
+  out.shader_wl = out.wl_nodes;
+
+  /* Materials */
+  std::map<const ssol_material*, int> mtl_index;
+  auto material_id = [&](ssol_material* m) {
+    auto it = mtl_index.find(m);
+    if(it != mtl_index.end()) return it->second;
+    DMaterial d;
+    d.type = m->type;
+    d.distrib = m->distrib == SSOL_MICROFACET_PILLBOX ? DISTRIB_PILLBOX
+                                                      : DISTRIB_BECKMANN;
+    d.in_medium = intern_medium(out, in, m->in_medium);
+    d.out_medium = intern_medium(out, in, m->out_medium);
+    d.slab_medium = intern_medium(out, in, m->slab_medium);
+    d.thickness = m->thickness;
+    d.table = (int32_t)out.shader_tab.size();
+    tabulate_shaders(out, m, dev);
+    const int id = (int)out.mtls.size();
+    out.mtls.push_back(d);
+    mtl_index.emplace(m, id);
+    return id;
+  };
+
+  /* Receivers and sampled instances, in attach order */
+  bool has_sampled = false, has_receiver = false;
+  std::vector<PrimBox> boxes;
+  std::vector<double> samp_area;
+  for(size_t ii = 0; ii < scn->instances.size(); ++ii) {
+    ssol_instance* inst = scn->instances[ii];
+    const ssol_object* obj = inst->object;
+    int rcv_slot[2] = {-1, -1};
+    for(int side = 0; side < 2; ++side) {
+      if(inst->receiver_mask & (side == 0 ? SSOL_FRONT : SSOL_BACK)) {
+        rcv_slot[side] = (int)out.meta.rcv.size();
+        out.meta.rcv.push_back({inst, side});
+      }
+    }
+    if(inst->receiver_mask) has_receiver = true;
+    int sampled_idx = -1;
+    if(inst->sample) {
+      sampled_idx = (int)out.meta.sampled.size();
+      out.meta.sampled.push_back(inst);
+      out.meta.sampled_area += obj->rt_area;
+      out.meta.sampled_area_proxy += obj->samp_area;
+      has_sampled = true;
+    }
+    for(const ShadedShape& ss : obj->shaded) {
+      const ssol_shape* shape = ss.shape;
+      if(!shape->ready) continue;
+      DShadedInst si;
+      si.instance = (int32_t)ii;
+      si.mtl[0] = material_id(ss.front);
+      si.mtl[1] = material_id(ss.back);
+      si.receiver_mask = inst->receiver_mask & (SSOL_FRONT | SSOL_BACK);
+      si.rcv_slot[0] = rcv_slot[0];
+      si.rcv_slot[1] = rcv_slot[1];
+      si.prim_base[0] = si.prim_base[1] = -1;
+      si.sampled = sampled_idx;
+      si.is_punched = shape->kind == SHAPE_PUNCHED;
+      si.quadric = -1;
+      si.virtual_mask = (ss.front->type == SSOL_MATERIAL_VIRTUAL ? 1 : 0)
+                      | (ss.back->type == SSOL_MATERIAL_VIRTUAL ? 2 : 0);
+      const int ntris = (int)(shape->ids.size() / 3);
+      if(inst->per_primitive) {
+        if(si.is_punched && !shape->grid_exact) {
+          dev->log_error("per-primitive tallies on a punched surface need a "
+                         "carving equal to its bounding rectangle.\n");
+          return RES_BAD_ARG;
+        }
+        for(int side = 0; side < 2; ++side) {
+          if(rcv_slot[side] < 0) continue;
+          si.prim_base[side] = out.meta.nprim_slots;
+          out.meta.prims.push_back({rcv_slot[side], shape,
+                                    out.meta.nprim_slots, ntris});
+          out.meta.nprim_slots += ntris;
+        }
+      }
+      const int sinst_id = (int)out.sinsts.size();
+      const double* T = inst->transform;
+
+      if(shape->kind == SHAPE_MESH) {
+        const int first_gid = (int)out.tris.size();
+        for(int t = 0; t < ntris; ++t) {
+          double v[3][3];
+          float vf[3][3];
+          for(int k = 0; k < 3; ++k) {
+            const double p[3] = {shape->pos[shape->ids[t * 3 + k] * 3 + 0],
+                                 shape->pos[shape->ids[t * 3 + k] * 3 + 1],
+                                 shape->pos[shape->ids[t * 3 + k] * 3 + 2]};
+            apply(T, p, v[k]);
+            for(int c = 0; c < 3; ++c) vf[k][c] = (float)v[k][c];
+          }
+          DTri<R> tri;
+          PrimBox box;
+          for(int c = 0; c < 3; ++c) {
+            /* Vertices go through FP32 like the reference's Star-3D scene */
+            const R a = (R)vf[0][c], b = (R)vf[1][c], d = (R)vf[2][c];
+            tri.v0[c] = a;
+            tri.e1[c] = b - a;
+            tri.e2[c] = d - a;
+            box.lo[c] = std::min({(double)vf[0][c], (double)vf[1][c],
+                                  (double)vf[2][c]});
+            box.hi[c] = std::max({(double)vf[0][c], (double)vf[1][c],
+                                  (double)vf[2][c]});
+          }
+          tri.sinst = sinst_id;
+          tri.prim = t;
+          tri.gid = first_gid + t;
+          box.ref = primref_make(PRIM_TRIANGLE, (uint32_t)out.tris.size());
+          out.tris.push_back(tri);
+          boxes.push_back(box);
+          if(inst->sample) {
+            DSampTri<R> st;
+            double n[3], e1[3], e2[3];
+            for(int c = 0; c < 3; ++c) {
+              e1[c] = (double)vf[1][c] - vf[0][c];
+              e2[c] = (double)vf[2][c] - vf[0][c];
+            }
+            /* Star-3D front normal: e2 x e1 */
+            n[0] = e2[1] * e1[2] - e2[2] * e1[1];
+            n[1] = e2[2] * e1[0] - e2[0] * e1[2];
+            n[2] = e2[0] * e1[1] - e2[1] * e1[0];
+            const double len = std::sqrt(n[0]*n[0] + n[1]*n[1] + n[2]*n[2]);
+            for(int c = 0; c < 3; ++c) {
+              st.v0[c] = tri.v0[c];
+              st.e1[c] = tri.e1[c];
+              st.e2[c] = tri.e2[c];
+              /* normalised in FP32 like f3_normalize */
+              st.n[c] = (R)(float)(len > 0 ? n[c] / len : 0);
+            }
+            st.sinst = sinst_id;
+            st.prim = t;
+            st.gid = tri.gid;
+            st.pad = 0;
+            out.samp.push_back(st);
+            samp_area.push_back(0.5 * len);
+          }
+        }
+      } else {
+        /* Punched: one analytic patch + flat sampling proxy */
+        double M[12], W[12];
+        compose(M, T, shape->quadric.transform);
+        if(!invert(W, M)) {
+          dev->log_error("singular instance transform.\n");
+          return RES_BAD_ARG;
+        }
+        DQuadric<R> q;
+        to_rows(q.w2l, W);
+        to_rows(q.l2w, M);
+        for(int c = 0; c < 4; ++c) q.param[c] = (R)shape->qparam[c];
+        if(shape->quadric.type == SSOL_QUADRIC_HEMISPHERE)
+          q.param[2] = (R)(shape->hemi_radius * shape->hemi_radius);
+        q.carve_lo[0] = (R)shape->carve_lo[0];
+        q.carve_lo[1] = (R)shape->carve_lo[1];
+        q.carve_hi[0] = (R)shape->carve_hi[0];
+        q.carve_hi[1] = (R)shape->carve_hi[1];
+        q.grid_delta = (R)shape->grid_delta;
+        q.type = shape->quadric.type;
+        q.sinst = sinst_id;
+        q.grid_n[0] = (int32_t)shape->grid_n[0];
+        q.grid_n[1] = (int32_t)shape->grid_n[1];
+        /* A single AND rectangle equal to the AABB needs no polygon test */
+        bool aabb_only = shape->carvings.size() == 1
+          && shape->carvings[0].op == SSOL_AND
+          && shape->carvings[0].xy.size() == 8;
+        if(aabb_only) {
+          const std::vector<double>& xy = shape->carvings[0].xy;
+          for(int v = 0; v < 4 && aabb_only; ++v) {
+            const double x = xy[2 * v], y = xy[2 * v + 1];
+            aabb_only = (x == shape->carve_lo[0] || x == shape->carve_hi[0])
+                     && (y == shape->carve_lo[1] || y == shape->carve_hi[1]);
+          }
+        }
+        q.carve_first = (int32_t)out.carvings.size();
+        q.carve_count = 0;
+        if(!aabb_only) {
+          for(const Carving& c : shape->carvings) {
+            DCarving d;
+            d.first = (int32_t)(out.carve_verts.size() / 2);
+            d.count = (int32_t)(c.xy.size() / 2);
+            d.op = c.op == SSOL_AND ? 0 : 1;
+            d.pad = 0;
+            for(double x : c.xy) out.carve_verts.push_back((R)x);
+            out.carvings.push_back(d);
+            ++q.carve_count;
+          }
+        }
+        /* World box of the patch: local box corners through M */
+        double zlo, zhi;
+        quadric_z_range(shape, zlo, zhi);
+        if(shape->quadric.type == SSOL_QUADRIC_HEMISPHERE) {
+          zlo = 0;
+          zhi = shape->qparam[0];
+        }
+        PrimBox box;
+        for(int c = 0; c < 3; ++c) {
+          box.lo[c] = std::numeric_limits<double>::max();
+          box.hi[c] = -std::numeric_limits<double>::max();
+        }
+        for(int corner = 0; corner < 8; ++corner) {
+          const double p[3] = {
+            (corner & 1) ? shape->carve_hi[0] : shape->carve_lo[0],
+            (corner & 2) ? shape->carve_hi[1] : shape->carve_lo[1],
+            (corner & 4) ? zhi : zlo};
+          double w[3];
+          apply(M, p, w);
+          for(int c = 0; c < 3; ++c) {
+            box.lo[c] = std::min(box.lo[c], w[c]);
+            box.hi[c] = std::max(box.hi[c], w[c]);
+          }
+        }
+        double ext = 0;
+        for(int c = 0; c < 3; ++c) ext = std::max(ext, box.hi[c] - box.lo[c]);
+        for(int c = 0; c < 3; ++c) {
+          const double pad = 1e-5 * ext + 1e-6 * std::max(std::fabs(box.lo[c]),
+                                                          std::fabs(box.hi[c]));
+          box.lo[c] -= pad;
+          box.hi[c] += pad;
+        }
+        si.quadric = (int32_t)out.quads.size();
+        box.ref = primref_make(PRIM_QUADRIC, (uint32_t)out.quads.size());
+        out.quads.push_back(q);
+        boxes.push_back(box);
+
+        if(inst->sample) {
+          for(size_t t = 0; t + 2 < shape->samp_ids.size(); t += 3) {
+            float vf[3][3];
+            for(int k = 0; k < 3; ++k) {
+              const uint32_t id = shape->samp_ids[t + k];
+              const double p[3] = {(double)(float)shape->samp_xy[id * 2],
+                                   (double)(float)shape->samp_xy[id * 2 + 1],
+                                   0.0};
+              double w[3];
+              apply(M, p, w);
+              for(int c = 0; c < 3; ++c) vf[k][c] = (float)w[c];
+            }
+            DSampTri<R> st;
+            double n[3], e1[3], e2[3];
+            for(int c = 0; c < 3; ++c) {
+              e1[c] = (double)vf[1][c] - vf[0][c];
+              e2[c] = (double)vf[2][c] - vf[0][c];
+            }
+            n[0] = e2[1] * e1[2] - e2[2] * e1[1];
+            n[1] = e2[2] * e1[0] - e2[0] * e1[2];
+            n[2] = e2[0] * e1[1] - e2[1] * e1[0];
+            const double len = std::sqrt(n[0]*n[0] + n[1]*n[1] + n[2]*n[2]);
+            for(int c = 0; c < 3; ++c) {
+              st.v0[c] = (R)vf[0][c];
+              st.e1[c] = (R)((R)vf[1][c] - (R)vf[0][c]);
+              st.e2[c] = (R)((R)vf[2][c] - (R)vf[0][c]);
+              st.n[c] = (R)(float)(len > 0 ? n[c] / len : 0);
+            }
+            st.sinst = sinst_id;
+            st.prim = (int32_t)(t / 3);
+            st.gid = -1;
+            st.pad = 0;
+            out.samp.push_back(st);
+            samp_area.push_back(0.5 * len);
+          }
+        }
+      }
+      out.sinsts.push_back(si);
+    }
+  }
+  if(!has_sampled || out.samp.empty()) {
+    dev->log_error("No solstice instance to sample.\n");
+    return RES_BAD_ARG;
+  }
+  if(!has_receiver) dev->log_warning("No receiver is defined.\n");
+
+  build_alias(samp_area, out.alias_prob, out.alias_idx);
+  build_bvh(boxes, bvh_params, out.bvh);
+  out.nodes = bvh_nodes<R>(out.bvh);
+  return RES_OK;
+}
+
+res_T flatten_scene
+  (ssol_scene* scn, const BvhBuildParams& bvh, FlatScene<float>& out)
+{ return flatten_impl<float>(scn, bvh, out); }
+
+res_T flatten_scene
+  (ssol_scene* scn, const BvhBuildParams& bvh, FlatScene<double>& out)
+{ return flatten_impl<double>(scn, bvh, out); }
+
+} /* namespace ssolb */

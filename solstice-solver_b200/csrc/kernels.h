@@ -1,0 +1,32 @@
+/*
+ * kernels.h - host-callable launchers of the realisation kernel
+ * (kernels.cu). Plain C++ types only, so that host code compiled by the
+ * system C++ compiler can call them.
+ */
+#ifndef SSOL_B200_KERNELS_H
+#define SSOL_B200_KERNELS_H
+
+#include "device_scene.h"
+
+namespace ssolb {
+
+struct LaunchConfig {
+  int block_size; /* threads per block, <= 256; 0 => 256 */
+  int grid_blocks; /* 0 => SMs x resident blocks x waves */
+  int waves; /* persistent grid multiplier, 0 => 1 */
+  unsigned long long max_segments; /* per path segment budget */
+};
+
+/* Enqueue the realisations [first, first + count) of the stream keyed by
+ * `seed` on `stream` (a cudaStream_t); tallies accumulate into T. Returns a
+ * cudaError_t value. */
+int launch_realisations_f32
+  (const DScene<float>& S, const DTallies& T, uint64_t seed, uint64_t first,
+   uint64_t count, const LaunchConfig& cfg, void* stream);
+int launch_realisations_f64
+  (const DScene<double>& S, const DTallies& T, uint64_t seed, uint64_t first,
+   uint64_t count, const LaunchConfig& cfg, void* stream);
+
+} /* namespace ssolb */
+
+#endif /* SSOL_B200_KERNELS_H */

@@ -1,0 +1,504 @@
+/*
+ * solve.cpp - ssol_solve and the plan API: snapshot -> HBM upload ->
+ * realisation launches -> tally readback -> estimator.
+ *
+ * Orchestration of src/ssol_solver.c:1132-1361: argument checks, scene
+ * views, sun samplers, the parallel loop (here: kernel launches), the merge
+ * of per-thread tallies (here: the device already holds one set of sums),
+ * the failure rule and the RNG end state.
+ */
+#include "flatten.h"
+#include "kernels.h"
+#include "objects.h"
+
+#define SSOL_SHARED_BUILD
+#include "../../include/ssol_b200.h"
+
+#include <cuda_runtime_api.h>
+
+#include <cstring>
+#include <map>
+#include <memory>
+
+using namespace ssolb;
+
+/*******************************************************************************
+ * Device binding
+ ******************************************************************************/
+static res_T device_bind(ssol_device* dev)
+{
+  if(dev->stream) return RES_OK;
+  int ndev = 0;
+  if(cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    dev->log_error("no CUDA device available.\n");
+    return RES_UNKNOWN_ERR;
+  }
+  int cur = 0;
+  cudaGetDevice(&cur);
+  dev->cuda_device = cur;
+  cudaStream_t s;
+  if(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  dev->stream = s;
+  return RES_OK;
+}
+
+void ssolb_device_release_gpu(ssol_device* dev)
+{
+  if(dev->stream) {
+    cudaStreamDestroy((cudaStream_t)dev->stream);
+    dev->stream = nullptr;
+  }
+}
+
+/*******************************************************************************
+ * Plan
+ ******************************************************************************/
+namespace {
+
+/* One contiguous device allocation holding several arrays */
+struct Blob {
+  std::vector<unsigned char> host;
+  std::vector<size_t> offsets;
+  template<class T> size_t add(const std::vector<T>& v)
+  {
+    size_t off = (host.size() + 255) & ~size_t(255);
+    host.resize(off + v.size() * sizeof(T));
+    if(!v.empty()) std::memcpy(host.data() + off, v.data(), v.size() * sizeof(T));
+    offsets.push_back(off);
+    return off;
+  }
+};
+
+struct TallyLayout {
+  size_t global, rcv, samp, samp_rcv, prim, nb_samples, counters, stats, total;
+};
+
+} /* namespace */
+
+struct ssol_b200_plan {
+  RefCount ref;
+  ssol_device* dev = nullptr;
+  ssol_scene* scn = nullptr;
+  ssol_b200_options opt = SSOL_B200_OPTIONS_DEFAULT;
+  FlatMeta meta;
+  int nrcv = 0, nsampled = 0;
+  void* d_scene = nullptr;
+  void* d_tally = nullptr;
+  size_t scene_bytes = 0;
+  TallyLayout tl{};
+  DScene<float> s32{};
+  DScene<double> s64{};
+  DTallies t{};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double kernel_ms = 0;
+  bool timing_valid = false;
+};
+
+template<class R>
+static void bind_scene(DScene<R>& S, const FlatScene<R>& f, const Blob& b,
+                       unsigned char* base)
+{
+  size_t i = 0;
+  auto ptr = [&](void) { return base + b.offsets[i++]; };
+  S.nodes = (const DNode<R>*)ptr();
+  S.primrefs = (const uint32_t*)ptr();
+  S.tris = (const DTri<R>*)ptr();
+  S.quads = (const DQuadric<R>*)ptr();
+  S.carvings = (const DCarving*)ptr();
+  S.carve_verts = (const R*)ptr();
+  S.sinsts = (const DShadedInst*)ptr();
+  S.mtls = (const DMaterial*)ptr();
+  S.media = (const DMedium*)ptr();
+  S.spectra = (const DSpectrum*)ptr();
+  S.spec_wl = (const double*)ptr();
+  S.spec_val = (const double*)ptr();
+  S.shader_tab = (const R*)ptr();
+  S.shader_wl = (const double*)ptr();
+  S.samp = (const DSampTri<R>*)ptr();
+  S.alias_prob = (const float*)ptr();
+  S.alias_idx = (const int32_t*)ptr();
+  S.wl_nodes = (const double*)ptr();
+  S.wl_pdf = (const double*)ptr();
+  S.wl_cdf = (const double*)ptr();
+  S.shader_nodes = (int32_t)f.shader_wl.size();
+  S.nsamp = (int32_t)f.samp.size();
+  S.sun_type = f.sun_type;
+  for(int c = 0; c < 3; ++c) S.sun_dir[c] = f.sun_dir[c];
+  for(int c = 0; c < 9; ++c) S.sun_basis[c] = f.sun_basis[c];
+  S.sun_param = f.sun_param;
+  for(int c = 0; c < 8; ++c) S.buie[c] = f.buie[c];
+  S.dni = f.dni;
+  S.wl_count = (int32_t)f.wl_nodes.size();
+  S.air_medium = f.air_medium;
+  S.area_proxy = f.meta.sampled_area_proxy;
+  S.area_rt = f.meta.sampled_area;
+  S.nrcv = (int32_t)f.meta.rcv.size();
+  S.nsampled = (int32_t)f.meta.sampled.size();
+  S.nprim_slots = f.meta.nprim_slots;
+}
+
+template<class R>
+static res_T upload(ssol_b200_plan* p, const FlatScene<R>& f, DScene<R>& S)
+{
+  Blob b;
+  b.add(f.nodes);
+  b.add(f.bvh.primrefs);
+  b.add(f.tris);
+  b.add(f.quads);
+  b.add(f.carvings);
+  b.add(f.carve_verts);
+  b.add(f.sinsts);
+  b.add(f.mtls);
+  b.add(f.media);
+  b.add(f.spectra);
+  b.add(f.spec_wl);
+  b.add(f.spec_val);
+  b.add(f.shader_tab);
+  b.add(f.shader_wl);
+  b.add(f.samp);
+  b.add(f.alias_prob);
+  b.add(f.alias_idx);
+  b.add(f.wl_nodes);
+  b.add(f.wl_pdf);
+  b.add(f.wl_cdf);
+  const size_t bytes = b.host.size() + 256;
+  if(cudaMalloc(&p->d_scene, bytes) != cudaSuccess) return RES_MEM_ERR;
+  if(cudaMemcpyAsync(p->d_scene, b.host.data(), b.host.size(),
+                     cudaMemcpyHostToDevice,
+                     (cudaStream_t)p->dev->stream) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  p->scene_bytes = b.host.size();
+  bind_scene(S, f, b, (unsigned char*)p->d_scene);
+  return RES_OK;
+}
+
+static void plan_release(ssol_b200_plan* p)
+{
+  if(p->d_scene) cudaFree(p->d_scene);
+  if(p->d_tally) cudaFree(p->d_tally);
+  if(p->ev0) cudaEventDestroy(p->ev0);
+  if(p->ev1) cudaEventDestroy(p->ev1);
+  if(p->scn) ssol_scene_ref_put(p->scn);
+  ssol_device* dev = p->dev;
+  delete p;
+  if(dev) ssol_device_ref_put(dev);
+}
+
+extern "C" res_T ssol_b200_plan_ref_get(ssol_b200_plan* p)
+{
+  if(!p) return RES_BAD_ARG;
+  p->ref.get();
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_plan_ref_put(ssol_b200_plan* p)
+{
+  if(!p) return RES_BAD_ARG;
+  if(p->ref.put()) plan_release(p);
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_plan_create
+  (ssol_scene* scn, const ssol_b200_options* options, ssol_b200_plan** out)
+{
+  if(!scn || !out) return RES_BAD_ARG;
+  ssol_b200_options opt = options ? *options : SSOL_B200_OPTIONS_DEFAULT;
+  if(opt.precision != SSOL_B200_FP32 && opt.precision != SSOL_B200_FP64)
+    return RES_BAD_ARG;
+  if(opt.block_size < 0 || opt.block_size > 256 || opt.grid_blocks < 0
+  || opt.waves < 0 || opt.bvh_leaf_size < 0)
+    return RES_BAD_ARG;
+  if(opt.block_size == 0) opt.block_size = 256;
+  if(opt.block_size % 32) return RES_BAD_ARG;
+  if(opt.bvh_leaf_size == 0) opt.bvh_leaf_size = 4;
+  if(opt.max_segments == 0) opt.max_segments = 1000000ull;
+
+  BvhBuildParams bp;
+  bp.max_leaf = opt.bvh_leaf_size;
+
+  /* Snapshot on the host first: argument errors need no GPU */
+  std::unique_ptr<FlatScene<float>> f32;
+  std::unique_ptr<FlatScene<double>> f64;
+  res_T res;
+  if(opt.precision == SSOL_B200_FP32) {
+    f32.reset(new FlatScene<float>());
+    res = flatten_scene(scn, bp, *f32);
+  } else {
+    f64.reset(new FlatScene<double>());
+    res = flatten_scene(scn, bp, *f64);
+  }
+  if(res != RES_OK) return res;
+
+  res = device_bind(scn->dev);
+  if(res != RES_OK) return res;
+
+  ssol_b200_plan* p = new (std::nothrow) ssol_b200_plan();
+  if(!p) return RES_MEM_ERR;
+  ssol_device_ref_get(scn->dev);
+  p->dev = scn->dev;
+  ssol_scene_ref_get(scn);
+  p->scn = scn;
+  p->opt = opt;
+  if(f32) {
+    p->meta = f32->meta;
+    res = upload(p, *f32, p->s32);
+  } else {
+    p->meta = f64->meta;
+    res = upload(p, *f64, p->s64);
+  }
+  if(res != RES_OK) { plan_release(p); return res; }
+  p->nrcv = (int)p->meta.rcv.size();
+  p->nsampled = (int)p->meta.sampled.size();
+
+  /* Tallies: FP64 sums, then integer counters */
+  TallyLayout& tl = p->tl;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = (off + bytes + 255) & ~size_t(255);
+    return o;
+  };
+  tl.global = take(NGLOBAL * 2 * sizeof(double));
+  tl.rcv = take((size_t)p->nrcv * NRCV_Q * 2 * sizeof(double));
+  tl.samp = take((size_t)p->nsampled * 4 * sizeof(double));
+  tl.samp_rcv = take((size_t)p->nsampled * p->nrcv * NRCV_Q * 2 * sizeof(double));
+  tl.prim = take((size_t)p->meta.nprim_slots * NRCV_Q * 2 * sizeof(double));
+  tl.nb_samples = take((size_t)p->nsampled * sizeof(unsigned long long));
+  tl.counters = take(4 * sizeof(unsigned long long));
+  tl.stats = take(sizeof(DStats));
+  tl.total = off;
+  if(cudaMalloc(&p->d_tally, tl.total) != cudaSuccess) {
+    plan_release(p);
+    return RES_MEM_ERR;
+  }
+  unsigned char* base = (unsigned char*)p->d_tally;
+  p->t.global = (double*)(base + tl.global);
+  p->t.rcv = (double*)(base + tl.rcv);
+  p->t.samp = (double*)(base + tl.samp);
+  p->t.samp_rcv = (double*)(base + tl.samp_rcv);
+  p->t.prim = (double*)(base + tl.prim);
+  p->t.nb_samples = (unsigned long long*)(base + tl.nb_samples);
+  p->t.counters = (unsigned long long*)(base + tl.counters);
+  p->t.stats = (DStats*)(base + tl.stats);
+  cudaEventCreate(&p->ev0);
+  cudaEventCreate(&p->ev1);
+  *out = p;
+  return ssol_b200_plan_reset(p, nullptr);
+}
+
+static cudaStream_t plan_stream(ssol_b200_plan* p, void* stream)
+{
+  return stream ? (cudaStream_t)stream : (cudaStream_t)p->dev->stream;
+}
+
+extern "C" res_T ssol_b200_plan_reset(ssol_b200_plan* p, void* stream)
+{
+  if(!p) return RES_BAD_ARG;
+  if(cudaMemsetAsync(p->d_tally, 0, p->tl.total, plan_stream(p, stream))
+     != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  p->kernel_ms = 0;
+  p->timing_valid = false;
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_plan_launch
+  (ssol_b200_plan* p, const ssp_rng* rng, const uint64_t first,
+   const uint64_t count, void* stream)
+{
+  if(!p || !rng) return RES_BAD_ARG;
+  if(!count) return RES_OK;
+  const cudaStream_t s = plan_stream(p, stream);
+  LaunchConfig cfg;
+  cfg.block_size = p->opt.block_size;
+  cfg.grid_blocks = p->opt.grid_blocks;
+  cfg.waves = p->opt.waves;
+  cfg.max_segments = p->opt.max_segments;
+  const uint64_t start = rng->position + first;
+  cudaEventRecord(p->ev0, s);
+  const int err = p->opt.precision == SSOL_B200_FP32
+    ? launch_realisations_f32(p->s32, p->t, rng->seed, start, count, cfg, s)
+    : launch_realisations_f64(p->s64, p->t, rng->seed, start, count, cfg, s);
+  cudaEventRecord(p->ev1, s);
+  if(err != 0) {
+    p->dev->log_error("kernel launch failed: %s\n",
+                      cudaGetErrorString((cudaError_t)err));
+    return RES_UNKNOWN_ERR;
+  }
+  p->timing_valid = true;
+  return RES_OK;
+}
+
+static void fill_sums(double dst[10][2], const double* src)
+{
+  for(int q = 0; q < 10; ++q) {
+    dst[q][0] = src[2 * q];
+    dst[q][1] = src[2 * q + 1];
+  }
+}
+
+extern "C" res_T ssol_b200_plan_finish
+  (ssol_b200_plan* p, const ssp_rng* rng, const uint64_t nreal,
+   const size_t max_failed, void* stream, ssol_estimator** out)
+{
+  if(!p || !rng || !out) return RES_BAD_ARG;
+  const cudaStream_t s = plan_stream(p, stream);
+  std::vector<unsigned char> h(p->tl.total);
+  if(cudaMemcpyAsync(h.data(), p->d_tally, p->tl.total,
+                     cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  const cudaError_t err = cudaStreamSynchronize(s);
+  if(err != cudaSuccess) {
+    p->dev->log_error("device error: %s\n", cudaGetErrorString(err));
+    return RES_UNKNOWN_ERR;
+  }
+  if(p->timing_valid) {
+    float ms = 0;
+    if(cudaEventElapsedTime(&ms, p->ev0, p->ev1) == cudaSuccess)
+      p->kernel_ms = ms;
+  }
+  const unsigned char* base = h.data();
+  const double* g = (const double*)(base + p->tl.global);
+  const double* rcv = (const double*)(base + p->tl.rcv);
+  const double* samp = (const double*)(base + p->tl.samp);
+  const double* samp_rcv = (const double*)(base + p->tl.samp_rcv);
+  const double* prim = (const double*)(base + p->tl.prim);
+  const unsigned long long* nbs =
+    (const unsigned long long*)(base + p->tl.nb_samples);
+  const unsigned long long* cnt =
+    (const unsigned long long*)(base + p->tl.counters);
+  const DStats* st = (const DStats*)(base + p->tl.stats);
+
+  ssol_estimator* e = new (std::nothrow) ssol_estimator();
+  if(!e) return RES_MEM_ERR;
+  ssol_device_ref_get(p->dev);
+  e->dev = p->dev;
+  const size_t failed = (size_t)cnt[0];
+  e->failed_count = failed;
+  e->realisation_count = (size_t)nreal - std::min<size_t>(failed, nreal);
+  for(int q = 0; q < NGLOBAL; ++q) {
+    e->global[q][0] = g[2 * q];
+    e->global[q][1] = g[2 * q + 1];
+  }
+  e->sampled_area = p->meta.sampled_area;
+
+  /* Receivers are pre-registered like create_mc_receivers
+   * (src/ssol_estimator.c:30-60) */
+  for(const ssol_instance* inst : p->scn->instances) {
+    if(inst->receiver_mask) e->receivers[inst].inst = inst;
+  }
+  for(int r = 0; r < p->nrcv; ++r) {
+    const FlatMeta::RcvSide& rs = p->meta.rcv[r];
+    fill_sums(e->receivers[rs.inst].side[rs.side].q,
+              rcv + (size_t)r * NRCV_Q * 2);
+  }
+  for(const FlatMeta::PrimRange& pr : p->meta.prims) {
+    const FlatMeta::RcvSide& rs = p->meta.rcv[pr.rcv_slot];
+    std::vector<double>& v = e->receivers[rs.inst].side[rs.side].prims[pr.shape];
+    v.assign(prim + (size_t)pr.base * NRCV_Q * 2,
+             prim + (size_t)(pr.base + pr.ntris) * NRCV_Q * 2);
+  }
+  for(int si = 0; si < p->nsampled; ++si) {
+    SampEntry& se = e->sampled[p->meta.sampled[si]];
+    se.cos[0] = samp[si * 4 + 0];
+    se.cos[1] = samp[si * 4 + 1];
+    se.shadow[0] = samp[si * 4 + 2];
+    se.shadow[1] = samp[si * 4 + 3];
+    se.nb_samples = (size_t)nbs[si];
+    for(int r = 0; r < p->nrcv; ++r) {
+      const double* src = samp_rcv + ((size_t)si * p->nrcv + r) * NRCV_Q * 2;
+      bool any = false;
+      for(int q = 0; q < NRCV_Q * 2 && !any; ++q) any = src[q] != 0;
+      if(!any) continue;
+      const FlatMeta::RcvSide& rs = p->meta.rcv[r];
+      RcvEntry& re = se.by_receiver[rs.inst];
+      re.inst = rs.inst;
+      fill_sums(re.side[rs.side].q, src);
+    }
+  }
+  e->kernel_ms = p->kernel_ms;
+  e->stats[0] = st->rays;
+  e->stats[1] = st->node_visits;
+  e->stats[2] = st->tri_tests;
+  e->stats[3] = st->quad_tests;
+  e->stats[4] = st->bounces;
+  e->stats[5] = st->paths;
+  e->killed = cnt[1];
+  e->scene_bytes = p->scene_bytes;
+  e->tally_bytes = p->tl.total;
+
+  /* End state: the next realisation index (src/ssol_estimator.c:368-418) */
+  res_T res = ssolb_rng_clone_advanced(rng, nreal, &e->rng);
+  if(res != RES_OK) {
+    ssol_estimator_ref_put(e);
+    return res;
+  }
+  *out = e;
+  /* Too many failed paths: RES_BAD_OP with a valid estimator
+   * (src/ssol_solver.c:1240-1245, 1340) */
+  if(failed > 0 && failed >= max_failed) {
+    p->dev->log_error("Too many unexpected radiative paths.\n");
+    return RES_BAD_OP;
+  }
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_plan_get_stats
+  (const ssol_b200_plan* p, ssol_b200_stats* s)
+{
+  if(!p || !s) return RES_BAD_ARG;
+  std::memset(s, 0, sizeof(*s));
+  s->kernel_ms = p->kernel_ms;
+  s->scene_bytes = p->scene_bytes;
+  s->tally_bytes = p->tl.total;
+  return RES_OK;
+}
+
+/*******************************************************************************
+ * ssol_solve
+ ******************************************************************************/
+extern "C" res_T ssol_solve_ex
+  (ssol_scene* scn, const ssp_rng* rng, const size_t n,
+   const size_t max_failed, const ssol_path_tracker* tracker,
+   const ssol_b200_options* options, ssol_estimator** out)
+{
+  (void)tracker;
+  if(!scn || !rng || !n || !out) return RES_BAD_ARG;
+  if(n > (size_t)INT64_MAX || max_failed > (size_t)INT64_MAX)
+    return RES_BAD_ARG;
+  ssol_b200_plan* plan = nullptr;
+  res_T res = ssol_b200_plan_create(scn, options, &plan);
+  if(res != RES_OK) return res;
+  res = ssol_b200_plan_launch(plan, rng, 0, n, nullptr);
+  if(res == RES_OK)
+    res = ssol_b200_plan_finish(plan, rng, n, max_failed, nullptr, out);
+  ssol_b200_plan_ref_put(plan);
+  return res;
+}
+
+extern "C" res_T ssol_solve
+  (ssol_scene* scn, const ssp_rng* rng, const size_t n,
+   const size_t max_failed, const ssol_path_tracker* tracker,
+   ssol_estimator** out)
+{
+  return ssol_solve_ex(scn, rng, n, max_failed, tracker, nullptr, out);
+}
+
+extern "C" res_T ssol_estimator_get_b200_stats
+  (const ssol_estimator* e, ssol_b200_stats* s)
+{
+  if(!e || !s) return RES_BAD_ARG;
+  std::memset(s, 0, sizeof(*s));
+  s->kernel_ms = e->kernel_ms;
+  s->rays = e->stats[0];
+  s->node_visits = e->stats[1];
+  s->triangle_tests = e->stats[2];
+  s->quadric_tests = e->stats[3];
+  s->bounces = e->stats[4];
+  s->paths = e->stats[5];
+  s->killed = e->killed;
+  s->scene_bytes = e->scene_bytes;
+  s->tally_bytes = e->tally_bytes;
+  return RES_OK;
+}
