@@ -1,0 +1,366 @@
+"""Throughput of the ssol_solve realisation loop on B200.
+
+Workload (default): the 1000-heliostat radial-staggered field with a 64x64
+per-primitive receiver (workloads.heliostat_field), 1e8 realisations per
+step, FP32 geometry/BSDFs and FP64 tallies.
+
+value: Mpaths/s with the scene resident in HBM (a plan created once; each
+       step is one launch of `paths` realisations on the current CUDA
+       stream), CUDA-event timed over the K steps, L2 flushed between steps.
+e2e:   the same metric through the public C API, `ssol_solve` per step:
+       host snapshot, BVH build, host->device copy, launch, device->host
+       tally read and estimator construction, wall-clock timed around the
+       synchronous call.
+--impl reference: the CPU restatement of the reference solver (oracle/)
+       on all host cores, each step a bounded sample of the same workload.
+Multi-GPU (torchrun): each rank traces a disjoint range of realisations of
+the same scene (weak scaling, no collective on the data path); the time is
+the max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "solstice-solver_b200")
+sys.path.insert(0, PKG)
+ORACLE_LIB = os.path.join(ROOT, "oracle", "_build", "liboracle_ssol.so")
+METRIC = "Mpaths/s"
+WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann "
+            "2 mrad, reflectivity 0.9), 12x12 receiver at 100 m with 64x64 per-primitive "
+            "map, pillbox sun 4.65 mrad el 30 az 180 DNI 900, extinction 1e-4/m")
+
+
+def flops_per_run(st):
+    """Algorithmic FP32 work model: 20 FLOP per child slab test (2 per node),
+    55 per triangle test, 90 per quadric test, 150 per shaded bounce, 120 per
+    primary sample."""
+    return (20 * 2 * st["node_visits"] + 55 * st["triangle_tests"]
+            + 90 * st["quadric_tests"] + 150 * st["bounces"] + 120 * st["paths"])
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons while running."""
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = max(smax, float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() in ("active", "0x1", "yes"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def build_workload(lib, args):
+    import workloads as W
+    if args.config == "mirror":
+        s, h = W.single_mirror(lib)
+        desc = "single 10x10 mirror, 4x4 receiver at 50 m, pillbox 4.65 mrad, DNI 1000"
+    else:
+        s, h = W.heliostat_field(lib, n_helio=args.heliostats)
+        desc = WORKLOAD if args.heliostats == 1000 else WORKLOAD.replace(
+            "1000", str(args.heliostats), 1)
+    return s, h, desc
+
+
+def cpu_reference_rate(args, seconds):
+    """Oracle paths/s on all host cores for a sample of about `seconds`."""
+    import pyssol as P
+    lib = P.Lib(ORACLE_LIB)
+    s, h, _ = build_workload(lib, args)
+    probe = 20000
+    t = time.perf_counter()
+    s.solve(probe, seed=123)
+    rate = probe / (time.perf_counter() - t)
+    n = int(min(max(rate * seconds, probe), 5e8))
+    t = time.perf_counter()
+    est = s.solve(n, seed=124)
+    dt = time.perf_counter() - t
+    del est
+    return n / dt, n, dt
+
+
+def run_reference(args):
+    """CPU restatement of the reference solver on the host cores."""
+    rank, world, _ = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("gloo")
+        if rank != 0:
+            dist.barrier()
+            dist.destroy_process_group()
+            return
+    import pyssol as P
+    if not os.path.exists(ORACLE_LIB):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True,
+                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    lib = P.Lib(ORACLE_LIB)
+    s, h, desc = build_workload(lib, args)
+    probe = 20000
+    t = time.perf_counter()
+    s.solve(probe, seed=1)
+    rate = probe / (time.perf_counter() - t)
+    n = int(min(max(rate * args.ref_step_seconds, probe), args.paths))
+    for w in range(args.warmup):
+        s.solve(n, seed=100 + w)
+    t = time.perf_counter()
+    for k in range(args.steps):
+        est = s.solve(n, seed=1000 + k)
+        del est
+    dt = time.perf_counter() - t
+    value = args.steps * n / dt / 1e6
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "paths_per_step": n, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
+                         "sample": "%d realisations per step of the same scene" % n},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_b200(args):
+    import torch
+    import pyssol as P
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    lib = P.load_product()
+    s, h, desc = build_workload(lib, args)
+    opt = P.options(P.FP64 if args.fp64 else P.FP32, block_size=args.block,
+                    waves=args.waves, leaf=args.leaf)
+    plan = P.C.c_void_p()
+    lib.call("ssol_b200_plan_create", s.scn, P.C.byref(opt), P.C.byref(plan))
+    rng = s.rng(seed=args.seed)
+    stream = torch.cuda.current_stream()
+    sp = P.C.c_void_p(stream.cuda_stream)
+    n = args.paths
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step(k):
+        first = (k * world + rank) * n
+        lib.call("ssol_b200_plan_launch", plan, rng, first, n, sp)
+
+    for w in range(args.warmup):
+        step(w)
+        flush.zero_()
+    lib.call("ssol_b200_plan_reset", plan, sp)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    ev0.record(stream)
+    for k in range(args.steps):
+        kev[k][0].record(stream)
+        step(args.warmup + k)
+        kev[k][1].record(stream)
+        flush.zero_()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    kernel_ms = sum(a.elapsed_time(b) for a, b in kev)
+    if dist:
+        t = torch.tensor([ms, kernel_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, kernel_ms = float(t[0]), float(t[1])
+    est = P.C.c_void_p()
+    res = lib.raw("ssol_b200_plan_finish", plan, rng, args.steps * n, 0, sp, P.C.byref(est))
+    e = P.Estimator(s, est, res)
+    st = e.stats()
+    g = e.globals()
+    lib.raw("ssol_b200_plan_ref_put", plan)
+    total_paths = args.steps * n * world
+    value = total_paths / (ms * 1e-3) / 1e6
+
+    # e2e through the public API
+    e2e_value, h2d, d2h = None, 0, 0
+    if not args.no_e2e:
+        e2e_n = n
+        for w in range(1):
+            e_w = s.solve(e2e_n, rng=rng)
+            del e_w
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        e2e_steps = max(1, min(args.steps, 3))
+        for k in range(e2e_steps):
+            ek = s.solve(e2e_n, rng=rng)
+            sk = ek.stats()
+            h2d, d2h = sk["scene_bytes"], sk["tally_bytes"]
+            del ek
+        dt = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([dt], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t[0])
+        e2e_value = e2e_steps * e2e_n * world / dt / 1e6
+
+    peaks = measured_peaks()
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
+    sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = nsm * 128 * 2 * sm_mhz * 1e6 / 1e12
+    achieved = flops_per_run(st) / (kernel_ms * 1e-3) / 1e12 if kernel_ms > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.fp64 else "f32",
+        "data": "synthetic (seeded generator, no public scene)",
+        "config": {"workload": desc, "paths_per_step": n, "precision":
+                   "FP64" if args.fp64 else "FP32 geometry/BSDF, FP64 tallies",
+                   "l2": "flushed: 256 MiB write between steps (scene < 2 MB)",
+                   "parallelism": "realisation ranges per GPU" if world > 1 else "1 GPU"},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "timing": "wall clock around synchronous ssol_solve"},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak else None,
+                     "traffic": None,
+                     "peak_source": "SMs x 128 FP32 lanes x 2 x measured max SM clock "
+                                    "(MEASURED_PEAKS.json sm_max_mhz)",
+                     "work_model": "20/slab x2 per node + 55/triangle + 90/quadric + "
+                                   "150/bounce + 120/path (counted on device)",
+                     "counters_per_path": {k: st[k] / max(1, st["paths"]) for k in
+                                           ("rays", "node_visits", "triangle_tests",
+                                            "quadric_tests", "bounces")},
+                     "kernel_ms": kernel_ms},
+        "clocks": clk,
+        "estimate": {"absorbed_by_receivers_W": g["absorbed_by_receivers"][0],
+                     "rel_se": g["absorbed_by_receivers"][2] / max(1e-30,
+                                                                  g["absorbed_by_receivers"][0])},
+    }
+    if rank == 0 and not args.no_cpu:
+        try:
+            rate, cn, cdt = cpu_reference_rate(args, args.cpu_seconds)
+            line["cpu_baseline"] = {
+                "value": rate / 1e6, "unit": METRIC, "cores": os.cpu_count(), "kind": "port",
+                "sample": "%d realisations of the same scene in %.1f s (OpenMP, all cores)"
+                          % (cn, cdt)}
+        except Exception as exc:
+            line["cpu_baseline"] = {"value": None, "unit": METRIC, "cores": os.cpu_count(),
+                                    "kind": "port", "sample": "failed: %s" % exc}
+    if rank == 0:
+        print(json.dumps(line))
+    del e
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--config", default="field", choices=["field", "mirror"])
+    p.add_argument("--heliostats", type=int, default=1000)
+    p.add_argument("--paths", type=int, default=100_000_000)
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--fp64", action="store_true")
+    p.add_argument("--block", type=int, default=256)
+    p.add_argument("--waves", type=int, default=1)
+    p.add_argument("--leaf", type=int, default=4)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=10.0)
+    p.add_argument("--ref-step-seconds", type=float, default=10.0)
+    args = p.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -484,6 +484,24 @@ __device__ __forceinline__ void test_triangle
   found = true;
 }
 
+/* Triangle of the RT tessellation grid that contains local (x, y): cell
+ * (ix, iy) holds triangles 2 (ix ny + iy) (below its diagonal) and + 1;
+ * only used when no carving cut the grid */
+template<class R>
+__device__ __forceinline__ int quad_grid_prim(const DQuadric<R>& Q, R x, R y)
+{
+  if(Q.grid_n[0] <= 0 || Q.grid_n[1] <= 0 || !(Q.grid_delta > R(0))) return 0;
+  const R d = Q.grid_delta;
+  int ix = (int)floor((x - Q.carve_lo[0]) / d);
+  int iy = (int)floor((y - Q.carve_lo[1]) / d);
+  ix = min(max(ix, 0), Q.grid_n[0] - 1);
+  iy = min(max(iy, 0), Q.grid_n[1] - 1);
+  const R x0 = Q.carve_lo[0] + (R)ix * d, y0 = Q.carve_lo[1] + (R)iy * d;
+  const R x1 = fmin(x0 + d, Q.carve_hi[0]), y1 = fmin(y0 + d, Q.carve_hi[1]);
+  const bool lower = (x - x0) * (y1 - y0) >= (y - y0) * (x1 - x0);
+  return (ix * Q.grid_n[1] + iy) * 2 + (lower ? 0 : 1);
+}
+
 /* Punched rule: analytic roots inside the carved domain, not below tmin, and
  * not the opposite side of the shape the ray leaves */
 template<class R>
@@ -515,7 +533,7 @@ __device__ __forceinline__ void test_quadric
     if(!side_passes(S, Q.sinst, side, self)) continue;
     best.t = t;
     best.sinst = Q.sinst;
-    best.prim = 0;
+    best.prim = quad_grid_prim(Q, pl.x, pl.y);
     best.gid = -1;
     best.n = nw;
     found = true;

@@ -138,6 +138,78 @@ static void bind_scene(DScene<R>& S, const FlatScene<R>& f, const Blob& b,
   S.nprim_slots = f.meta.nprim_slots;
 }
 
+/* Every index the kernel dereferences, checked on the host before upload */
+template<class R>
+static bool validate(const FlatScene<R>& f)
+{
+  const int64_t nnodes = (int64_t)f.nodes.size();
+  const int64_t nrefs = (int64_t)f.bvh.primrefs.size();
+  if(nnodes < 1) return false;
+  for(const DNode<R>& n : f.nodes) {
+    for(int k = 0; k < 2; ++k) {
+      if(n.count[k] == 0) {
+        if(n.child[k] <= 0 || n.child[k] >= nnodes) return false;
+      } else if(n.count[k] > 0) {
+        if(n.child[k] < 0 || (int64_t)n.child[k] + n.count[k] > nrefs) return false;
+      }
+    }
+  }
+  for(uint32_t ref : f.bvh.primrefs) {
+    const uint32_t i = primref_index(ref);
+    if(primref_kind(ref) == PRIM_TRIANGLE ? i >= f.tris.size() : i >= f.quads.size())
+      return false;
+  }
+  const int64_t nsi = (int64_t)f.sinsts.size();
+  const int nrcv = (int)f.meta.rcv.size();
+  const int nsampled = (int)f.meta.sampled.size();
+  for(const DTri<R>& t : f.tris)
+    if(t.sinst < 0 || t.sinst >= nsi) return false;
+  for(const DQuadric<R>& q : f.quads) {
+    if(q.sinst < 0 || q.sinst >= nsi) return false;
+    if(q.carve_first < 0
+    || (size_t)q.carve_first + (size_t)q.carve_count > f.carvings.size()) return false;
+  }
+  for(const DCarving& c : f.carvings)
+    if(c.first < 0 || (size_t)(c.first + c.count) * 2 > f.carve_verts.size()) return false;
+  for(const DShadedInst& si : f.sinsts) {
+    for(int k = 0; k < 2; ++k) {
+      if(si.mtl[k] < 0 || si.mtl[k] >= (int)f.mtls.size()) return false;
+      if(si.rcv_slot[k] >= nrcv) return false;
+      if(si.prim_base[k] >= 0 && si.rcv_slot[k] < 0) return false;
+    }
+    if(si.sampled >= nsampled) return false;
+    if(si.is_punched && (si.quadric < 0 || si.quadric >= (int)f.quads.size())) return false;
+  }
+  for(const DMaterial& m : f.mtls) {
+    const int nm = (int)f.media.size();
+    if(m.in_medium < 0 || m.in_medium >= nm || m.out_medium < 0
+    || m.out_medium >= nm || m.slab_medium < 0 || m.slab_medium >= nm)
+      return false;
+    if(m.table < 0 || (size_t)m.table + 2 * f.shader_wl.size() > f.shader_tab.size())
+      return false;
+  }
+  for(const DMedium& m : f.media)
+    for(const DData* d : {&m.extinction, &m.refractive_index})
+      if(d->spectrum >= (int)f.spectra.size()) return false;
+  for(const DSpectrum& sp : f.spectra)
+    if(sp.count < 1 || (size_t)(sp.first + sp.count) > f.spec_wl.size()) return false;
+  const int64_t nsamp = (int64_t)f.samp.size();
+  if(nsamp < 1 || f.alias_prob.size() != f.samp.size()
+  || f.alias_idx.size() != f.samp.size()) return false;
+  for(int32_t a : f.alias_idx) if(a < 0 || a >= nsamp) return false;
+  for(const DSampTri<R>& t : f.samp) {
+    if(t.sinst < 0 || t.sinst >= nsi) return false;
+    if(f.sinsts[t.sinst].sampled < 0) return false;
+    if(t.gid >= (int64_t)f.tris.size()) return false;
+  }
+  /* per-primitive slots stay inside the tally array */
+  for(const FlatMeta::PrimRange& pr : f.meta.prims)
+    if(pr.base < 0 || pr.base + pr.ntris > f.meta.nprim_slots) return false;
+  if(f.air_medium < 0 || f.air_medium >= (int)f.media.size()) return false;
+  if(f.wl_nodes.empty() || f.wl_cdf.size() != f.wl_nodes.size()) return false;
+  return true;
+}
+
 template<class R>
 static res_T upload(ssol_b200_plan* p, const FlatScene<R>& f, DScene<R>& S)
 {
@@ -229,6 +301,10 @@ extern "C" res_T ssol_b200_plan_create
     res = flatten_scene(scn, bp, *f64);
   }
   if(res != RES_OK) return res;
+  if(f32 ? !validate(*f32) : !validate(*f64)) {
+    scn->dev->log_error("inconsistent device scene snapshot.\n");
+    return RES_UNKNOWN_ERR;
+  }
 
   res = device_bind(scn->dev);
   if(res != RES_OK) return res;

@@ -1,0 +1,163 @@
+"""Synthetic solar-field workloads, described through the ssol C API.
+
+No public benchmark scene ships with the reference, so these seeded
+generators stand in for the solar fields the solver is used on. Every choice
+that the workload descriptions leave open (frame, azimuth convention, field
+sector, receiver tilt, back-face materials) is fixed here and documented in
+the function docstrings.
+
+Conventions: z up; azimuth measured from +y (north) clockwise toward +x
+(east); the sun direction passed to ssol_sun_set_direction points from the
+sun toward the scene.
+"""
+import math
+
+import pyssol as P
+
+
+def _unit(v):
+    n = math.sqrt(sum(c * c for c in v))
+    return tuple(c / n for c in v)
+
+
+def _cross(a, b):
+    return (a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0])
+
+
+def to_sun(elevation_deg, azimuth_deg):
+    el, az = math.radians(elevation_deg), math.radians(azimuth_deg)
+    return (math.sin(az) * math.cos(el), math.cos(az) * math.cos(el), math.sin(el))
+
+
+def frame_z_to(n, up=(0.0, 0.0, 1.0)):
+    """Row-major rotation whose third column is n (local +z -> n)."""
+    n = _unit(n)
+    x = _cross(up, n)
+    if sum(c * c for c in x) < 1e-12:
+        x = (1.0, 0.0, 0.0)
+    x = _unit(x)
+    y = _cross(n, x)
+    return ((x[0], y[0], n[0]), (x[1], y[1], n[1]), (x[2], y[2], n[2]))
+
+
+def grid_mesh(scene, size_x, size_y, nx, ny):
+    """Flat size_x x size_y rectangle split into nx x ny quads (2 triangles
+    each, front face +z like the reference rectangle)."""
+    verts = []
+    for j in range(ny + 1):
+        for i in range(nx + 1):
+            verts.append((-0.5 * size_x + size_x * i / nx, -0.5 * size_y + size_y * j / ny, 0.0))
+    ids = []
+    for j in range(ny):
+        for i in range(nx):
+            a = j * (nx + 1) + i
+            b, c, d = a + 1, a + nx + 2, a + nx + 1
+            ids.append((a, c, b))
+            ids.append((c, a, d))
+    return scene.mesh(verts, ids)
+
+
+# --------------------------------------------------------------- config 1
+def single_mirror(lib, n_paths=1_000_000):
+    """One 10x10 flat mirror and a 4x4 receiver 50 m along the reflected ray.
+
+    Frame: to-sun s = (0, -cos45, sin45), to-receiver r = (0, cos45, sin45),
+    so the mirror is horizontal at the origin. Sun: pillbox 4.65 mrad,
+    DNI 1000, no atmosphere. Mirror: specular, reflectivity 0.9, both sides.
+    Receiver: 4x4 at 50 r, front face toward the mirror, specular
+    reflectivity 0.05 (absorptivity 0.95), front side receiver, not sampled.
+    """
+    s = P.Scene(lib)
+    c = math.cos(math.pi / 4)
+    sun_to = (0.0, -c, c)
+    r = (0.0, c, c)
+    mirror = s.rectangle(5, 5)
+    m_mtl = s.mirror(0.9, 0.0)
+    helio = s.instance(s.object([(mirror, m_mtl, m_mtl)]))
+    rshape = s.rectangle(2, 2)
+    r_mtl = s.mirror(0.05, 0.0)
+    R = frame_z_to((-r[0], -r[1], -r[2]), up=(1.0, 0.0, 0.0))
+    rcv = s.instance(s.object([(rshape, r_mtl, r_mtl)]),
+                     P.transform_from(R, (50 * r[0], 50 * r[1], 50 * r[2])),
+                     receiver=P.SSOL_FRONT, sample=0)
+    s.set_sun("pillbox", tuple(-x for x in sun_to), 1000.0, param=4.65e-3)
+    return s, {"heliostat": helio, "receiver": rcv, "receiver_shape": rshape,
+               "n_paths": n_paths}
+
+
+# --------------------------------------------------------------- config 2
+def field_layout(n=1000, r_min=100.0, r_max=600.0, spacing=15.0, dr=14.0,
+                 height=5.0):
+    """Radial-staggered positions in a north sector, nearest first.
+
+    Rows every `dr` metres from r_min; `spacing` metres between neighbours
+    along a row; odd rows shifted by half a spacing. The sector half angle is
+    the smallest (0.5 degree steps) that yields n positions within r_max.
+    """
+    def layout(half):
+        pts = []
+        k = 0
+        rr = r_min
+        while rr <= r_max + 1e-9:
+            dphi = spacing / rr
+            m = int(2 * half / dphi)
+            off = 0.5 * dphi if k % 2 else 0.0
+            for i in range(m + 1):
+                phi = -half + off + i * dphi
+                if phi > half:
+                    break
+                pts.append((rr * math.sin(phi), rr * math.cos(phi), height))
+            k += 1
+            rr += dr
+        return pts
+
+    half = math.radians(20)
+    while True:
+        pts = layout(half)
+        if len(pts) >= n or half > math.radians(89):
+            break
+        half += math.radians(0.5)
+    pts.sort(key=lambda p: (p[0] ** 2 + p[1] ** 2, p[0]))
+    return pts[:n]
+
+
+def heliostat_field(lib, n_helio=1000, elevation=30.0, azimuth=180.0, dni=900.0,
+                    aim=(0.0, 0.0, 100.0), slope_error=2e-3, extinction=1e-4,
+                    receiver_cells=64, per_primitive=True, reaim=None):
+    """1000 flat 10x10 heliostats aimed at a 12x12 receiver on a 100 m tower.
+
+    Heliostats: one object (2 triangles), instanced n_helio times on
+    field_layout(); front: mirror reflectivity 0.9 with Beckmann slope error
+    2 mrad; back: absorbing matte. Each normal bisects the to-sun direction
+    and the direction to `aim`. Receiver: 12x12 plate centred on `aim`,
+    facing the field centroid, specular reflectivity 0.05 (absorptivity
+    0.95), split into receiver_cells^2 quads (2 triangles each) with
+    per-primitive tallies on its front side. Sun: pillbox 4.65 mrad at
+    (elevation, azimuth), DNI 900. Atmosphere: extinction 1e-4 /m.
+    """
+    s = P.Scene(lib)
+    sun = to_sun(elevation, azimuth)
+    pts = field_layout(n_helio)
+    helio_shape = s.rectangle(5, 5)
+    front = s.mirror(0.9, slope_error, P.BECKMANN)
+    back = s.matte(0.0)
+    hobj = s.object([(helio_shape, front, back)])
+    helios = []
+    for p in pts:
+        a = _unit((aim[0] - p[0], aim[1] - p[1], aim[2] - p[2]))
+        n = _unit((sun[0] + a[0], sun[1] + a[1], sun[2] + a[2]))
+        helios.append(s.instance(hobj, P.transform_from(frame_z_to(n), p)))
+    cx = sum(p[0] for p in pts) / len(pts)
+    cy = sum(p[1] for p in pts) / len(pts)
+    cz = sum(p[2] for p in pts) / len(pts)
+    rn = _unit((cx - aim[0], cy - aim[1], cz - aim[2]))
+    rshape = grid_mesh(s, 12.0, 12.0, receiver_cells, receiver_cells)
+    rmtl = s.mirror(0.05, 0.0)
+    rcv = s.instance(s.object([(rshape, rmtl, rmtl)]), P.transform_from(frame_z_to(rn), aim),
+                     receiver=P.SSOL_FRONT, per_primitive=1 if per_primitive else 0,
+                     sample=0)
+    s.set_sun("pillbox", tuple(-x for x in sun), dni, param=4.65e-3)
+    if extinction:
+        s.atmosphere(extinction)
+    return s, {"heliostats": helios, "receiver": rcv, "receiver_shape": rshape,
+               "positions": pts, "sun": sun}

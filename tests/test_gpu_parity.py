@@ -1,0 +1,174 @@
+"""Parity of the B200 library with the CPU oracle, through the C-ABI.
+
+Every estimate (global, per receiver side, per sampled x receiver, per
+primitive) must agree within 3 combined standard errors:
+    |E_gpu - E_oracle| <= 3 sqrt(SE_gpu^2 + SE_oracle^2)
+(a 1e-9 relative floor absorbs FP64 summation-order noise when both SE are 0).
+Both libraries consume the same Philox streams, so most paths are identical
+and the agreement is usually far tighter than the bound. The reference's
+closed forms are also checked directly on the GPU.
+"""
+import math
+
+import pytest
+
+import pyssol as P
+import ref_scenes as R
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+K = 3.0
+REL_FLOOR = 1e-9
+
+
+def close(a, b):
+    return abs(a[0] - b[0]) <= K * math.hypot(a[2], b[2]) + REL_FLOOR * max(1.0, abs(b[0]))
+
+
+def assert_dict_close(got, ref, what):
+    bad = {k: (got[k], ref[k]) for k in ref if not close(got[k], ref[k])}
+    assert not bad, "%s differs: %r" % (what, bad)
+
+
+def run_both(product, oracle, builder, n, seed=0, **kw):
+    sg, hg = builder(product, **kw)
+    sc, hc = builder(oracle, **kw)
+    return (sg, hg, sg.solve(n, seed=seed)), (sc, hc, sc.solve(n, seed=seed))
+
+
+def test_single_mirror_vs_oracle(product, oracle):
+    (sg, hg, eg), (sc, hc, ec) = run_both(product, oracle, W.single_mirror, 500000, seed=11)
+    assert eg.count("realisation_count") == ec.count("realisation_count") == 500000
+    assert_dict_close(eg.globals(), ec.globals(), "globals")
+    assert_dict_close(eg.receiver(hg["receiver"]), ec.receiver(hc["receiver"]), "receiver")
+    assert_dict_close(eg.sampled_x_receiver(hg["heliostat"], hg["receiver"]),
+                      ec.sampled_x_receiver(hc["heliostat"], hc["receiver"]), "samp x rcv")
+    sg_, sc_ = eg.sampled(hg["heliostat"]), ec.sampled(hc["heliostat"])
+    assert sg_["nb_samples"] == sc_["nb_samples"] == 500000
+    assert close(sg_["cos_factor"], sc_["cos_factor"])
+    assert eg.sampled_area() == pytest.approx(ec.sampled_area(), rel=1e-12)
+    # Shared streams: the mean incoming flux matches to far below one SE
+    gi, ci = eg.receiver(hg["receiver"])["incoming_flux"], ec.receiver(hc["receiver"])["incoming_flux"]
+    assert abs(gi[0] - ci[0]) <= 0.05 * ci[2]
+
+
+def test_field_vs_oracle(product, oracle):
+    """120 heliostats of the radial-staggered field, Beckmann 2 mrad, k=1e-4,
+    per-primitive 16x16 receiver."""
+    kw = dict(n_helio=120, receiver_cells=16)
+    (sg, hg, eg), (sc, hc, ec) = run_both(product, oracle, W.heliostat_field, 400000,
+                                          seed=3, **kw)
+    assert eg.count("failed_count") == ec.count("failed_count") == 0
+    assert_dict_close(eg.globals(), ec.globals(), "globals")
+    assert_dict_close(eg.receiver(hg["receiver"]), ec.receiver(hc["receiver"]), "receiver")
+    pg = eg.primitives(hg["receiver"], hg["receiver_shape"])
+    pc = ec.primitives(hc["receiver"], hc["receiver_shape"])
+    assert len(pg) == len(pc) == 16 * 16 * 2
+    for i, (a, b) in enumerate(zip(pg, pc)):
+        assert_dict_close(a, b, "primitive %d" % i)
+    for k in (0, 7, 60, 119):
+        assert_dict_close(eg.sampled_x_receiver(hg["heliostats"][k], hg["receiver"]),
+                          ec.sampled_x_receiver(hc["heliostats"][k], hc["receiver"]),
+                          "heliostat %d x receiver" % k)
+        a, b = eg.sampled(hg["heliostats"][k]), ec.sampled(hc["heliostats"][k])
+        assert a["nb_samples"] == b["nb_samples"]
+        assert close(a["cos_factor"], b["cos_factor"]) and close(a["shadowed"], b["shadowed"])
+
+
+def test_fp32_vs_fp64(product):
+    """The FP32 build against the all-FP64 build on identical random numbers."""
+    s, h = W.heliostat_field(product, n_helio=120, receiver_cells=16)
+    e32 = s.solve(400000, seed=5, options=P.options(P.FP32))
+    e64 = s.solve(400000, seed=5, options=P.options(P.FP64))
+    g32, g64 = e32.globals(), e64.globals()
+    for k in g64:
+        assert close(g32[k], g64[k]), k
+    r32, r64 = e32.receiver(h["receiver"]), e64.receiver(h["receiver"])
+    for k in r64:
+        assert close(r32[k], r64[k]), k
+    a, b = r32["absorbed_flux"][0], r64["absorbed_flux"][0]
+    assert abs(a - b) <= 1e-3 * abs(b)
+
+
+def test_gpu_solver1_closed_forms(product):
+    """src/test_ssol_solver1.c:312-373 on the GPU."""
+    s, h = R.solver1_base(product)
+    n = 10000
+    est = s.solve(n, seed=1)
+    m = 4 * R.DNI * R.COS45
+    std = math.sqrt(((12 * R.DNI * R.COS45) ** 2 / 3 - m ** 2) / n)
+    g = est.globals()
+    assert abs(g["shadowed"][0] - m) <= 2 * std
+    rcv = est.receiver(h["target"])
+    assert abs(rcv["incoming_flux"][0] - m) <= 3 * std
+    product.call("ssol_instance_sample", h["target"], 0)
+    product.call("ssol_instance_sample", h["secondary"], 0)
+    est = s.solve(n, seed=2)
+    g = est.globals()
+    assert abs(g["shadowed"][0]) <= 1e-4
+    assert g["cos_factor"][0] == pytest.approx(R.COS45, rel=1e-4)
+    rcv = est.receiver(h["target"])
+    assert rcv["incoming_flux"][0] == pytest.approx(m, rel=1e-6)
+    assert abs(rcv["incoming_flux"][2]) <= 1e-3
+
+
+def test_gpu_atmosphere_and_primitives(product, oracle):
+    """src/test_ssol_solver1.c:402-485 on the GPU, and against the oracle."""
+    outs = []
+    for lib in (product, oracle):
+        s, h = R.solver1_base(lib)
+        lib.call("ssol_instance_sample", h["target"], 0)
+        lib.call("ssol_instance_sample", h["secondary"], 0)
+        lib.call("ssol_scene_detach_instance", s.scn, h["heliostat"])
+        m2 = s.mirror(0.87, 0.0)
+        s.instance(s.object([(h["square"], m2, m2)]), receiver=P.SSOL_FRONT)
+        s.atmosphere(0.03)
+        lib.call("ssol_instance_set_receiver", h["target"], P.SSOL_FRONT, 1)
+        est = s.solve(10000, seed=3)
+        outs.append((s, h, est))
+    (sg, hg, eg), (sc, hc, ec) = outs
+    a_m = 0.87 * 4 * math.exp(-0.03 * 4 * math.sqrt(2)) * R.DNI * R.COS45
+    rcv = eg.receiver(hg["target"])
+    assert rcv["incoming_flux"][0] == pytest.approx(a_m, rel=1e-4)
+    prims = eg.primitives(hg["target"], hg["square"])
+    assert sum(p["incoming_flux"][0] * 2.0 for p in prims) == pytest.approx(a_m, rel=1e-4)
+    assert_dict_close(eg.globals(), ec.globals(), "globals")
+    assert_dict_close(rcv, ec.receiver(hc["target"]), "receiver")
+
+
+@pytest.mark.parametrize("kind,param", [("pillbox", 1.0), ("gaussian", 0.01),
+                                        ("buie", 0.1)])
+def test_gpu_flat_exact_and_parabol(product, oracle, kind, param):
+    """src/test_ssol_solver10.c, 11.c, 12.c on the GPU: exact DNI x 100 with
+    zero variance on the flat square; paraboloid within 3 SE of DNI x 100."""
+    s, h = R.flat_and_parabol(product, kind, param)
+    est = s.solve(10000, seed=5)
+    g = est.globals()
+    assert g["cos_factor"][0] == 1.0 and g["cos_factor"][2] == 0.0
+    assert g["absorbed_by_receivers"][0] == R.DNI * 100
+    assert g["absorbed_by_receivers"][2] == 0.0
+    R.add_parabol_10(s, h["matte"])
+    product.call("ssol_scene_detach_instance", s.scn, h["geom1"])
+    est = s.solve(100000, seed=6)
+    g = est.globals()
+    assert abs(g["absorbed_by_receivers"][0] - R.DNI * 100) <= 3 * g["absorbed_by_receivers"][2]
+    so, ho = R.flat_and_parabol(oracle, kind, param)
+    R.add_parabol_10(so, ho["matte"])
+    oracle.call("ssol_scene_detach_instance", so.scn, ho["geom1"])
+    assert_dict_close(g, so.solve(100000, seed=6).globals(), "paraboloid globals")
+
+
+def test_gpu_rng_continuation(product):
+    """src/test_ssol_solver6.c:204-235: a solve started from the estimator's
+    RNG end state uses disjoint streams."""
+    s, h = W.single_mirror(product)
+    rng = s.rng(seed=9)
+    e1 = s.solve(100000, rng=rng)
+    state = P.C.c_void_p()
+    product.call("ssol_estimator_get_rng_state", e1.h, P.C.byref(state))
+    e2 = s.solve(100000, rng=state)
+    a = e1.receiver(h["receiver"])["incoming_flux"]
+    b = e2.receiver(h["receiver"])["incoming_flux"]
+    assert a[0] != b[0]
+    assert close(a, b)
