@@ -209,8 +209,12 @@ def run_b200(args):
     plan = P.C.c_void_p()
     lib.call("ssol_b200_plan_create", s.scn, P.C.byref(opt), P.C.byref(plan))
     rng = s.rng(seed=args.seed)
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: its handle is what the library launches on (a NULL
+    # handle would select the plan's own stream, outside these events)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sp = P.C.c_void_p(stream.cuda_stream)
+    assert sp.value, "expected a non-default CUDA stream"
     n = args.paths
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 

@@ -565,7 +565,13 @@ __device__ bool trace_ray
    Hit<R>& best, Counters& cnt)
 {
   ++cnt.rays;
-  const V3<R> inv = mk(R(1) / d.x, R(1) / d.y, R(1) / d.z);
+  /* A zero direction component would make lo * inv - o * inv an inf - inf
+   * NaN for boxes the ray runs parallel to; clamp it to +-2^-64 so that the
+   * FMA form of the slab test stays finite (Aila and Laine, HPG 2009) */
+  const R tiny = R(5.42101086242752217e-20);
+  const V3<R> inv = mk(R(1) / (fabs(d.x) > tiny ? d.x : cpsgn(tiny, d.x)),
+                       R(1) / (fabs(d.y) > tiny ? d.y : cpsgn(tiny, d.y)),
+                       R(1) / (fabs(d.z) > tiny ? d.z : cpsgn(tiny, d.z)));
   const V3<R> oinv = mk(o.x * inv.x, o.y * inv.y, o.z * inv.z);
   /* Self-hit epsilon of the mesh rule: the reference's 1e-6, scaled by the
    * magnitude of the origin so that it stays above the FP32 resolution */

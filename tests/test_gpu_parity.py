@@ -3,7 +3,7 @@
 Every estimate (global, per receiver side, per sampled x receiver, per
 primitive) must agree within 3 combined standard errors:
     |E_gpu - E_oracle| <= 3 sqrt(SE_gpu^2 + SE_oracle^2)
-(a 1e-9 relative floor absorbs FP64 summation-order noise when both SE are 0).
+(a 1e-6 relative floor covers FP32 geometry on zero-variance estimates).
 Both libraries consume the same Philox streams, so most paths are identical
 and the agreement is usually far tighter than the bound. The reference's
 closed forms are also checked directly on the GPU.
@@ -19,7 +19,7 @@ import workloads as W
 pytestmark = pytest.mark.gpu
 
 K = 3.0
-REL_FLOOR = 1e-9
+REL_FLOOR = 1e-6  # FP32 geometry on zero-variance estimates (north_star: <= 1e-5)
 
 
 def close(a, b):
