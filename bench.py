@@ -205,7 +205,7 @@ def run_b200(args):
     lib = P.load_product()
     s, h, desc = build_workload(lib, args)
     opt = P.options(P.FP64 if args.fp64 else P.FP32, block_size=args.block,
-                    waves=args.waves, leaf=args.leaf)
+                    waves=args.waves, leaf=args.leaf, min_blocks=args.minb)
     plan = P.C.c_void_p()
     lib.call("ssol_b200_plan_create", s.scn, P.C.byref(opt), P.C.byref(plan))
     rng = s.rng(seed=args.seed)
@@ -354,7 +354,8 @@ def main():
     p.add_argument("--fp64", action="store_true")
     p.add_argument("--block", type=int, default=256)
     p.add_argument("--waves", type=int, default=1)
-    p.add_argument("--leaf", type=int, default=4)
+    p.add_argument("--leaf", type=int, default=0)
+    p.add_argument("--minb", type=int, default=0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=10.0)

@@ -31,10 +31,12 @@ struct ssol_b200_options {
   int block_size; /* threads per block, <= 256; 0 => 256 */
   int grid_blocks; /* 0 => one persistent wave sized from occupancy */
   int waves; /* persistent grid multiplier when grid_blocks == 0 */
-  int bvh_leaf_size; /* primitives per BVH leaf; 0 => 4 */
+  int bvh_leaf_size; /* primitives per BVH leaf; 0 => 1 */
   unsigned long long max_segments; /* path segment budget; 0 => 1e6 */
+  int min_blocks_per_sm; /* register budget of the kernel variant: 1, 2, 3;
+                          * 0 => 2 */
 };
-#define SSOL_B200_OPTIONS_DEFAULT__ { SSOL_B200_FP32, 256, 0, 1, 4, 0 }
+#define SSOL_B200_OPTIONS_DEFAULT__ { SSOL_B200_FP32, 256, 0, 1, 0, 0, 0 }
 static const struct ssol_b200_options SSOL_B200_OPTIONS_DEFAULT =
   SSOL_B200_OPTIONS_DEFAULT__;
 

@@ -61,6 +61,8 @@ int split(std::vector<PrimBox>& p, int b, int e, const BvhBuildParams& prm,
 {
   const int n = e - b;
   if(n <= prm.max_leaf) return -1;
+  /* Depth cap: a large leaf is slower but keeps the traversal stack bounded */
+  if(depth >= prm.max_depth - 1) return -1;
   Box cb;
   cb.reset();
   for(int i = b; i < e; ++i) {
@@ -68,7 +70,7 @@ int split(std::vector<PrimBox>& p, int b, int e, const BvhBuildParams& prm,
     for(int k = 0; k < 3; ++k) c[k] = centroid(p[i], k);
     cb.grow(c, c);
   }
-  const bool force_median = depth >= prm.max_depth - 8;
+  const bool force_median = depth >= prm.max_depth - 10;
   double best_cost = std::numeric_limits<double>::max();
   int best_axis = -1, best_bin = -1;
   const int nb = prm.bins;

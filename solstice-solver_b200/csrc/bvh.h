@@ -21,7 +21,7 @@ struct PrimBox {
 struct BvhBuildParams {
   int max_leaf = 4; /* primitives per leaf */
   int bins = 16; /* SAH bins per axis */
-  int max_depth = 60; /* below the device traversal stack */
+  int max_depth = 30; /* the device traversal stack holds 32 entries */
 };
 
 struct BvhResult {

@@ -174,7 +174,7 @@ __device__ __forceinline__ V3<R> sun_local_to_world(const DScene<R>& S, V3<R> p)
 /* Buie zenith angle by rejection (src/ssol_ranst_sun_dir.c:177-195); the
  * draws of attempt k come from event 2 + k of the primary domain */
 template<class R>
-__device__ double buie_theta(const DScene<R>& S, const Rng& rng)
+__device__ __noinline__ double buie_theta(const DScene<R>& S, const Rng& rng)
 {
   const double thetaSD = S.buie[0], dCSSD = S.buie[1], gamma = S.buie[2];
   const double ek1000g = S.buie[3], alpha = S.buie[4];
@@ -556,13 +556,17 @@ __device__ __forceinline__ bool slab
   return t0 <= t1;
 }
 
-constexpr int STACK_SIZE = 64;
+/* The builder bounds the BVH depth to 30, so a traversal never holds more
+ * than 30 deferred nodes */
+constexpr int STACK_SIZE = 32;
 
-/* Closest accepted hit (ANY == false) or any accepted hit (ANY == true) */
-template<class R, bool ANY>
+/* Closest accepted hit, or the first accepted hit when `any` (shadow rays).
+ * The deferred-node stack lives in shared memory: entry i of this thread is
+ * stack[i * stride]. */
+template<class R>
 __device__ bool trace_ray
   (const DScene<R>& S, V3<R> o, V3<R> d, R tmin, const SelfInfo& self,
-   Hit<R>& best, Counters& cnt)
+   bool any, Hit<R>& best, Counters& cnt, int* stack, int stride)
 {
   ++cnt.rays;
   /* A zero direction component would make lo * inv - o * inv an inf - inf
@@ -579,7 +583,6 @@ __device__ bool trace_ray
   const R eps = R(1e-6) * (R(1) + amax);
   best.t = rmax<R>();
   bool found = false;
-  int stack[STACK_SIZE];
   int sp = 0;
   int node = 0;
   for(;;) {
@@ -607,7 +610,7 @@ __device__ bool trace_ray
             test_quadric(S, (int)primref_index(ref), o, d, tmin, self,
                          best, found);
           }
-          if(ANY && found) return true;
+          if(any && found) return true;
         }
       } else {
         next[nnext++] = k;
@@ -615,13 +618,13 @@ __device__ bool trace_ray
     }
     if(nnext == 2) {
       const int nearer = te[0] <= te[1] ? 0 : 1;
-      if(sp < STACK_SIZE) stack[sp++] = N.child[1 - nearer];
+      if(sp < STACK_SIZE) stack[(sp++) * stride] = N.child[1 - nearer];
       node = N.child[nearer];
     } else if(nnext == 1) {
       node = N.child[next[0]];
     } else {
       if(sp == 0) break;
-      node = stack[--sp];
+      node = stack[(--sp) * stride];
     }
   }
   return found;
@@ -651,7 +654,7 @@ __device__ __forceinline__ V3<R> local_to(V3<R> n, R x, R y, R z)
 
 /* Returns false on an inconsistent medium (RES_BAD_OP) */
 template<class R>
-__device__ bool shade
+__device__ __noinline__ bool shade
   (const DScene<R>& S, const Rng& rng, uint32_t scatter, int mtl_idx,
    int medium, double wl, V3<R> wo, V3<R> N, R& prop, V3<R>& out,
    int& type, int& next_medium)
@@ -765,42 +768,23 @@ __device__ bool shade
 }
 
 /*******************************************************************************
- * Per path tallies
+ * Realisation state machine
+ *
+ * Each warp iteration casts exactly one ray per active lane, from a single
+ * call site: the shadow ray of a new path (any hit) or the next segment of a
+ * path (closest hit). Around it, lanes regenerate (fetch a new realisation
+ * through a warp-aggregated atomic counter), interact with the surface they
+ * reached, or commit a finished path. Lanes never wait for the longest path
+ * of their warp, and lanes in different phases still trace together.
  ******************************************************************************/
-constexpr int MAX_RCV_ENTRIES = 4;
-constexpr int MAX_PRIM_ENTRIES = 4;
-
-struct PathTally {
-  int nrcv, nprim;
-  int rcv_slot[MAX_RCV_ENTRIES];
-  double rcv[MAX_RCV_ENTRIES][6];
-  int prim_slot[MAX_PRIM_ENTRIES];
-  double prim[MAX_PRIM_ENTRIES][6];
-  bool overflow;
-
-  __device__ void add(int rslot, int pslot, const double v[6])
-  {
-    int k = 0;
-    while(k < nrcv && rcv_slot[k] != rslot) ++k;
-    if(k == nrcv) {
-      if(nrcv == MAX_RCV_ENTRIES) { overflow = true; return; }
-      rcv_slot[nrcv] = rslot;
-      for(int q = 0; q < 6; ++q) rcv[nrcv][q] = 0;
-      ++nrcv;
-    }
-    for(int q = 0; q < 6; ++q) rcv[k][q] += v[q];
-    if(pslot < 0) return;
-    k = 0;
-    while(k < nprim && prim_slot[k] != pslot) ++k;
-    if(k == nprim) {
-      if(nprim == MAX_PRIM_ENTRIES) { overflow = true; return; }
-      prim_slot[nprim] = pslot;
-      for(int q = 0; q < 6; ++q) prim[nprim][q] = 0;
-      ++nprim;
-    }
-    for(int q = 0; q < 6; ++q) prim[k][q] += v[q];
-  }
+enum : int { PH_NONE = 0, PH_SHADOW = 1, PH_BOUNCE = 2 };
+enum : int {
+  END_NONE = 0, END_SHADOW, END_MISS, END_ZERO, END_KILL, END_FAIL
 };
+
+/* Extra (receiver side, primitive) entries of one path beyond the first,
+ * kept in local memory: only paths reaching several receivers touch them */
+constexpr int MAX_EXTRA = 7;
 
 /* 10 receiver quantities from the 6 accumulated ones, in MC_RECEIVER_DATA
  * order (src/ssol_solver.c:735-755) */
@@ -824,23 +808,49 @@ __device__ __forceinline__ void red_add(double* p, double v)
   if(v != 0.0) atomicAdd(p, v);
 }
 
-/*******************************************************************************
- * The realisation (src/ssol_solver.c:873-1127)
- ******************************************************************************/
-enum PathStatus { PATH_OK = 0, PATH_KILLED = 1, PATH_FAILED = 2 };
+__device__ __noinline__ void commit10(double* dst, const double v[6], double f)
+{
+  double q[NRCV_Q];
+  expand10(v, f, q);
+#pragma unroll 1
+  for(int k = 0; k < NRCV_Q; ++k) {
+    red_add(dst + 2 * k, q[k]);
+    red_add(dst + 2 * k + 1, q[k] * q[k]);
+  }
+}
 
-template<class R> struct ThreadAcc {
-  double sum[NGLOBAL];
-  double sq[NGLOBAL];
+template<class R> struct PathState {
+  int phase;
+  int samp;
+  /* current point / ray: the point is org (+ rd t after a hit) */
+  int sinst, side, prim, gid, medium, out_medium;
+  V3<R> N, org, rd;
+  R tmin, hit_t;
+  double wl;
+  /* weights (FP64) */
+  double prev[3];
+  double inc0;
+  bool virt;
+  /* counters */
+  uint32_t depth, interval, scatter, nroul, segments;
+  int score;
+  /* receiver entries: the first one's values live in shared memory */
+  int nent;
+  int r0, p0;
+  bool overflow;
 };
 
+/* Per-thread FP64 path sums kept in shared memory (column `tid`, stride
+ * blockDim): the first receiver entry's 6 values, the 3 global quantities
+ * accumulated along the path and the cosine factor */
+enum : int { PS_V0 = 0, PS_ABS = 6, PS_ATM = 7, PS_OTHER = 8, PS_COS = 9,
+             PS_COUNT = 10 };
+
+/* point_init (src/ssol_solver.c:207-352) up to the shadow ray */
 template<class R>
-__device__ void trace_realisation
-  (const DScene<R>& S, const DTallies& T, const Rng& rng,
-   ThreadAcc<R>& acc, double* smem_rcv, Counters& cnt, uint32_t& bounces,
-   unsigned long long max_segments)
+__device__ __noinline__ void init_path
+  (const DScene<R>& S, const Rng& rng, PathState<R>& p, double* ps, int stride)
 {
-  /* ---- point_init (src/ssol_solver.c:207-358) ---- */
   const U32x4 r0 = rng.get(0u, RNG_PRIMARY);
   /* bucket = floor(u * n) computed exactly on the 24-bit integer draw */
   int k = (int)(((unsigned long long)(r0.v[0] >> 8)
@@ -854,13 +864,10 @@ __device__ void trace_realisation
   const V3<R> nproxy = ld3(st.n);
 
   const U32x4 r1 = rng.get(1u, RNG_PRIMARY);
-  V3<R> dir = sample_sun_dir(S, rng, r1);
-  const double wl = sample_wavelength(S, u01d(r1.v[2]));
+  const V3<R> dir = sample_sun_dir(S, rng, r1);
+  p.wl = sample_wavelength(S, u01d(r1.v[2]));
 
-  int sinst = st.sinst;
-  DShadedInst si = S.sinsts[sinst];
-  int prim = st.prim;
-  int gid = st.gid;
+  const DShadedInst si = S.sinsts[st.sinst];
   V3<R> N = nproxy;
   if(si.is_punched) {
     /* punched_shape_project_point (src/ssol_shape.c:1408-1447) */
@@ -880,198 +887,211 @@ __device__ void trace_realisation
   const R surface_proxy_cos = si.is_punched ? fabs(dot(nproxy, N)) : R(1);
   const R cos_ratio = fabs(surface_sun_cos / (surface_proxy_cos * sun0_sun_cos));
   const double w0 = S.dni * S.area_proxy * (double)cos_ratio;
-  const double cos_factor = S.area_proxy / S.area_rt
+  ps[PS_COS * stride] = S.area_proxy / S.area_rt
     * (double)surface_sun0_cos / (double)surface_proxy_cos;
-  const int samp_idx = si.sampled;
+  ps[PS_ABS * stride] = ps[PS_ATM * stride] = ps[PS_OTHER * stride] = 0;
+  p.samp = si.sampled;
 
-  int mtl = si.mtl[side - 1];
-  const int mtype0 = S.mtls[mtl].type;
-  int medium = S.air_medium;
-  if(mtype0 == MTL_DIELECTRIC || mtype0 == MTL_THIN_DIELECTRIC) {
-    medium = side == 1 ? S.mtls[mtl].in_medium : S.mtls[mtl].out_medium;
-  }
+  const DMaterial m = S.mtls[si.mtl[side - 1]];
+  p.medium = S.air_medium;
+  if(m.type == MTL_DIELECTRIC || m.type == MTL_THIN_DIELECTRIC)
+    p.medium = side == 1 ? m.in_medium : m.out_medium;
 
-  double g[NGLOBAL] = {0, 0, 0, 0, 0, 0};
-  double samp_shadow = 0;
-  PathTally pt;
-  pt.nrcv = pt.nprim = 0;
-  pt.overflow = false;
-  int status = PATH_OK;
-  int score = 0;
-
+  p.sinst = st.sinst;
+  p.side = side;
+  p.prim = st.prim;
+  p.gid = st.gid;
+  p.N = N;
+  p.hit_t = R(0);
+  p.prev[0] = p.prev[1] = p.prev[2] = w0;
+  p.inc0 = 0;
+  p.virt = false;
+  p.depth = p.scatter = p.nroul = p.segments = 0;
+  p.interval = 64;
+  p.score = 0;
+  p.nent = 0;
+  p.overflow = false;
   /* Shadow ray toward the sun (src/ssol_solver.c:320-352) */
-  SelfInfo self;
-  self.gid = gid;
-  self.sinst = sinst;
-  self.side = side;
-  self.discard_virtual = true;
-  self.reversed = true;
-  Hit<R> h;
-  const bool occluded = trace_ray<R, true>(S, pos, -dir, R(0), self, h, cnt);
+  p.org = pos;
+  p.rd = -dir;
+  p.tmin = R(0);
+  p.phase = PH_SHADOW;
+}
 
-  if(occluded) {
-    g[G_SHADOW] = w0;
-    samp_shadow = w0;
-  } else {
-    double prev[3] = {w0, w0, w0};
-    double inc[3], out[3];
-    R hit_t = R(0);
-    R tmin = R(0);
-    V3<R> org = pos, rd = dir;
-    uint32_t depth = 0, roulette_interval = 64;
-    uint32_t scatter = 0, nroulette = 0;
-    unsigned long long segments = 0;
-    for(;;) {
-      const bool in_atm = medium == S.air_medium;
-      const bool hit_receiver = (si.receiver_mask & side) != 0;
-      const bool hit_virtual = (si.virtual_mask & side) != 0;
-      double trans = 1;
-      if(hit_t > R(0)) {
-        const double kext = data_value(S, S.media[medium].extinction, wl);
-        if(kext > 0) trans = (double)ex((R)(-kext * (double)hit_t));
-      }
-      inc[0] = prev[0] * trans;
-      inc[1] = in_atm ? prev[1] : prev[1] * trans;
-      inc[2] = !in_atm ? prev[2] : prev[2] * trans;
-
-      double kabs;
-      int out_medium = medium;
-      if(hit_virtual) {
-        kabs = 0;
-        out[0] = inc[0]; out[1] = inc[1]; out[2] = inc[2];
-      } else {
-        R prop;
-        V3<R> ndir;
-        int type;
-        ++bounces;
-        if(!shade(S, rng, scatter++, mtl, medium, wl, -dir, N, prop, ndir,
-                  type, out_medium)) {
-          status = PATH_FAILED;
-          break;
-        }
-        const double p = (double)prop;
-        kabs = 1.0 - p;
-        out[0] = inc[0] * p;
-        out[1] = inc[1] * p;
-        out[2] = hit_receiver ? inc[2] * p : inc[2];
-        if(type) dir = ndir;
-      }
-
-      if(hit_receiver) {
-        const int si_side = side - 1;
-        const double v[6] = {inc[0], inc[1], inc[2],
-                             inc[0] * kabs, inc[1] * kabs, inc[2] * kabs};
-        const int pslot = si.prim_base[si_side] >= 0
-          ? si.prim_base[si_side] + prim : -1;
-        pt.add(si.rcv_slot[si_side], pslot, v);
-        g[G_ABS_RCV] += inc[0] - out[0];
-      } else {
-        g[G_OTHER] += inc[0] * kabs;
-      }
-
-      const bool weight_zero = out[0] == 0.0;
-      bool last = false;
-      if(!weight_zero) {
-        if(hit_virtual) {
-          tmin = nxt(hit_t);
-        } else {
-          tmin = R(0);
-          org = pos;
-          rd = dir;
-        }
-        self.gid = gid;
-        self.sinst = sinst;
-        self.side = side;
-        self.discard_virtual = false;
-        self.reversed = false;
-        if(!trace_ray<R, false>(S, org, rd, tmin, self, h, cnt)) {
-          last = true;
-          if(out_medium != S.air_medium) { status = PATH_FAILED; break; }
-        }
-      }
-      if(weight_zero || last || !hit_virtual) {
-        const double absorbed = prev[0] - inc[0];
-        if(in_atm) g[G_ATM] += absorbed; else g[G_OTHER] += absorbed;
-        if(weight_zero || last) break;
-        prev[0] = out[0]; prev[1] = out[1]; prev[2] = out[2];
-      }
-      depth += hit_virtual ? 0u : 1u;
-      if(depth > roulette_interval && depth % roulette_interval == 1) {
-        const double p = u01d(rng.get(nroulette++, RNG_ROULETTE).v[0]);
-        if(p > 0.5) {
-          ++score;
-          roulette_interval = 16;
-        } else {
-          status = PATH_KILLED;
-          break;
-        }
-      }
-      if(++segments >= max_segments) { status = PATH_FAILED; break; }
-
-      /* point_update_from_hit (src/ssol_solver.c:360-411) */
-      sinst = h.sinst;
-      si = S.sinsts[sinst];
-      prim = h.prim;
-      gid = h.gid;
-      N = normalize(h.n);
-      pos = org + rd * h.t;
-      side = dot(rd, N) < R(0) ? 1 : 2;
-      if(side == 2) N = -N;
-      mtl = si.mtl[side - 1];
-      hit_t = h.t;
-      medium = out_medium;
-    }
-    if(status == PATH_OK) g[G_MISSING] += out[0];
-  }
-  if(status == PATH_OK) g[G_COS] += cos_factor;
-  if(pt.overflow) status = PATH_FAILED;
-
-  /* ---- commit ---- */
-  atomicAdd(&T.nb_samples[samp_idx], 1ull);
-  if(status == PATH_FAILED) {
-    atomicAdd(&T.counters[0], 1ull);
-    if(pt.overflow) atomicAdd(&T.counters[2], 1ull);
+template<class R>
+__device__ __forceinline__ void add_entry
+  (PathState<R>& p, int rslot, int pslot, const double v[6], double* ps,
+   int stride, int* xr, int* xp, double (*xv)[6])
+{
+  if(p.nent == 0) {
+    p.nent = 1;
+    p.r0 = rslot;
+    p.p0 = pslot;
+    for(int q = 0; q < 6; ++q) ps[(PS_V0 + q) * stride] = v[q];
     return;
   }
-  if(status == PATH_KILLED) {
+  if(p.r0 == rslot && p.p0 == pslot) {
+    for(int q = 0; q < 6; ++q) ps[(PS_V0 + q) * stride] += v[q];
+    return;
+  }
+  for(int e = 0; e < p.nent - 1; ++e) {
+    if(xr[e] == rslot && xp[e] == pslot) {
+      for(int q = 0; q < 6; ++q) xv[e][q] += v[q];
+      return;
+    }
+  }
+  if(p.nent - 1 >= MAX_EXTRA) { p.overflow = true; return; }
+  const int e = p.nent - 1;
+  xr[e] = rslot;
+  xp[e] = pslot;
+  for(int q = 0; q < 6; ++q) xv[e][q] = v[q];
+  ++p.nent;
+}
+
+/* One surface interaction (src/ssol_solver.c:939-1011): extinction of the
+ * incoming segment, virtual pass-through or BSDF sample, receiver tallies,
+ * then either the next ray or the end of the path */
+template<class R>
+__device__ int interact
+  (const DScene<R>& S, const Rng& rng, PathState<R>& p, V3<R> pos, V3<R> dir,
+   uint32_t& bounces, unsigned long long max_segments, double* ps, int stride,
+   int* xr, int* xp, double (*xv)[6])
+{
+  const DShadedInst si = S.sinsts[p.sinst];
+  const bool in_atm = p.medium == S.air_medium;
+  const bool hit_receiver = (si.receiver_mask & p.side) != 0;
+  const bool hit_virtual = (si.virtual_mask & p.side) != 0;
+  double trans = 1;
+  if(p.hit_t > R(0)) {
+    const double kext = data_value(S, S.media[p.medium].extinction, p.wl);
+    if(kext > 0) trans = (double)ex((R)(-kext * (double)p.hit_t));
+  }
+  const double inc0 = p.prev[0] * trans;
+  const double inc1 = in_atm ? p.prev[1] : p.prev[1] * trans;
+  const double inc2 = !in_atm ? p.prev[2] : p.prev[2] * trans;
+  double out0, out1, out2, kabs;
+  int out_medium = p.medium;
+  if(hit_virtual) {
+    kabs = 0;
+    out0 = inc0; out1 = inc1; out2 = inc2;
+  } else {
+    R prop;
+    V3<R> ndir;
+    int type;
+    ++bounces;
+    if(!shade(S, rng, p.scatter++, si.mtl[p.side - 1], p.medium, p.wl, -dir,
+              p.N, prop, ndir, type, out_medium))
+      return END_FAIL;
+    const double pr = (double)prop;
+    kabs = 1.0 - pr;
+    out0 = inc0 * pr;
+    out1 = inc1 * pr;
+    out2 = hit_receiver ? inc2 * pr : inc2;
+    if(type) dir = ndir;
+  }
+  if(hit_receiver) {
+    const int s = p.side - 1;
+    const double v[6] = {inc0, inc1, inc2, inc0 * kabs, inc1 * kabs, inc2 * kabs};
+    const int pslot = si.prim_base[s] >= 0 ? si.prim_base[s] + p.prim : -1;
+    add_entry(p, si.rcv_slot[s], pslot, v, ps, stride, xr, xp, xv);
+    ps[PS_ABS * stride] += inc0 - out0;
+  } else {
+    ps[PS_OTHER * stride] += inc0 * kabs;
+  }
+  /* Loss along the incoming segment, accounted at non-virtual points or at
+   * the end of the path (src/ssol_solver.c:1036-1054) */
+  const double seg_loss = p.prev[0] - inc0;
+  if(out0 == 0.0 || !hit_virtual)
+    ps[(in_atm ? PS_ATM : PS_OTHER) * stride] += seg_loss;
+  if(out0 == 0.0) return END_ZERO;
+  if(!hit_virtual) {
+    p.prev[0] = out0; p.prev[1] = out1; p.prev[2] = out2;
+    p.org = pos;
+    p.rd = dir;
+    p.tmin = R(0);
+  } else {
+    /* Virtual: pursue the same ray beyond the hit (src/ssol_solver.c:988-995) */
+    p.inc0 = inc0;
+    p.tmin = nxt(p.hit_t);
+  }
+  p.virt = hit_virtual;
+  p.out_medium = out_medium;
+  if(++p.segments >= max_segments) return END_FAIL;
+  p.phase = PH_BOUNCE;
+  return END_NONE;
+}
+
+/* Commit a finished path: FP64 (w, w^2) of its totals, x 2^score for
+ * roulette survivors (src/ssol_solver.c:1087-1108) */
+template<class R>
+__device__ __noinline__ void commit_path
+  (const DScene<R>& S, const DTallies& T, PathState<R>& p, int end,
+   double* acc, double* ps, int stride, double* smem_rcv, const int* xr,
+   const int* xp, const double (*xv)[6])
+{
+  atomicAdd(&T.nb_samples[p.samp], 1ull);
+  if(p.overflow) end = END_FAIL;
+  if(end == END_FAIL) {
+    atomicAdd(&T.counters[0], 1ull);
+    if(p.overflow) atomicAdd(&T.counters[2], 1ull);
+    return;
+  }
+  if(end == END_KILL) {
     atomicAdd(&T.counters[1], 1ull);
     return;
   }
-  const double f = (double)(1ull << score);
+  const double f = (double)(1ull << p.score);
+  double g[NGLOBAL];
+  g[G_COS] = ps[PS_COS * stride];
+  g[G_ABS_RCV] = ps[PS_ABS * stride];
+  g[G_SHADOW] = end == END_SHADOW ? p.prev[0] : 0.0;
+  g[G_MISSING] = end == END_MISS ? (p.virt ? p.inc0 : p.prev[0]) : 0.0;
+  g[G_ATM] = ps[PS_ATM * stride];
+  g[G_OTHER] = ps[PS_OTHER * stride];
+#pragma unroll
   for(int q = 0; q < NGLOBAL; ++q) {
     const double w = f * g[q];
-    acc.sum[q] += w;
-    acc.sq[q] += w * w;
+    acc[(2 * q) * stride] += w;
+    acc[(2 * q + 1) * stride] += w * w;
   }
   {
-    const double wc = f * cos_factor, ws = f * samp_shadow;
-    double* sp = T.samp + (size_t)samp_idx * 4;
+    const double wc = f * g[G_COS], ws = f * g[G_SHADOW];
+    double* sp = T.samp + (size_t)p.samp * 4;
     red_add(sp + 0, wc);
     red_add(sp + 1, wc * wc);
     red_add(sp + 2, ws);
     red_add(sp + 3, ws * ws);
   }
-  for(int e = 0; e < pt.nrcv; ++e) {
-    double v10[NRCV_Q];
-    expand10(pt.rcv[e], f, v10);
-    const int r = pt.rcv_slot[e];
-    double* dst = smem_rcv ? smem_rcv + (size_t)r * NRCV_Q * 2
-                           : T.rcv + (size_t)r * NRCV_Q * 2;
-    double* dsr = T.samp_rcv + ((size_t)samp_idx * S.nrcv + r) * NRCV_Q * 2;
-    for(int q = 0; q < NRCV_Q; ++q) {
-      red_add(dst + 2 * q, v10[q]);
-      red_add(dst + 2 * q + 1, v10[q] * v10[q]);
-      red_add(dsr + 2 * q, v10[q]);
-      red_add(dsr + 2 * q + 1, v10[q] * v10[q]);
-    }
+  if(p.nent == 0) return;
+  double v0[6];
+  for(int q = 0; q < 6; ++q) v0[q] = ps[(PS_V0 + q) * stride];
+  double* rbase = smem_rcv ? smem_rcv : T.rcv;
+  if(p.nent == 1) {
+    commit10(rbase + (size_t)p.r0 * NRCV_Q * 2, v0, f);
+    commit10(T.samp_rcv + ((size_t)p.samp * S.nrcv + p.r0) * NRCV_Q * 2, v0, f);
+    if(p.p0 >= 0) commit10(T.prim + (size_t)p.p0 * NRCV_Q * 2, v0, f);
+    return;
   }
-  for(int e = 0; e < pt.nprim; ++e) {
-    double v10[NRCV_Q];
-    expand10(pt.prim[e], f, v10);
-    double* dst = T.prim + (size_t)pt.prim_slot[e] * NRCV_Q * 2;
-    for(int q = 0; q < NRCV_Q; ++q) {
-      red_add(dst + 2 * q, v10[q]);
-      red_add(dst + 2 * q + 1, v10[q] * v10[q]);
+  /* Several entries: sum per receiver side and per primitive before
+   * squaring (deferred mc_data semantics) */
+  const int n = p.nent;
+  for(int e = 0; e < n; ++e) {
+    const int re = e == 0 ? p.r0 : xr[e - 1];
+    bool seen = false;
+    for(int k = 0; k < e && !seen; ++k) seen = (k == 0 ? p.r0 : xr[k - 1]) == re;
+    if(!seen) {
+      double v[6] = {0, 0, 0, 0, 0, 0};
+      for(int k = e; k < n; ++k) {
+        if((k == 0 ? p.r0 : xr[k - 1]) != re) continue;
+        for(int q = 0; q < 6; ++q) v[q] += k == 0 ? v0[q] : xv[k - 1][q];
+      }
+      commit10(rbase + (size_t)re * NRCV_Q * 2, v, f);
+      commit10(T.samp_rcv + ((size_t)p.samp * S.nrcv + re) * NRCV_Q * 2, v, f);
+    }
+    const int pe = e == 0 ? p.p0 : xp[e - 1];
+    if(pe >= 0) {
+      /* (receiver side, primitive) keys are unique among the entries */
+      commit10(T.prim + (size_t)pe * NRCV_Q * 2, e == 0 ? v0 : xv[e - 1], f);
     }
   }
 }
@@ -1093,72 +1113,164 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 }
 
 constexpr int SMEM_RCV_MAX = 16;
+constexpr int MAX_BLOCK = 256;
 
-template<class R>
-__global__ void __launch_bounds__(256)
+template<class R, int MINB>
+__global__ void __launch_bounds__(MAX_BLOCK, MINB)
 realisation_kernel
   (const DScene<R> S, const DTallies T, uint64_t seed, uint64_t first,
-   uint64_t count, unsigned long long max_segments)
+   uint64_t count, unsigned long long max_segments,
+   unsigned long long* next_path)
 {
+  /* Shared memory: per-thread FP64 global sums [12][blockDim], per-thread
+   * path sums [10][blockDim], the receiver-side sums, the per-thread
+   * traversal stacks [32][blockDim] */
   extern __shared__ double smem[];
-  __shared__ double red[32][2 * NGLOBAL];
-  const bool use_smem = S.nrcv <= SMEM_RCV_MAX;
-  double* smem_rcv = use_smem ? smem : nullptr;
-  if(use_smem) {
-    for(int i = threadIdx.x; i < S.nrcv * NRCV_Q * 2; i += blockDim.x)
-      smem_rcv[i] = 0;
-  }
+  __shared__ double red[MAX_BLOCK / 32][2 * NGLOBAL];
+  const int bd = blockDim.x, tid = threadIdx.x;
+  const unsigned lane = tid & 31u;
+  const bool use_smem_rcv = S.nrcv <= SMEM_RCV_MAX;
+  double* acc = smem + tid;
+  double* ps = smem + 2 * NGLOBAL * bd + tid;
+  double* smem_rcv = use_smem_rcv ? smem + (2 * NGLOBAL + PS_COUNT) * bd : nullptr;
+  const int rcv_doubles = use_smem_rcv ? S.nrcv * NRCV_Q * 2 : 0;
+  int* stack = reinterpret_cast<int*>(smem + (2 * NGLOBAL + PS_COUNT) * bd
+                                      + rcv_doubles) + tid;
+  for(int q = 0; q < 2 * NGLOBAL; ++q) acc[q * bd] = 0;
+  for(int i = tid; i < rcv_doubles; i += bd) smem_rcv[i] = 0;
   __syncthreads();
 
-  ThreadAcc<R> acc;
-  for(int q = 0; q < NGLOBAL; ++q) acc.sum[q] = acc.sq[q] = 0;
-  Counters cnt = {0, 0, 0, 0};
-  uint32_t bounces = 0, paths = 0;
-
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   Rng rng;
   rng.k0 = (uint32_t)seed;
   rng.k1 = (uint32_t)(seed >> 32);
-  for(uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
-      i += stride) {
-    const uint64_t id = first + i;
-    rng.i_lo = (uint32_t)id;
-    rng.i_hi = (uint32_t)(id >> 32);
-    trace_realisation(S, T, rng, acc, smem_rcv, cnt, bounces, max_segments);
-    ++paths;
+  PathState<R> p;
+  p.phase = PH_NONE;
+  bool done = false;
+  Counters cnt = {0, 0, 0, 0};
+  uint32_t bounces = 0, npaths = 0;
+  int xr[MAX_EXTRA], xp[MAX_EXTRA];
+  double xv[MAX_EXTRA][6];
+
+  for(;;) {
+    /* Regeneration: idle lanes take the next realisations */
+    const unsigned need = __ballot_sync(0xffffffffu, p.phase == PH_NONE && !done);
+    if(need) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if((int)lane == leader)
+        base = atomicAdd(next_path, (unsigned long long)__popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if(p.phase == PH_NONE && !done) {
+        const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
+        if(idx >= count) {
+          done = true;
+        } else {
+          const uint64_t id = first + idx;
+          rng.i_lo = (uint32_t)id;
+          rng.i_hi = (uint32_t)(id >> 32);
+          init_path(S, rng, p, ps, bd);
+          ++npaths;
+        }
+      }
+    }
+    if(!__any_sync(0xffffffffu, p.phase != PH_NONE)) break;
+
+    /* One ray per active lane */
+    Hit<R> h;
+    bool found = false;
+    if(p.phase != PH_NONE) {
+      const bool shadow = p.phase == PH_SHADOW;
+      SelfInfo self;
+      self.gid = p.gid;
+      self.sinst = p.sinst;
+      self.side = p.side;
+      self.discard_virtual = shadow;
+      self.reversed = shadow;
+      found = trace_ray(S, p.org, p.rd, p.tmin, self, shadow, h, cnt, stack, bd);
+    }
+
+    int end = END_NONE;
+    bool do_interact = false;
+    V3<R> pos = p.org, dir = -p.rd;
+    if(p.phase == PH_SHADOW) {
+      if(found) end = END_SHADOW;
+      else do_interact = true;
+    } else if(p.phase == PH_BOUNCE) {
+      if(!found) {
+        /* Last segment: the medium the ray leaves into must be the air
+         * (src/ssol_solver.c:1012-1032) */
+        if(p.out_medium != S.air_medium) {
+          end = END_FAIL;
+        } else {
+          if(p.virt) {
+            const double loss = p.prev[0] - p.inc0;
+            ps[(p.medium == S.air_medium ? PS_ATM : PS_OTHER) * bd] += loss;
+          }
+          end = END_MISS;
+        }
+      } else {
+        /* Russian roulette on deep paths (src/ssol_solver.c:1056-1075) */
+        p.depth += p.virt ? 0u : 1u;
+        if(p.depth > p.interval && p.depth % p.interval == 1) {
+          const double u = u01d(rng.get(p.nroul++, RNG_ROULETTE).v[0]);
+          if(u > 0.5) {
+            ++p.score;
+            p.interval = 16;
+          } else {
+            end = END_KILL;
+          }
+        }
+        if(end == END_NONE) {
+          /* point_update_from_hit (src/ssol_solver.c:360-411) */
+          p.sinst = h.sinst;
+          p.prim = h.prim;
+          p.gid = h.gid;
+          dir = p.rd;
+          p.N = normalize(h.n);
+          pos = p.org + p.rd * h.t;
+          p.side = dot(p.rd, p.N) < R(0) ? 1 : 2;
+          if(p.side == 2) p.N = -p.N;
+          p.hit_t = h.t;
+          p.medium = p.out_medium;
+          do_interact = true;
+        }
+      }
+    }
+    if(do_interact)
+      end = interact(S, rng, p, pos, dir, bounces, max_segments, ps, bd, xr, xp, xv);
+    if(end != END_NONE) {
+      commit_path(S, T, p, end, acc, ps, bd, smem_rcv, xr, xp, xv);
+      p.phase = PH_NONE;
+    }
   }
 
   /* Warp then block reduction of the global sums, one commit per block */
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for(int q = 0; q < NGLOBAL; ++q) {
-    const double s = warp_sum(acc.sum[q]);
-    const double s2 = warp_sum(acc.sq[q]);
-    if(lane == 0) { red[warp][2 * q] = s; red[warp][2 * q + 1] = s2; }
+  const int warp = tid >> 5;
+  for(int q = 0; q < 2 * NGLOBAL; ++q) {
+    const double s = warp_sum(acc[q * bd]);
+    if(lane == 0) red[warp][q] = s;
   }
   unsigned long long c[6] = {cnt.rays, cnt.nodes, cnt.tris, cnt.quads,
-                             bounces, paths};
+                             bounces, npaths};
   for(int q = 0; q < 6; ++q) c[q] = warp_sum_u64(c[q]);
   if(lane == 0) {
     unsigned long long* st = &T.stats->rays;
     for(int q = 0; q < 6; ++q) if(c[q]) atomicAdd(st + q, c[q]);
   }
   __syncthreads();
-  if(threadIdx.x < 2 * NGLOBAL) {
+  if(tid < 2 * NGLOBAL) {
     double v = 0;
-    for(int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
-    red_add(T.global + threadIdx.x, v);
+    for(int w = 0; w < (bd >> 5); ++w) v += red[w][tid];
+    red_add(T.global + tid, v);
   }
-  if(use_smem) {
-    for(int i = threadIdx.x; i < S.nrcv * NRCV_Q * 2; i += blockDim.x)
-      red_add(T.rcv + i, smem_rcv[i]);
-  }
+  for(int i = tid; i < rcv_doubles; i += bd) red_add(T.rcv + i, smem_rcv[i]);
 }
 
 /*******************************************************************************
  * Host launchers
  ******************************************************************************/
-template<class R>
-static int launch_impl
+template<class R, int MINB>
+static int launch_variant
   (const DScene<R>& S, const DTallies& T, uint64_t seed, uint64_t first,
    uint64_t count, const LaunchConfig& cfg, void* stream)
 {
@@ -1166,12 +1278,21 @@ static int launch_impl
   cudaGetDevice(&dev);
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int block = cfg.block_size > 0 ? cfg.block_size : 256;
-  const size_t smem = S.nrcv <= SMEM_RCV_MAX
-    ? (size_t)S.nrcv * NRCV_Q * 2 * sizeof(double) : 0;
+  const int block = cfg.block_size > 0 ? cfg.block_size : MAX_BLOCK;
+  if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
+  const int rcv_doubles = S.nrcv <= SMEM_RCV_MAX ? S.nrcv * NRCV_Q * 2 : 0;
+  const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block + rcv_doubles)
+                      * sizeof(double)
+                    + (size_t)STACK_SIZE * block * sizeof(int);
+  static bool attr_set = false;
+  if(!attr_set) {
+    cudaFuncSetAttribute(realisation_kernel<R, MINB>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    attr_set = true;
+  }
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor
-    (&per_sm, realisation_kernel<R>, block, smem);
+    (&per_sm, realisation_kernel<R, MINB>, block, smem);
   if(per_sm < 1) per_sm = 1;
   uint64_t blocks = cfg.grid_blocks > 0
     ? (uint64_t)cfg.grid_blocks
@@ -1179,10 +1300,26 @@ static int launch_impl
   const uint64_t needed = (count + block - 1) / block;
   if(blocks > needed) blocks = needed;
   if(blocks < 1) blocks = 1;
-  realisation_kernel<R><<<(unsigned)blocks, block, smem,
-                          (cudaStream_t)stream>>>
-    (S, T, seed, first, count, cfg.max_segments);
+  /* Work counter of this launch: counters[3] */
+  cudaMemsetAsync(T.counters + 3, 0, sizeof(unsigned long long),
+                  (cudaStream_t)stream);
+  realisation_kernel<R, MINB><<<(unsigned)blocks, block, smem,
+                                (cudaStream_t)stream>>>
+    (S, T, seed, first, count, cfg.max_segments, T.counters + 3);
   return (int)cudaGetLastError();
+}
+
+/* Register budget variants: at least MINB blocks of 256 threads per SM */
+template<class R>
+static int launch_impl
+  (const DScene<R>& S, const DTallies& T, uint64_t seed, uint64_t first,
+   uint64_t count, const LaunchConfig& cfg, void* stream)
+{
+  switch(cfg.min_blocks) {
+    case 1: return launch_variant<R, 1>(S, T, seed, first, count, cfg, stream);
+    case 3: return launch_variant<R, 3>(S, T, seed, first, count, cfg, stream);
+    default: return launch_variant<R, 2>(S, T, seed, first, count, cfg, stream);
+  }
 }
 
 int launch_realisations_f32

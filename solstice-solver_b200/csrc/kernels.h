@@ -15,6 +15,7 @@ struct LaunchConfig {
   int grid_blocks; /* 0 => SMs x resident blocks x waves */
   int waves; /* persistent grid multiplier, 0 => 1 */
   unsigned long long max_segments; /* per path segment budget */
+  int min_blocks; /* register budget: 1 (255 regs), 2 (128) or 3 (85) */
 };
 
 /* Enqueue the realisations [first, first + count) of the stream keyed by

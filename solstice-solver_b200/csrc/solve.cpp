@@ -145,6 +145,8 @@ static bool validate(const FlatScene<R>& f)
   const int64_t nnodes = (int64_t)f.nodes.size();
   const int64_t nrefs = (int64_t)f.bvh.primrefs.size();
   if(nnodes < 1) return false;
+  /* the traversal defers at most depth - 1 nodes on its 32-entry stack */
+  if(f.bvh.depth > 30) return false;
   for(const DNode<R>& n : f.nodes) {
     for(int k = 0; k < 2; ++k) {
       if(n.count[k] == 0) {
@@ -283,8 +285,10 @@ extern "C" res_T ssol_b200_plan_create
     return RES_BAD_ARG;
   if(opt.block_size == 0) opt.block_size = 256;
   if(opt.block_size % 32) return RES_BAD_ARG;
-  if(opt.bvh_leaf_size == 0) opt.bvh_leaf_size = 4;
+  if(opt.bvh_leaf_size == 0) opt.bvh_leaf_size = 1;
   if(opt.max_segments == 0) opt.max_segments = 1000000ull;
+  if(opt.min_blocks_per_sm < 0 || opt.min_blocks_per_sm > 3) return RES_BAD_ARG;
+  if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = 2;
 
   BvhBuildParams bp;
   bp.max_leaf = opt.bvh_leaf_size;
@@ -391,6 +395,7 @@ extern "C" res_T ssol_b200_plan_launch
   cfg.grid_blocks = p->opt.grid_blocks;
   cfg.waves = p->opt.waves;
   cfg.max_segments = p->opt.max_segments;
+  cfg.min_blocks = p->opt.min_blocks_per_sm;
   const uint64_t start = rng->position + first;
   cudaEventRecord(p->ev0, s);
   const int err = p->opt.precision == SSOL_B200_FP32

@@ -139,7 +139,7 @@ class PunchedSurface(C.Structure):
 class B200Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("block_size", C.c_int), ("grid_blocks", C.c_int),
                 ("waves", C.c_int), ("bvh_leaf_size", C.c_int),
-                ("max_segments", C.c_ulonglong)]
+                ("max_segments", C.c_ulonglong), ("min_blocks_per_sm", C.c_int)]
 
 
 class B200Stats(C.Structure):
@@ -600,8 +600,8 @@ class Scene:
         return Estimator(self, est, res) if est else None
 
 
-def options(precision=FP32, block_size=256, grid_blocks=0, waves=1, leaf=4,
-            max_segments=0):
+def options(precision=FP32, block_size=256, grid_blocks=0, waves=1, leaf=0,
+            max_segments=0, min_blocks=0):
     o = B200Options()
     o.precision = precision
     o.block_size = block_size
@@ -609,6 +609,7 @@ def options(precision=FP32, block_size=256, grid_blocks=0, waves=1, leaf=4,
     o.waves = waves
     o.bvh_leaf_size = leaf
     o.max_segments = max_segments
+    o.min_blocks_per_sm = min_blocks
     return o
 
 
