@@ -95,6 +95,31 @@ SSOL_API res_T ssol_b200_plan_finish
 SSOL_API res_T ssol_b200_plan_get_stats
   (const struct ssol_b200_plan* plan, struct ssol_b200_stats* stats);
 
+/* Batches: several scenes (typically one per sun position, each with its own
+ * re-aimed field and sun) traced by one persistent kernel launch replayed
+ * from a captured CUDA graph, each item with its own budget and tallies */
+struct ssol_b200_batch;
+
+SSOL_API res_T ssol_b200_batch_create
+  (struct ssol_scene* const* scenes, const size_t nscenes,
+   const struct ssol_b200_options* options, struct ssol_b200_batch** batch);
+SSOL_API res_T ssol_b200_batch_ref_get(struct ssol_b200_batch* batch);
+SSOL_API res_T ssol_b200_batch_ref_put(struct ssol_b200_batch* batch);
+/* Zero every item's tallies and realisation counts */
+SSOL_API res_T ssol_b200_batch_reset(struct ssol_b200_batch* batch, void* stream);
+/* One launch: budgets[i] more realisations of item i, continuing its own
+ * stream (realisation ids position + k of `rng`, k counted per item since
+ * the last reset). Returns when the launch has completed. */
+SSOL_API res_T ssol_b200_batch_launch
+  (struct ssol_b200_batch* batch, const struct ssp_rng* rng,
+   const uint64_t* budgets, void* stream);
+/* One estimator per item (nscenes entries), as ssol_solve would return for
+ * the realisations the item received */
+SSOL_API res_T ssol_b200_batch_finish
+  (struct ssol_b200_batch* batch, const struct ssp_rng* rng,
+   const size_t max_failed_count, void* stream,
+   struct ssol_estimator** estimators);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1266,6 +1266,160 @@ realisation_kernel
   for(int i = tid; i < rcv_doubles; i += bd) red_add(T.rcv + i, smem_rcv[i]);
 }
 
+/* Batched form: several scenes (e.g. one re-aimed field per sun position)
+ * and their realisation budgets in one persistent launch. Global work index
+ * g maps to item it = max{i : prefix[i] <= g} and to realisation
+ * firsts[it] + g - prefix[it] of that item's streams. Every item has its own
+ * tallies; the per-thread FP64 global sums are flushed when a thread moves
+ * to another item. The launch's total is prefix[nitems], read from device
+ * memory so that a captured CUDA graph replays with new budgets. */
+template<class R, int MINB>
+__global__ void __launch_bounds__(MAX_BLOCK, MINB)
+batch_kernel
+  (const DScene<R>* __restrict__ scenes, const DTallies* __restrict__ tallies,
+   const unsigned long long* __restrict__ prefix,
+   const unsigned long long* __restrict__ firsts, int nitems, uint64_t seed,
+   unsigned long long max_segments, unsigned long long* next_path,
+   DStats* stats)
+{
+  extern __shared__ double smem[];
+  const int bd = blockDim.x, tid = threadIdx.x;
+  const unsigned lane = tid & 31u;
+  double* acc = smem + tid;
+  double* ps = smem + 2 * NGLOBAL * bd + tid;
+  int* stack = reinterpret_cast<int*>(smem + (2 * NGLOBAL + PS_COUNT) * bd) + tid;
+  for(int q = 0; q < 2 * NGLOBAL; ++q) acc[q * bd] = 0;
+  int acc_item = -1;
+
+  const unsigned long long count = prefix[nitems];
+  Rng rng;
+  rng.k0 = (uint32_t)seed;
+  rng.k1 = (uint32_t)(seed >> 32);
+  PathState<R> p;
+  p.phase = PH_NONE;
+  int it = 0;
+  bool done = false;
+  Counters cnt = {0, 0, 0, 0};
+  uint32_t bounces = 0, npaths = 0;
+  int xr[MAX_EXTRA], xp[MAX_EXTRA];
+  double xv[MAX_EXTRA][6];
+
+  for(;;) {
+    const unsigned need = __ballot_sync(0xffffffffu, p.phase == PH_NONE && !done);
+    if(need) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if((int)lane == leader)
+        base = atomicAdd(next_path, (unsigned long long)__popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if(p.phase == PH_NONE && !done) {
+        const unsigned long long g = base + __popc(need & ((1u << lane) - 1u));
+        if(g >= count) {
+          done = true;
+        } else {
+          int lo = 0, hi = nitems; /* prefix[lo] <= g < prefix[hi] */
+          while(hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if(prefix[mid] <= g) lo = mid; else hi = mid;
+          }
+          it = lo;
+          if(it != acc_item) {
+            if(acc_item >= 0) {
+              for(int q = 0; q < 2 * NGLOBAL; ++q) {
+                red_add(tallies[acc_item].global + q, acc[q * bd]);
+                acc[q * bd] = 0;
+              }
+            }
+            acc_item = it;
+          }
+          const uint64_t id = firsts[it] + (g - prefix[it]);
+          rng.i_lo = (uint32_t)id;
+          rng.i_hi = (uint32_t)(id >> 32);
+          init_path(scenes[it], rng, p, ps, bd);
+          ++npaths;
+        }
+      }
+    }
+    if(!__any_sync(0xffffffffu, p.phase != PH_NONE)) break;
+
+    const DScene<R>& S = scenes[it];
+    Hit<R> h;
+    bool found = false;
+    if(p.phase != PH_NONE) {
+      const bool shadow = p.phase == PH_SHADOW;
+      SelfInfo self;
+      self.gid = p.gid;
+      self.sinst = p.sinst;
+      self.side = p.side;
+      self.discard_virtual = shadow;
+      self.reversed = shadow;
+      found = trace_ray(S, p.org, p.rd, p.tmin, self, shadow, h, cnt, stack, bd);
+    }
+
+    int end = END_NONE;
+    bool do_interact = false;
+    V3<R> pos = p.org, dir = -p.rd;
+    if(p.phase == PH_SHADOW) {
+      if(found) end = END_SHADOW;
+      else do_interact = true;
+    } else if(p.phase == PH_BOUNCE) {
+      if(!found) {
+        if(p.out_medium != S.air_medium) {
+          end = END_FAIL;
+        } else {
+          if(p.virt) {
+            const double loss = p.prev[0] - p.inc0;
+            ps[(p.medium == S.air_medium ? PS_ATM : PS_OTHER) * bd] += loss;
+          }
+          end = END_MISS;
+        }
+      } else {
+        p.depth += p.virt ? 0u : 1u;
+        if(p.depth > p.interval && p.depth % p.interval == 1) {
+          const double u = u01d(rng.get(p.nroul++, RNG_ROULETTE).v[0]);
+          if(u > 0.5) {
+            ++p.score;
+            p.interval = 16;
+          } else {
+            end = END_KILL;
+          }
+        }
+        if(end == END_NONE) {
+          p.sinst = h.sinst;
+          p.prim = h.prim;
+          p.gid = h.gid;
+          dir = p.rd;
+          p.N = normalize(h.n);
+          pos = p.org + p.rd * h.t;
+          p.side = dot(p.rd, p.N) < R(0) ? 1 : 2;
+          if(p.side == 2) p.N = -p.N;
+          p.hit_t = h.t;
+          p.medium = p.out_medium;
+          do_interact = true;
+        }
+      }
+    }
+    if(do_interact)
+      end = interact(S, rng, p, pos, dir, bounces, max_segments, ps, bd, xr, xp, xv);
+    if(end != END_NONE) {
+      commit_path(S, tallies[it], p, end, acc, ps, bd, nullptr, xr, xp, xv);
+      p.phase = PH_NONE;
+    }
+  }
+
+  if(acc_item >= 0) {
+    for(int q = 0; q < 2 * NGLOBAL; ++q)
+      red_add(tallies[acc_item].global + q, acc[q * bd]);
+  }
+  unsigned long long c[6] = {cnt.rays, cnt.nodes, cnt.tris, cnt.quads,
+                             bounces, npaths};
+  for(int q = 0; q < 6; ++q) c[q] = warp_sum_u64(c[q]);
+  if(lane == 0) {
+    unsigned long long* st = &stats->rays;
+    for(int q = 0; q < 6; ++q) if(c[q]) atomicAdd(st + q, c[q]);
+  }
+}
+
 /*******************************************************************************
  * Host launchers
  ******************************************************************************/
@@ -1321,6 +1475,57 @@ static int launch_impl
     default: return launch_variant<R, 2>(S, T, seed, first, count, cfg, stream);
   }
 }
+
+template<class R, int MINB>
+static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg,
+                                void* stream)
+{
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int block = cfg.block_size > 0 ? cfg.block_size : MAX_BLOCK;
+  if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
+  const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block) * sizeof(double)
+                    + (size_t)STACK_SIZE * block * sizeof(int);
+  static bool attr_set = false;
+  if(!attr_set) {
+    cudaFuncSetAttribute(batch_kernel<R, MINB>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    attr_set = true;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor
+    (&per_sm, batch_kernel<R, MINB>, block, smem);
+  if(per_sm < 1) per_sm = 1;
+  const uint64_t blocks = cfg.grid_blocks > 0
+    ? (uint64_t)cfg.grid_blocks
+    : (uint64_t)nsm * (uint64_t)per_sm * (uint64_t)(cfg.waves > 0 ? cfg.waves : 1);
+  cudaMemsetAsync(b.next_path, 0, sizeof(unsigned long long), (cudaStream_t)stream);
+  batch_kernel<R, MINB><<<(unsigned)blocks, block, smem, (cudaStream_t)stream>>>
+    (b.scenes, b.tallies, b.prefix, b.firsts, b.nitems, b.seed, cfg.max_segments,
+     b.next_path, b.stats);
+  return (int)cudaGetLastError();
+}
+
+template<class R>
+static int launch_batch_impl(const BatchLaunch<R>& b, const LaunchConfig& cfg,
+                             void* stream)
+{
+  switch(cfg.min_blocks) {
+    case 1: return launch_batch_variant<R, 1>(b, cfg, stream);
+    case 3: return launch_batch_variant<R, 3>(b, cfg, stream);
+    default: return launch_batch_variant<R, 2>(b, cfg, stream);
+  }
+}
+
+int launch_batch_f32(const BatchLaunch<float>& b, const LaunchConfig& cfg,
+                     void* stream)
+{ return launch_batch_impl<float>(b, cfg, stream); }
+
+int launch_batch_f64(const BatchLaunch<double>& b, const LaunchConfig& cfg,
+                     void* stream)
+{ return launch_batch_impl<double>(b, cfg, stream); }
 
 int launch_realisations_f32
   (const DScene<float>& S, const DTallies& T, uint64_t seed, uint64_t first,

@@ -28,6 +28,25 @@ int launch_realisations_f64
   (const DScene<double>& S, const DTallies& T, uint64_t seed, uint64_t first,
    uint64_t count, const LaunchConfig& cfg, void* stream);
 
+/* Batched launch: device arrays of per-item scenes and tallies, the item
+ * budgets as an inclusive prefix (nitems + 1 entries; the last one is the
+ * launch total) and the first realisation index of each item */
+template<class R> struct BatchLaunch {
+  const DScene<R>* scenes;
+  const DTallies* tallies;
+  const unsigned long long* prefix;
+  const unsigned long long* firsts;
+  int nitems;
+  uint64_t seed;
+  unsigned long long* next_path; /* work counter (scratch) */
+  DStats* stats;
+};
+
+int launch_batch_f32(const BatchLaunch<float>& b, const LaunchConfig& cfg,
+                     void* stream);
+int launch_batch_f64(const BatchLaunch<double>& b, const LaunchConfig& cfg,
+                     void* stream);
+
 } /* namespace ssolb */
 
 #endif /* SSOL_B200_KERNELS_H */

@@ -95,11 +95,144 @@ struct ssol_b200_plan {
   bool timing_valid = false;
 };
 
+static TallyLayout tally_layout(int nrcv, int nsampled, int nprim_slots)
+{
+  TallyLayout tl;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = (off + bytes + 255) & ~size_t(255);
+    return o;
+  };
+  tl.global = take(NGLOBAL * 2 * sizeof(double));
+  tl.rcv = take((size_t)nrcv * NRCV_Q * 2 * sizeof(double));
+  tl.samp = take((size_t)nsampled * 4 * sizeof(double));
+  tl.samp_rcv = take((size_t)nsampled * nrcv * NRCV_Q * 2 * sizeof(double));
+  tl.prim = take((size_t)nprim_slots * NRCV_Q * 2 * sizeof(double));
+  tl.nb_samples = take((size_t)nsampled * sizeof(unsigned long long));
+  tl.counters = take(4 * sizeof(unsigned long long));
+  tl.stats = take(sizeof(DStats));
+  tl.total = off;
+  return tl;
+}
+
+static DTallies bind_tallies(const TallyLayout& tl, unsigned char* base)
+{
+  DTallies t;
+  t.global = (double*)(base + tl.global);
+  t.rcv = (double*)(base + tl.rcv);
+  t.samp = (double*)(base + tl.samp);
+  t.samp_rcv = (double*)(base + tl.samp_rcv);
+  t.prim = (double*)(base + tl.prim);
+  t.nb_samples = (unsigned long long*)(base + tl.nb_samples);
+  t.counters = (unsigned long long*)(base + tl.counters);
+  t.stats = (DStats*)(base + tl.stats);
+  return t;
+}
+
+static void fill_sums(double dst[10][2], const double* src);
+
+/* Estimator of `nreal` realisations from host copies of one tally layout
+ * (the merge step of src/ssol_solver.c:1254-1333 is already done on the
+ * device; this only maps slots back to instances) */
+static res_T make_estimator
+  (ssol_device* dev, ssol_scene* scn, const FlatMeta& meta,
+   const TallyLayout& tl, const unsigned char* base, uint64_t nreal,
+   const ssp_rng* rng, uint64_t rng_advance, const DStats* st,
+   double kernel_ms, size_t scene_bytes, size_t max_failed,
+   ssol_estimator** out)
+{
+  const int nrcv = (int)meta.rcv.size();
+  const int nsampled = (int)meta.sampled.size();
+  const double* g = (const double*)(base + tl.global);
+  const double* rcv = (const double*)(base + tl.rcv);
+  const double* samp = (const double*)(base + tl.samp);
+  const double* samp_rcv = (const double*)(base + tl.samp_rcv);
+  const double* prim = (const double*)(base + tl.prim);
+  const unsigned long long* nbs =
+    (const unsigned long long*)(base + tl.nb_samples);
+  const unsigned long long* cnt =
+    (const unsigned long long*)(base + tl.counters);
+
+  ssol_estimator* e = new (std::nothrow) ssol_estimator();
+  if(!e) return RES_MEM_ERR;
+  ssol_device_ref_get(dev);
+  e->dev = dev;
+  const size_t failed = (size_t)cnt[0];
+  e->failed_count = failed;
+  e->realisation_count = (size_t)nreal - std::min<size_t>(failed, nreal);
+  for(int q = 0; q < NGLOBAL; ++q) {
+    e->global[q][0] = g[2 * q];
+    e->global[q][1] = g[2 * q + 1];
+  }
+  e->sampled_area = meta.sampled_area;
+
+  /* Receivers are pre-registered like create_mc_receivers
+   * (src/ssol_estimator.c:30-60) */
+  for(const ssol_instance* inst : scn->instances) {
+    if(inst->receiver_mask) e->receivers[inst].inst = inst;
+  }
+  for(int r = 0; r < nrcv; ++r) {
+    const FlatMeta::RcvSide& rs = meta.rcv[r];
+    fill_sums(e->receivers[rs.inst].side[rs.side].q,
+              rcv + (size_t)r * NRCV_Q * 2);
+  }
+  for(const FlatMeta::PrimRange& pr : meta.prims) {
+    const FlatMeta::RcvSide& rs = meta.rcv[pr.rcv_slot];
+    std::vector<double>& v = e->receivers[rs.inst].side[rs.side].prims[pr.shape];
+    v.assign(prim + (size_t)pr.base * NRCV_Q * 2,
+             prim + (size_t)(pr.base + pr.ntris) * NRCV_Q * 2);
+  }
+  for(int si = 0; si < nsampled; ++si) {
+    SampEntry& se = e->sampled[meta.sampled[si]];
+    se.cos[0] = samp[si * 4 + 0];
+    se.cos[1] = samp[si * 4 + 1];
+    se.shadow[0] = samp[si * 4 + 2];
+    se.shadow[1] = samp[si * 4 + 3];
+    se.nb_samples = (size_t)nbs[si];
+    for(int r = 0; r < nrcv; ++r) {
+      const double* src = samp_rcv + ((size_t)si * nrcv + r) * NRCV_Q * 2;
+      bool any = false;
+      for(int q = 0; q < NRCV_Q * 2 && !any; ++q) any = src[q] != 0;
+      if(!any) continue;
+      const FlatMeta::RcvSide& rs = meta.rcv[r];
+      RcvEntry& re = se.by_receiver[rs.inst];
+      re.inst = rs.inst;
+      fill_sums(re.side[rs.side].q, src);
+    }
+  }
+  e->kernel_ms = kernel_ms;
+  e->stats[0] = st->rays;
+  e->stats[1] = st->node_visits;
+  e->stats[2] = st->tri_tests;
+  e->stats[3] = st->quad_tests;
+  e->stats[4] = st->bounces;
+  e->stats[5] = st->paths;
+  e->killed = cnt[1];
+  e->scene_bytes = scene_bytes;
+  e->tally_bytes = tl.total;
+
+  /* End state: the next realisation index (src/ssol_estimator.c:368-418) */
+  res_T res = ssolb_rng_clone_advanced(rng, rng_advance, &e->rng);
+  if(res != RES_OK) {
+    ssol_estimator_ref_put(e);
+    return res;
+  }
+  *out = e;
+  /* Too many failed paths: RES_BAD_OP with a valid estimator
+   * (src/ssol_solver.c:1240-1245, 1340) */
+  if(failed > 0 && failed >= max_failed) {
+    dev->log_error("Too many unexpected radiative paths.\n");
+    return RES_BAD_OP;
+  }
+  return RES_OK;
+}
+
 template<class R>
 static void bind_scene(DScene<R>& S, const FlatScene<R>& f, const Blob& b,
-                       unsigned char* base)
+                       unsigned char* base, size_t i0 = 0)
 {
-  size_t i = 0;
+  size_t i = i0;
   auto ptr = [&](void) { return base + b.offsets[i++]; };
   S.nodes = (const DNode<R>*)ptr();
   S.primrefs = (const uint32_t*)ptr();
@@ -210,6 +343,31 @@ static bool validate(const FlatScene<R>& f)
   if(f.air_medium < 0 || f.air_medium >= (int)f.media.size()) return false;
   if(f.wl_nodes.empty() || f.wl_cdf.size() != f.wl_nodes.size()) return false;
   return true;
+}
+
+template<class R>
+static void add_scene(Blob& b, const FlatScene<R>& f)
+{
+  b.add(f.nodes);
+  b.add(f.bvh.primrefs);
+  b.add(f.tris);
+  b.add(f.quads);
+  b.add(f.carvings);
+  b.add(f.carve_verts);
+  b.add(f.sinsts);
+  b.add(f.mtls);
+  b.add(f.media);
+  b.add(f.spectra);
+  b.add(f.spec_wl);
+  b.add(f.spec_val);
+  b.add(f.shader_tab);
+  b.add(f.shader_wl);
+  b.add(f.samp);
+  b.add(f.alias_prob);
+  b.add(f.alias_idx);
+  b.add(f.wl_nodes);
+  b.add(f.wl_pdf);
+  b.add(f.wl_cdf);
 }
 
 template<class R>
@@ -332,35 +490,12 @@ extern "C" res_T ssol_b200_plan_create
   p->nsampled = (int)p->meta.sampled.size();
 
   /* Tallies: FP64 sums, then integer counters */
-  TallyLayout& tl = p->tl;
-  size_t off = 0;
-  auto take = [&](size_t bytes) {
-    const size_t o = off;
-    off = (off + bytes + 255) & ~size_t(255);
-    return o;
-  };
-  tl.global = take(NGLOBAL * 2 * sizeof(double));
-  tl.rcv = take((size_t)p->nrcv * NRCV_Q * 2 * sizeof(double));
-  tl.samp = take((size_t)p->nsampled * 4 * sizeof(double));
-  tl.samp_rcv = take((size_t)p->nsampled * p->nrcv * NRCV_Q * 2 * sizeof(double));
-  tl.prim = take((size_t)p->meta.nprim_slots * NRCV_Q * 2 * sizeof(double));
-  tl.nb_samples = take((size_t)p->nsampled * sizeof(unsigned long long));
-  tl.counters = take(4 * sizeof(unsigned long long));
-  tl.stats = take(sizeof(DStats));
-  tl.total = off;
-  if(cudaMalloc(&p->d_tally, tl.total) != cudaSuccess) {
+  p->tl = tally_layout(p->nrcv, p->nsampled, p->meta.nprim_slots);
+  if(cudaMalloc(&p->d_tally, p->tl.total) != cudaSuccess) {
     plan_release(p);
     return RES_MEM_ERR;
   }
-  unsigned char* base = (unsigned char*)p->d_tally;
-  p->t.global = (double*)(base + tl.global);
-  p->t.rcv = (double*)(base + tl.rcv);
-  p->t.samp = (double*)(base + tl.samp);
-  p->t.samp_rcv = (double*)(base + tl.samp_rcv);
-  p->t.prim = (double*)(base + tl.prim);
-  p->t.nb_samples = (unsigned long long*)(base + tl.nb_samples);
-  p->t.counters = (unsigned long long*)(base + tl.counters);
-  p->t.stats = (DStats*)(base + tl.stats);
+  p->t = bind_tallies(p->tl, (unsigned char*)p->d_tally);
   cudaEventCreate(&p->ev0);
   cudaEventCreate(&p->ev1);
   *out = p;
@@ -439,90 +574,9 @@ extern "C" res_T ssol_b200_plan_finish
     if(cudaEventElapsedTime(&ms, p->ev0, p->ev1) == cudaSuccess)
       p->kernel_ms = ms;
   }
-  const unsigned char* base = h.data();
-  const double* g = (const double*)(base + p->tl.global);
-  const double* rcv = (const double*)(base + p->tl.rcv);
-  const double* samp = (const double*)(base + p->tl.samp);
-  const double* samp_rcv = (const double*)(base + p->tl.samp_rcv);
-  const double* prim = (const double*)(base + p->tl.prim);
-  const unsigned long long* nbs =
-    (const unsigned long long*)(base + p->tl.nb_samples);
-  const unsigned long long* cnt =
-    (const unsigned long long*)(base + p->tl.counters);
-  const DStats* st = (const DStats*)(base + p->tl.stats);
-
-  ssol_estimator* e = new (std::nothrow) ssol_estimator();
-  if(!e) return RES_MEM_ERR;
-  ssol_device_ref_get(p->dev);
-  e->dev = p->dev;
-  const size_t failed = (size_t)cnt[0];
-  e->failed_count = failed;
-  e->realisation_count = (size_t)nreal - std::min<size_t>(failed, nreal);
-  for(int q = 0; q < NGLOBAL; ++q) {
-    e->global[q][0] = g[2 * q];
-    e->global[q][1] = g[2 * q + 1];
-  }
-  e->sampled_area = p->meta.sampled_area;
-
-  /* Receivers are pre-registered like create_mc_receivers
-   * (src/ssol_estimator.c:30-60) */
-  for(const ssol_instance* inst : p->scn->instances) {
-    if(inst->receiver_mask) e->receivers[inst].inst = inst;
-  }
-  for(int r = 0; r < p->nrcv; ++r) {
-    const FlatMeta::RcvSide& rs = p->meta.rcv[r];
-    fill_sums(e->receivers[rs.inst].side[rs.side].q,
-              rcv + (size_t)r * NRCV_Q * 2);
-  }
-  for(const FlatMeta::PrimRange& pr : p->meta.prims) {
-    const FlatMeta::RcvSide& rs = p->meta.rcv[pr.rcv_slot];
-    std::vector<double>& v = e->receivers[rs.inst].side[rs.side].prims[pr.shape];
-    v.assign(prim + (size_t)pr.base * NRCV_Q * 2,
-             prim + (size_t)(pr.base + pr.ntris) * NRCV_Q * 2);
-  }
-  for(int si = 0; si < p->nsampled; ++si) {
-    SampEntry& se = e->sampled[p->meta.sampled[si]];
-    se.cos[0] = samp[si * 4 + 0];
-    se.cos[1] = samp[si * 4 + 1];
-    se.shadow[0] = samp[si * 4 + 2];
-    se.shadow[1] = samp[si * 4 + 3];
-    se.nb_samples = (size_t)nbs[si];
-    for(int r = 0; r < p->nrcv; ++r) {
-      const double* src = samp_rcv + ((size_t)si * p->nrcv + r) * NRCV_Q * 2;
-      bool any = false;
-      for(int q = 0; q < NRCV_Q * 2 && !any; ++q) any = src[q] != 0;
-      if(!any) continue;
-      const FlatMeta::RcvSide& rs = p->meta.rcv[r];
-      RcvEntry& re = se.by_receiver[rs.inst];
-      re.inst = rs.inst;
-      fill_sums(re.side[rs.side].q, src);
-    }
-  }
-  e->kernel_ms = p->kernel_ms;
-  e->stats[0] = st->rays;
-  e->stats[1] = st->node_visits;
-  e->stats[2] = st->tri_tests;
-  e->stats[3] = st->quad_tests;
-  e->stats[4] = st->bounces;
-  e->stats[5] = st->paths;
-  e->killed = cnt[1];
-  e->scene_bytes = p->scene_bytes;
-  e->tally_bytes = p->tl.total;
-
-  /* End state: the next realisation index (src/ssol_estimator.c:368-418) */
-  res_T res = ssolb_rng_clone_advanced(rng, nreal, &e->rng);
-  if(res != RES_OK) {
-    ssol_estimator_ref_put(e);
-    return res;
-  }
-  *out = e;
-  /* Too many failed paths: RES_BAD_OP with a valid estimator
-   * (src/ssol_solver.c:1240-1245, 1340) */
-  if(failed > 0 && failed >= max_failed) {
-    p->dev->log_error("Too many unexpected radiative paths.\n");
-    return RES_BAD_OP;
-  }
-  return RES_OK;
+  return make_estimator(p->dev, p->scn, p->meta, p->tl, h.data(), nreal, rng,
+                        nreal, (const DStats*)(h.data() + p->tl.stats),
+                        p->kernel_ms, p->scene_bytes, max_failed, out);
 }
 
 extern "C" res_T ssol_b200_plan_get_stats
@@ -534,6 +588,322 @@ extern "C" res_T ssol_b200_plan_get_stats
   s->scene_bytes = p->scene_bytes;
   s->tally_bytes = p->tl.total;
   return RES_OK;
+}
+
+
+/*******************************************************************************
+ * Batches: many scenes, one persistent launch (see ssol_b200.h)
+ ******************************************************************************/
+struct ssol_b200_batch {
+  RefCount ref;
+  ssol_device* dev = nullptr;
+  std::vector<ssol_scene*> scenes;
+  ssol_b200_options opt = SSOL_B200_OPTIONS_DEFAULT;
+  std::vector<FlatMeta> meta;
+  std::vector<TallyLayout> tl;
+  std::vector<size_t> tally_off; /* item tallies inside d_tally */
+  size_t tally_total = 0;
+  size_t scene_bytes = 0;
+  void* d_scene = nullptr; /* item scene arrays, then the DScene array */
+  void* d_tally = nullptr; /* item tallies, DTallies array, prefix, firsts,
+                              work counter and launch stats */
+  unsigned long long* d_prefix = nullptr;
+  unsigned long long* d_firsts = nullptr;
+  unsigned long long* d_next = nullptr;
+  DStats* d_stats = nullptr;
+  const void* d_scenes = nullptr;
+  const DTallies* d_tallies = nullptr;
+  std::vector<unsigned long long> done; /* realisations launched per item */
+  std::vector<unsigned long long> h_prefix, h_firsts;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double kernel_ms = 0;
+  bool timing_valid = false;
+  uint64_t h_seed = 0;
+};
+
+static void batch_release(ssol_b200_batch* b)
+{
+  if(b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+  if(b->graph) cudaGraphDestroy(b->graph);
+  if(b->d_scene) cudaFree(b->d_scene);
+  if(b->d_tally) cudaFree(b->d_tally);
+  if(b->ev0) cudaEventDestroy(b->ev0);
+  if(b->ev1) cudaEventDestroy(b->ev1);
+  for(ssol_scene* s : b->scenes) ssol_scene_ref_put(s);
+  ssol_device* dev = b->dev;
+  delete b;
+  if(dev) ssol_device_ref_put(dev);
+}
+
+extern "C" res_T ssol_b200_batch_ref_get(ssol_b200_batch* b)
+{
+  if(!b) return RES_BAD_ARG;
+  b->ref.get();
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_batch_ref_put(ssol_b200_batch* b)
+{
+  if(!b) return RES_BAD_ARG;
+  if(b->ref.put()) batch_release(b);
+  return RES_OK;
+}
+
+template<class R>
+static res_T batch_upload(ssol_b200_batch* b, std::vector<FlatScene<R>>& f)
+{
+  const size_t n = f.size();
+  Blob blob;
+  std::vector<size_t> first_index(n);
+  for(size_t i = 0; i < n; ++i) {
+    first_index[i] = blob.offsets.size();
+    add_scene(blob, f[i]);
+  }
+  /* DScene array at the end, filled once the base address is known */
+  std::vector<DScene<R>> S(n);
+  const size_t s_off = blob.add(S);
+  if(cudaMalloc(&b->d_scene, blob.host.size() + 256) != cudaSuccess)
+    return RES_MEM_ERR;
+  unsigned char* base = (unsigned char*)b->d_scene;
+  for(size_t i = 0; i < n; ++i) bind_scene(S[i], f[i], blob, base, first_index[i]);
+  std::memcpy(blob.host.data() + s_off, S.data(), n * sizeof(DScene<R>));
+  if(cudaMemcpyAsync(b->d_scene, blob.host.data(), blob.host.size(),
+                     cudaMemcpyHostToDevice, (cudaStream_t)b->dev->stream)
+     != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  if(cudaStreamSynchronize((cudaStream_t)b->dev->stream) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  b->scene_bytes = blob.host.size();
+  b->d_scenes = base + s_off;
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_batch_create
+  (ssol_scene* const* scenes, const size_t nscenes,
+   const ssol_b200_options* options, ssol_b200_batch** out)
+{
+  if(!scenes || !nscenes || !out || nscenes > (size_t)INT32_MAX)
+    return RES_BAD_ARG;
+  for(size_t i = 0; i < nscenes; ++i) if(!scenes[i]) return RES_BAD_ARG;
+  ssol_b200_options opt = options ? *options : SSOL_B200_OPTIONS_DEFAULT;
+  if(opt.precision != SSOL_B200_FP32 && opt.precision != SSOL_B200_FP64)
+    return RES_BAD_ARG;
+  if(opt.block_size < 0 || opt.block_size > 256 || opt.grid_blocks < 0
+  || opt.waves < 0 || opt.bvh_leaf_size < 0 || opt.min_blocks_per_sm < 0
+  || opt.min_blocks_per_sm > 3)
+    return RES_BAD_ARG;
+  if(opt.block_size == 0) opt.block_size = 256;
+  if(opt.block_size % 32) return RES_BAD_ARG;
+  if(opt.bvh_leaf_size == 0) opt.bvh_leaf_size = 1;
+  if(opt.max_segments == 0) opt.max_segments = 1000000ull;
+  if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = 2;
+
+  ssol_device* dev = scenes[0]->dev;
+  ssol_b200_batch* b = new (std::nothrow) ssol_b200_batch();
+  if(!b) return RES_MEM_ERR;
+  ssol_device_ref_get(dev);
+  b->dev = dev;
+  for(size_t i = 0; i < nscenes; ++i) {
+    ssol_scene_ref_get(scenes[i]);
+    b->scenes.push_back(scenes[i]);
+  }
+  b->opt = opt;
+  BvhBuildParams bp;
+  bp.max_leaf = opt.bvh_leaf_size;
+
+  /* Host snapshots first: argument errors need no GPU */
+  res_T res;
+  std::vector<FlatScene<float>> f32;
+  std::vector<FlatScene<double>> f64;
+  if(opt.precision == SSOL_B200_FP32) {
+    f32.resize(nscenes);
+    for(size_t i = 0; i < nscenes; ++i) {
+      res = flatten_scene(scenes[i], bp, f32[i]);
+      if(res == RES_OK && !validate(f32[i])) res = RES_UNKNOWN_ERR;
+      if(res != RES_OK) { batch_release(b); return res; }
+      b->meta.push_back(f32[i].meta);
+    }
+  } else {
+    f64.resize(nscenes);
+    for(size_t i = 0; i < nscenes; ++i) {
+      res = flatten_scene(scenes[i], bp, f64[i]);
+      if(res == RES_OK && !validate(f64[i])) res = RES_UNKNOWN_ERR;
+      if(res != RES_OK) { batch_release(b); return res; }
+      b->meta.push_back(f64[i].meta);
+    }
+  }
+  res = device_bind(dev);
+  if(res == RES_OK)
+    res = opt.precision == SSOL_B200_FP32 ? batch_upload(b, f32) : batch_upload(b, f64);
+  if(res != RES_OK) { batch_release(b); return res; }
+
+  /* Tallies of every item, then the batch bookkeeping */
+  size_t off = 0;
+  for(size_t i = 0; i < nscenes; ++i) {
+    const FlatMeta& m = b->meta[i];
+    b->tl.push_back(tally_layout((int)m.rcv.size(), (int)m.sampled.size(),
+                                 m.nprim_slots));
+    b->tally_off.push_back(off);
+    off += b->tl.back().total;
+  }
+  b->tally_total = off;
+  const size_t o_tallies = off;
+  off = (off + nscenes * sizeof(DTallies) + 255) & ~size_t(255);
+  const size_t o_prefix = off;
+  off = (off + (nscenes + 1) * sizeof(unsigned long long) + 255) & ~size_t(255);
+  const size_t o_firsts = off;
+  off = (off + nscenes * sizeof(unsigned long long) + 255) & ~size_t(255);
+  const size_t o_next = off;
+  off += 256;
+  const size_t o_stats = off;
+  off += (sizeof(DStats) + 255) & ~size_t(255);
+  if(cudaMalloc(&b->d_tally, off) != cudaSuccess) { batch_release(b); return RES_MEM_ERR; }
+  unsigned char* base = (unsigned char*)b->d_tally;
+  std::vector<DTallies> T(nscenes);
+  for(size_t i = 0; i < nscenes; ++i)
+    T[i] = bind_tallies(b->tl[i], base + b->tally_off[i]);
+  b->d_tallies = (const DTallies*)(base + o_tallies);
+  b->d_prefix = (unsigned long long*)(base + o_prefix);
+  b->d_firsts = (unsigned long long*)(base + o_firsts);
+  b->d_next = (unsigned long long*)(base + o_next);
+  b->d_stats = (DStats*)(base + o_stats);
+  const cudaStream_t s = (cudaStream_t)dev->stream;
+  if(cudaMemcpyAsync((void*)b->d_tallies, T.data(), nscenes * sizeof(DTallies),
+                     cudaMemcpyHostToDevice, s) != cudaSuccess
+  || cudaStreamSynchronize(s) != cudaSuccess) {
+    batch_release(b);
+    return RES_UNKNOWN_ERR;
+  }
+  b->done.assign(nscenes, 0);
+  b->h_prefix.assign(nscenes + 1, 0);
+  b->h_firsts.assign(nscenes, 0);
+  cudaEventCreate(&b->ev0);
+  cudaEventCreate(&b->ev1);
+  *out = b;
+  return ssol_b200_batch_reset(b, nullptr);
+}
+
+extern "C" res_T ssol_b200_batch_reset(ssol_b200_batch* b, void* stream)
+{
+  if(!b) return RES_BAD_ARG;
+  const cudaStream_t s = stream ? (cudaStream_t)stream : (cudaStream_t)b->dev->stream;
+  if(cudaMemsetAsync(b->d_tally, 0, b->tally_total, s) != cudaSuccess
+  || cudaMemsetAsync(b->d_stats, 0, sizeof(DStats), s) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  std::fill(b->done.begin(), b->done.end(), 0ull);
+  b->kernel_ms = 0;
+  b->timing_valid = false;
+  return RES_OK;
+}
+
+/* The captured graph: work-counter reset + the persistent batch kernel. Its
+ * parameters are device pointers only, so one capture serves every launch */
+static res_T batch_graph(ssol_b200_batch* b, const ssp_rng* rng, cudaStream_t s)
+{
+  if(b->graph_exec && b->graph_stream == s) return RES_OK;
+  if(b->graph_exec) { cudaGraphExecDestroy(b->graph_exec); b->graph_exec = nullptr; }
+  if(b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+  LaunchConfig cfg;
+  cfg.block_size = b->opt.block_size;
+  cfg.grid_blocks = b->opt.grid_blocks;
+  cfg.waves = b->opt.waves;
+  cfg.max_segments = b->opt.max_segments;
+  cfg.min_blocks = b->opt.min_blocks_per_sm;
+  if(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  int err;
+  if(b->opt.precision == SSOL_B200_FP32) {
+    BatchLaunch<float> L = {(const DScene<float>*)b->d_scenes, b->d_tallies,
+      b->d_prefix, b->d_firsts, (int)b->scenes.size(), rng->seed, b->d_next,
+      b->d_stats};
+    err = launch_batch_f32(L, cfg, s);
+  } else {
+    BatchLaunch<double> L = {(const DScene<double>*)b->d_scenes, b->d_tallies,
+      b->d_prefix, b->d_firsts, (int)b->scenes.size(), rng->seed, b->d_next,
+      b->d_stats};
+    err = launch_batch_f64(L, cfg, s);
+  }
+  const cudaError_t e2 = cudaStreamEndCapture(s, &b->graph);
+  if(err != 0 || e2 != cudaSuccess) return RES_UNKNOWN_ERR;
+  if(cudaGraphInstantiate(&b->graph_exec, b->graph, 0) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  b->graph_stream = s;
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_batch_launch
+  (ssol_b200_batch* b, const ssp_rng* rng, const uint64_t* budgets, void* stream)
+{
+  if(!b || !rng || !budgets) return RES_BAD_ARG;
+  const size_t n = b->scenes.size();
+  unsigned long long total = 0;
+  for(size_t i = 0; i < n; ++i) {
+    b->h_prefix[i] = total;
+    b->h_firsts[i] = rng->position + b->done[i];
+    total += budgets[i];
+  }
+  b->h_prefix[n] = total;
+  if(!total) return RES_OK;
+  const cudaStream_t s = stream ? (cudaStream_t)stream : (cudaStream_t)b->dev->stream;
+  /* The seed is a kernel argument baked into the graph */
+  if(b->graph_exec && b->graph_stream == s && rng->seed != b->h_seed) {
+    cudaGraphExecDestroy(b->graph_exec);
+    b->graph_exec = nullptr;
+  }
+  b->h_seed = rng->seed;
+  res_T res = batch_graph(b, rng, s);
+  if(res != RES_OK) return res;
+  if(cudaMemcpyAsync(b->d_prefix, b->h_prefix.data(), (n + 1) * sizeof(unsigned long long),
+                     cudaMemcpyHostToDevice, s) != cudaSuccess
+  || cudaMemcpyAsync(b->d_firsts, b->h_firsts.data(), n * sizeof(unsigned long long),
+                     cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  cudaEventRecord(b->ev0, s);
+  if(cudaGraphLaunch(b->graph_exec, s) != cudaSuccess) return RES_UNKNOWN_ERR;
+  cudaEventRecord(b->ev1, s);
+  /* Host arrays must stay untouched until the copies ran */
+  if(cudaStreamSynchronize(s) != cudaSuccess) return RES_UNKNOWN_ERR;
+  float ms = 0;
+  if(cudaEventElapsedTime(&ms, b->ev0, b->ev1) == cudaSuccess) b->kernel_ms += ms;
+  for(size_t i = 0; i < n; ++i) b->done[i] += budgets[i];
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_batch_finish
+  (ssol_b200_batch* b, const ssp_rng* rng, const size_t max_failed,
+   void* stream, ssol_estimator** out)
+{
+  if(!b || !rng || !out) return RES_BAD_ARG;
+  const cudaStream_t s = stream ? (cudaStream_t)stream : (cudaStream_t)b->dev->stream;
+  std::vector<unsigned char> h(b->tally_total);
+  DStats st;
+  if(cudaMemcpyAsync(h.data(), b->d_tally, b->tally_total, cudaMemcpyDeviceToHost, s)
+     != cudaSuccess
+  || cudaMemcpyAsync(&st, b->d_stats, sizeof(DStats), cudaMemcpyDeviceToHost, s)
+     != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  const cudaError_t err = cudaStreamSynchronize(s);
+  if(err != cudaSuccess) {
+    b->dev->log_error("device error: %s\n", cudaGetErrorString(err));
+    return RES_UNKNOWN_ERR;
+  }
+  res_T worst = RES_OK;
+  for(size_t i = 0; i < b->scenes.size(); ++i) {
+    out[i] = nullptr;
+    const res_T r = make_estimator(b->dev, b->scenes[i], b->meta[i], b->tl[i],
+      h.data() + b->tally_off[i], b->done[i], rng, b->done[i], &st, b->kernel_ms,
+      b->scene_bytes, max_failed, &out[i]);
+    if(r != RES_OK && r != RES_BAD_OP) {
+      for(size_t k = 0; k <= i; ++k)
+        if(out[k]) { ssol_estimator_ref_put(out[k]); out[k] = nullptr; }
+      return r;
+    }
+    if(r == RES_BAD_OP) worst = RES_BAD_OP;
+  }
+  return worst;
 }
 
 /*******************************************************************************

@@ -218,6 +218,11 @@ _OPTIONAL = {
     "ssol_b200_plan_reset": [VP, VP],
     "ssol_b200_plan_launch": [VP, VP, C.c_uint64, C.c_uint64, VP],
     "ssol_b200_plan_finish": [VP, VP, C.c_uint64, C.c_size_t, VP, PVP],
+    "ssol_b200_batch_create": [PVP, C.c_size_t, C.POINTER(B200Options), PVP],
+    "ssol_b200_batch_ref_put": [VP],
+    "ssol_b200_batch_reset": [VP, VP],
+    "ssol_b200_batch_launch": [VP, VP, C.POINTER(C.c_uint64), VP],
+    "ssol_b200_batch_finish": [VP, VP, C.c_size_t, VP, PVP],
 }
 
 
@@ -598,6 +603,45 @@ class Scene:
                 self.lib.raw("ssol_estimator_ref_put", est)
             raise SsolError("ssol_solve", res)
         return Estimator(self, est, res) if est else None
+
+
+class Batch:
+    """Several scenes traced by one persistent launch (ssol_b200_batch_*)."""
+
+    def __init__(self, lib, scenes, opts=None):
+        self.lib = lib
+        self.scenes = list(scenes)
+        arr = (C.c_void_p * len(scenes))(*[s.scn.value for s in scenes])
+        self.h = C.c_void_p()
+        lib.call("ssol_b200_batch_create", C.cast(arr, PVP), len(scenes),
+                 C.byref(opts) if opts is not None else None, C.byref(self.h))
+
+    def reset(self, stream=None):
+        self.lib.call("ssol_b200_batch_reset", self.h, stream)
+
+    def launch(self, rng, budgets, stream=None):
+        b = (C.c_uint64 * len(budgets))(*[int(x) for x in budgets])
+        self.lib.call("ssol_b200_batch_launch", self.h, rng, b, stream)
+
+    def finish(self, rng, max_failed=0, stream=None):
+        n = len(self.scenes)
+        arr = (C.c_void_p * n)()
+        res = self.lib.raw("ssol_b200_batch_finish", self.h, rng, max_failed, stream,
+                           C.cast(arr, PVP))
+        if res not in (RES_OK, RES_BAD_OP):
+            raise SsolError("ssol_b200_batch_finish", res)
+        return [Estimator(s, C.c_void_p(arr[i]), res) for i, s in enumerate(self.scenes)]
+
+    def close(self):
+        if self.h:
+            self.lib.raw("ssol_b200_batch_ref_put", self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def options(precision=FP32, block_size=256, grid_blocks=0, waves=1, leaf=0,

@@ -161,3 +161,35 @@ def heliostat_field(lib, n_helio=1000, elevation=30.0, azimuth=180.0, dni=900.0,
         s.atmosphere(extinction)
     return s, {"heliostats": helios, "receiver": rcv, "receiver_shape": rshape,
                "positions": pts, "sun": sun}
+
+
+# --------------------------------------------------------------- config 3
+def sun_grid(n_el=16, n_az=16, el_range=(5.0, 85.0), seed=0, dni_range=(300.0, 1000.0),
+             budget_range=(1e5, 1e7)):
+    """Sun positions of the batched workload: n_el elevations evenly spaced in
+    el_range x n_az azimuths 0, 360/n_az, ...; per sun a DNI uniform in
+    dni_range and a realisation budget log-uniform in budget_range, both
+    drawn from a seeded generator."""
+    import random
+    rnd = random.Random(seed)
+    suns = []
+    for i in range(n_el):
+        el = el_range[0] + (el_range[1] - el_range[0]) * i / max(1, n_el - 1)
+        for j in range(n_az):
+            az = 360.0 * j / n_az
+            dni = rnd.uniform(*dni_range)
+            lo, hi = math.log(budget_range[0]), math.log(budget_range[1])
+            budget = int(math.exp(rnd.uniform(lo, hi)))
+            suns.append({"elevation": el, "azimuth": az, "dni": dni, "budget": budget})
+    return suns
+
+
+def batched_fields(lib, suns, n_helio=1000, receiver_cells=64):
+    """One heliostat_field scene per sun, heliostats re-aimed for that sun."""
+    out = []
+    for sun in suns:
+        s, h = heliostat_field(lib, n_helio=n_helio, elevation=sun["elevation"],
+                               azimuth=sun["azimuth"], dni=sun["dni"],
+                               receiver_cells=receiver_cells)
+        out.append((s, h))
+    return out

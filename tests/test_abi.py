@@ -133,3 +133,25 @@ def test_rng_shim_matches_between_libraries(product, oracle):
         outs.append([lib.dll.ssp_rng_get(r) for _ in range(8)])
         lib.call("ssp_rng_ref_put", r)
     assert outs[0] == outs[1]
+
+
+def test_batch_host_path(product):
+    """Batch creation validates and snapshots every scene on the host; without
+    a GPU it stops at device binding (RES_UNKNOWN_ERR), with bad arguments at
+    RES_BAD_ARG."""
+    import workloads as W
+    fields = W.batched_fields(product, [{"elevation": 30.0, "azimuth": 180.0, "dni": 900.0},
+                                        {"elevation": 50.0, "azimuth": 90.0, "dni": 600.0}],
+                              n_helio=10, receiver_cells=4)
+    arr = (C.c_void_p * 2)(*[f[0].scn.value for f in fields])
+    h = C.c_void_p()
+    assert product.raw("ssol_b200_batch_create", None, 2, None, C.byref(h)) == P.RES_BAD_ARG
+    assert product.raw("ssol_b200_batch_create", C.cast(arr, P.PVP), 0, None,
+                       C.byref(h)) == P.RES_BAD_ARG
+    res = product.raw("ssol_b200_batch_create", C.cast(arr, P.PVP), 2, None, C.byref(h))
+    import conftest
+    if conftest.gpu_available():
+        assert res == P.RES_OK
+        product.raw("ssol_b200_batch_ref_put", h)
+    else:
+        assert res == P.RES_UNKNOWN_ERR
