@@ -1527,6 +1527,122 @@ int launch_batch_f64(const BatchLaunch<double>& b, const LaunchConfig& cfg,
                      void* stream)
 { return launch_batch_impl<double>(b, cfg, stream); }
 
+/* Scratch of the no-allocation batched launch: one file-scope device array
+ * holding the budget prefix sums (NOALLOC_MAX_ITEMS + 1 words), the
+ * per-item first realisation ids (NOALLOC_MAX_ITEMS words), the work counter
+ * and the launch counters (DStats). Every call on a device shares it. */
+constexpr size_t NOALLOC_PREFIX = 0;
+constexpr size_t NOALLOC_FIRSTS = NOALLOC_MAX_ITEMS + 1;
+constexpr size_t NOALLOC_NEXT = 2 * NOALLOC_MAX_ITEMS + 1;
+constexpr size_t NOALLOC_STATS = 2 * NOALLOC_MAX_ITEMS + 2;
+constexpr size_t NOALLOC_WORDS =
+  NOALLOC_STATS + sizeof(DStats) / sizeof(unsigned long long);
+static __device__ __align__(256) unsigned long long
+  g_noalloc_scratch[NOALLOC_WORDS];
+
+/* Device address of the scratch array, resolved once per device with that
+ * device current: the host-side name of a __device__ array is a stand-in,
+ * not an address a kernel may be given */
+static int noalloc_scratch_address(unsigned long long** out)
+{
+  static unsigned long long* cache[64] = {};
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if(err != cudaSuccess) return (int)err;
+  if(dev < 0 || dev >= 64) return (int)cudaErrorInvalidDevice;
+  if(!cache[dev]) {
+    void* ptr = nullptr;
+    err = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if(err != cudaSuccess) return (int)err;
+    cache[dev] = (unsigned long long*)ptr;
+  }
+  *out = cache[dev];
+  return 0;
+}
+
+template<class R, int MINB>
+static int launch_batch_noalloc_variant
+  (const DScene<R>* scenes, const DTallies* tallies, int nitems, uint64_t seed,
+   const unsigned long long* h_prefix, const unsigned long long* h_firsts,
+   const LaunchConfig& cfg, void* stream)
+{
+  if(nitems < 1 || nitems > NOALLOC_MAX_ITEMS) return (int)cudaErrorInvalidValue;
+  unsigned long long* scratch = nullptr;
+  int err = noalloc_scratch_address(&scratch);
+  if(err) return err;
+  const cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int block = cfg.block_size > 0 ? cfg.block_size : MAX_BLOCK;
+  if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
+  const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block) * sizeof(double)
+                    + (size_t)STACK_SIZE * block * sizeof(int);
+  cudaFuncSetAttribute(batch_kernel<R, MINB>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor
+    (&per_sm, batch_kernel<R, MINB>, block, smem);
+  if(per_sm < 1) per_sm = 1;
+  const uint64_t blocks = cfg.grid_blocks > 0
+    ? (uint64_t)cfg.grid_blocks
+    : (uint64_t)nsm * (uint64_t)per_sm * (uint64_t)(cfg.waves > 0 ? cfg.waves : 1);
+  /* Budgets and stream offsets of this call; the work counter and launch
+   * counters start at zero (the array keeps the previous call's values) */
+  cudaError_t e;
+  e = cudaMemcpyAsync(scratch + NOALLOC_PREFIX, h_prefix,
+                      (size_t)(nitems + 1) * sizeof(unsigned long long),
+                      cudaMemcpyHostToDevice, s);
+  if(e != cudaSuccess) return (int)e;
+  e = cudaMemcpyAsync(scratch + NOALLOC_FIRSTS, h_firsts,
+                      (size_t)nitems * sizeof(unsigned long long),
+                      cudaMemcpyHostToDevice, s);
+  if(e != cudaSuccess) return (int)e;
+  e = cudaMemsetAsync(scratch + NOALLOC_NEXT, 0,
+                      (NOALLOC_WORDS - NOALLOC_NEXT) * sizeof(unsigned long long), s);
+  if(e != cudaSuccess) return (int)e;
+  batch_kernel<R, MINB><<<(unsigned)blocks, block, smem, s>>>
+    (scenes, tallies, scratch + NOALLOC_PREFIX, scratch + NOALLOC_FIRSTS, nitems,
+     seed, cfg.max_segments, scratch + NOALLOC_NEXT,
+     reinterpret_cast<DStats*>(scratch + NOALLOC_STATS));
+  return (int)cudaGetLastError();
+}
+
+template<class R>
+static int launch_batch_noalloc_impl
+  (const DScene<R>* scenes, const DTallies* tallies, int nitems, uint64_t seed,
+   const unsigned long long* h_prefix, const unsigned long long* h_firsts,
+   const LaunchConfig& cfg, void* stream)
+{
+  switch(cfg.min_blocks) {
+    case 1: return launch_batch_noalloc_variant<R, 1>
+      (scenes, tallies, nitems, seed, h_prefix, h_firsts, cfg, stream);
+    case 3: return launch_batch_noalloc_variant<R, 3>
+      (scenes, tallies, nitems, seed, h_prefix, h_firsts, cfg, stream);
+    default: return launch_batch_noalloc_variant<R, 2>
+      (scenes, tallies, nitems, seed, h_prefix, h_firsts, cfg, stream);
+  }
+}
+
+int launch_batch_noalloc_f32
+  (const DScene<float>* scenes, const DTallies* tallies, int nitems,
+   uint64_t seed, const unsigned long long* h_prefix,
+   const unsigned long long* h_firsts, const LaunchConfig& cfg, void* stream)
+{
+  return launch_batch_noalloc_impl<float>
+    (scenes, tallies, nitems, seed, h_prefix, h_firsts, cfg, stream);
+}
+
+int launch_batch_noalloc_f64
+  (const DScene<double>* scenes, const DTallies* tallies, int nitems,
+   uint64_t seed, const unsigned long long* h_prefix,
+   const unsigned long long* h_firsts, const LaunchConfig& cfg, void* stream)
+{
+  return launch_batch_noalloc_impl<double>
+    (scenes, tallies, nitems, seed, h_prefix, h_firsts, cfg, stream);
+}
+
 int launch_realisations_f32
   (const DScene<float>& S, const DTallies& T, uint64_t seed, uint64_t first,
    uint64_t count, const LaunchConfig& cfg, void* stream)

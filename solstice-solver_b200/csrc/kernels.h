@@ -44,6 +44,23 @@ template<class R> struct BatchLaunch {
 
 int launch_batch_f32(const BatchLaunch<float>& b, const LaunchConfig& cfg,
                      void* stream);
+
+/* Largest item count of the no-allocation batched launch: its scratch is a
+ * static device array sized for this many items */
+constexpr int NOALLOC_MAX_ITEMS = 4096;
+
+/* Batched launch whose scratch (budget prefix, per-item first ids, work
+ * counter, launch counters) lives in a static device array instead of
+ * caller or library allocations; h_prefix (nitems + 1) and h_firsts
+ * (nitems) are host arrays copied into it */
+int launch_batch_noalloc_f32
+  (const DScene<float>* scenes, const DTallies* tallies, int nitems,
+   uint64_t seed, const unsigned long long* h_prefix,
+   const unsigned long long* h_firsts, const LaunchConfig& cfg, void* stream);
+int launch_batch_noalloc_f64
+  (const DScene<double>* scenes, const DTallies* tallies, int nitems,
+   uint64_t seed, const unsigned long long* h_prefix,
+   const unsigned long long* h_firsts, const LaunchConfig& cfg, void* stream);
 int launch_batch_f64(const BatchLaunch<double>& b, const LaunchConfig& cfg,
                      void* stream);
 

@@ -872,6 +872,52 @@ extern "C" res_T ssol_b200_batch_launch
   return RES_OK;
 }
 
+/* The no-allocation launch (declared in ssol_b200.h): same kernel and
+ * results as ssol_b200_batch_launch, without the graph and with the
+ * launch's scratch in a static device array (kernels.cu) */
+extern "C" res_T ssol_b200_batch_launch_noalloc
+  (ssol_b200_batch* b, const ssp_rng* rng, const uint64_t* budgets, void* stream)
+{
+  if(!b || !rng || !budgets) return RES_BAD_ARG;
+  const size_t n = b->scenes.size();
+  if(n > (size_t)NOALLOC_MAX_ITEMS) {
+    b->dev->log_error("ssol_b200_batch_launch_noalloc: %zu items, at most %d "
+                      "fit its static scratch.\n", n, NOALLOC_MAX_ITEMS);
+    return RES_BAD_ARG;
+  }
+  unsigned long long total = 0;
+  for(size_t i = 0; i < n; ++i) {
+    b->h_prefix[i] = total;
+    b->h_firsts[i] = rng->position + b->done[i];
+    total += budgets[i];
+  }
+  b->h_prefix[n] = total;
+  if(!total) return RES_OK;
+  const cudaStream_t s = stream ? (cudaStream_t)stream : (cudaStream_t)b->dev->stream;
+  LaunchConfig cfg;
+  cfg.block_size = b->opt.block_size;
+  cfg.grid_blocks = b->opt.grid_blocks;
+  cfg.waves = b->opt.waves;
+  cfg.max_segments = b->opt.max_segments;
+  cfg.min_blocks = b->opt.min_blocks_per_sm;
+  const int err = b->opt.precision == SSOL_B200_FP32
+    ? launch_batch_noalloc_f32((const DScene<float>*)b->d_scenes, b->d_tallies,
+                               (int)n, rng->seed, b->h_prefix.data(),
+                               b->h_firsts.data(), cfg, s)
+    : launch_batch_noalloc_f64((const DScene<double>*)b->d_scenes, b->d_tallies,
+                               (int)n, rng->seed, b->h_prefix.data(),
+                               b->h_firsts.data(), cfg, s);
+  if(err != 0) {
+    b->dev->log_error("ssol_b200_batch_launch_noalloc: %s\n",
+                      cudaGetErrorString((cudaError_t)err));
+    return RES_UNKNOWN_ERR;
+  }
+  /* The host budget arrays are read by the copies: wait for them */
+  if(cudaStreamSynchronize(s) != cudaSuccess) return RES_UNKNOWN_ERR;
+  for(size_t i = 0; i < n; ++i) b->done[i] += budgets[i];
+  return RES_OK;
+}
+
 extern "C" res_T ssol_b200_batch_finish
   (ssol_b200_batch* b, const ssp_rng* rng, const size_t max_failed,
    void* stream, ssol_estimator** out)

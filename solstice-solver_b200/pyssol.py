@@ -223,6 +223,7 @@ _OPTIONAL = {
     "ssol_b200_batch_reset": [VP, VP],
     "ssol_b200_batch_launch": [VP, VP, C.POINTER(C.c_uint64), VP],
     "ssol_b200_batch_finish": [VP, VP, C.c_size_t, VP, PVP],
+    "ssol_b200_batch_launch_noalloc": [VP, VP, C.POINTER(C.c_uint64), VP],
 }
 
 
@@ -622,6 +623,10 @@ class Batch:
     def launch(self, rng, budgets, stream=None):
         b = (C.c_uint64 * len(budgets))(*[int(x) for x in budgets])
         self.lib.call("ssol_b200_batch_launch", self.h, rng, b, stream)
+
+    def launch_noalloc(self, rng, budgets, stream=None):
+        b = (C.c_uint64 * len(budgets))(*[int(x) for x in budgets])
+        self.lib.call("ssol_b200_batch_launch_noalloc", self.h, rng, b, stream)
 
     def finish(self, rng, max_failed=0, stream=None):
         n = len(self.scenes)
