@@ -114,11 +114,21 @@ def dist_env():
     return rank, world, local
 
 
+BEAMDOWN = ("beam-down tower: 5000 punched 8x8 paraboloid heliostats (surround field, "
+            "r <= 440 m, focal = slant range to the secondary), hyperboloid secondary at "
+            "120 m (40x40 m, reflectivity 0.95, pillbox microfacet 1.5 mrad), 6x6 ground "
+            "receiver (absorptivity 0.9, 30x30 per-primitive map) under a thin-dielectric "
+            "window (n 1.5, 20/m, 5 mm), Gaussian sun 2.5 mrad el 60 az 180 DNI 1000")
+
+
 def build_workload(lib, args):
     import workloads as W
     if args.config == "mirror":
         s, h = W.single_mirror(lib)
         desc = "single 10x10 mirror, 4x4 receiver at 50 m, pillbox 4.65 mrad, DNI 1000"
+    elif args.config == "beamdown":
+        s, h = W.beam_down(lib)
+        desc = BEAMDOWN
     else:
         s, h = W.heliostat_field(lib, n_helio=args.heliostats)
         desc = WORKLOAD if args.heliostats == 1000 else WORKLOAD.replace(
@@ -206,6 +216,12 @@ def run_b200(args):
     s, h, desc = build_workload(lib, args)
     opt = P.options(P.FP64 if args.fp64 else P.FP32, block_size=args.block,
                     waves=args.waves, leaf=args.leaf, min_blocks=args.minb)
+    tuned_ms = None
+    if args.autotune:
+        opt, tuned_ms = P.autotune(s, args.autotune_paths, opt, seed=args.seed + 77)
+    launch_shape = {"block": opt.block_size, "blocks_per_sm_budget": opt.min_blocks_per_sm,
+                    "waves": opt.waves, "bvh_leaf": opt.bvh_leaf_size,
+                    "autotuned": bool(args.autotune)}
     plan = P.C.c_void_p()
     lib.call("ssol_b200_plan_create", s.scn, P.C.byref(opt), P.C.byref(plan))
     rng = s.rng(seed=args.seed)
@@ -301,7 +317,8 @@ def run_b200(args):
         "config": {"workload": desc, "paths_per_step": n, "precision":
                    "FP64" if args.fp64 else "FP32 geometry/BSDF, FP64 tallies",
                    "l2": "flushed: 256 MiB write between steps (scene < 2 MB)",
-                   "parallelism": "realisation ranges per GPU" if world > 1 else "1 GPU"},
+                   "parallelism": "realisation ranges per GPU" if world > 1 else "1 GPU",
+                   "launch": launch_shape},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
                 "timing": "wall clock around synchronous ssol_solve"},
@@ -341,28 +358,224 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+SUNS = ("256 suns (16 elevations 5-85 deg x 16 azimuths, DNI U[300,1000]) over the "
+        "1000-heliostat field re-aimed per sun; per-sun budgets = realisations for 0.1% "
+        "relative SE on absorbed power (from a pilot of log-U[1e5,1e7] budgets)")
+
+
+def run_suns(args):
+    """Batched multi-sun form against plain per-sun launches.
+
+    Pilot: one batched launch with the seeded log-uniform budgets gives each
+    sun's relative SE on absorbed power, hence the realisations n_i it needs
+    for 0.1% (SE ~ 1/sqrt(n)). Timed, for the same n_i: (a) the batched
+    launch (all suns in one persistent kernel replayed from a CUDA graph),
+    (b) a loop of plain plan launches, one per sun, scenes resident in HBM,
+    (c) end to end through the public API, per step: batch create (scene
+    build and upload), launch, finish (tally read-back and estimators);
+    and (d) the reference user's loop of one ssol_solve per sun."""
+    import torch
+    import pyssol as P
+    import workloads as W
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    lib = P.load_product()
+    suns = W.sun_grid()[rank::world]
+    built = W.batched_fields(lib, suns, n_helio=args.heliostats)
+    scenes = [b[0] for b in built]
+    rcv = [b[1]["receiver"] for b in built]
+    opt = P.options(P.FP64 if args.fp64 else P.FP32, block_size=args.block,
+                    waves=args.waves, leaf=args.leaf, min_blocks=args.minb)
+    if args.autotune:
+        opt, _ = P.autotune(scenes[len(scenes) // 2], args.autotune_paths, opt,
+                            seed=args.seed + 77)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp = P.C.c_void_p(stream.cuda_stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    rng = scenes[0].rng(seed=args.seed)
+
+    # pilot
+    pilot = P.Batch(lib, scenes, opt)
+    pilot.launch(rng, [sn["budget"] for sn in suns], sp)
+    ests = pilot.finish(rng, 0, sp)
+    target = 1e-3
+    need = []
+    for sn, e in zip(suns, ests):
+        a = e.globals()["absorbed_by_receivers"]
+        rse = a[2] / a[0] if a[0] > 0 else 1.0
+        need.append(int(min(max(sn["budget"] * (rse / target) ** 2, 1e5), 1e8)))
+    del ests
+    pilot.close()
+    n_total = sum(need)
+
+    def timed(step, steps):
+        for w in range(args.warmup):
+            step()
+            flush.zero_()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        for k in range(steps):
+            ev[k][0].record(stream)
+            step()
+            ev[k][1].record(stream)
+            flush.zero_()
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev)
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t[0])
+        return ms
+
+    # (a) batched
+    batch = P.Batch(lib, scenes, opt)
+    clocks = Clocks(local)
+    clocks.start()
+    ms_batched = timed(lambda: batch.launch(rng, need, sp), args.steps)
+    clk = clocks.stop()
+    ests = batch.finish(rng, 0, sp)
+    # counters and scene bytes are batch-wide (every item's estimator carries
+    # them); tally bytes are per item
+    bstats = ests[0].stats()
+    tally_bytes = sum(e.stats()["tally_bytes"] for e in ests)
+    reached = sum(1 for e in ests if e.globals()["absorbed_by_receivers"][2]
+                  <= target * e.globals()["absorbed_by_receivers"][0] * 1.05)
+    del ests
+    batch.close()
+
+    # (b) plain plan launches, one per sun
+    plans = []
+    for sc in scenes:
+        pl = P.C.c_void_p()
+        lib.call("ssol_b200_plan_create", sc.scn, P.C.byref(opt), P.C.byref(pl))
+        plans.append(pl)
+
+    def plain_step():
+        for pl, n in zip(plans, need):
+            lib.call("ssol_b200_plan_launch", pl, rng, 0, n, sp)
+    ms_plain = timed(plain_step, args.steps)
+    for pl in plans:
+        lib.raw("ssol_b200_plan_ref_put", pl)
+
+    # (c) end to end through the batch API, and (d) one ssol_solve per sun
+    h2d = bstats["scene_bytes"]
+    d2h = tally_bytes
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(max(1, min(args.steps, 2))):
+        b = P.Batch(lib, scenes, opt)
+        b.launch(rng, need, sp)
+        es = b.finish(rng, 0, sp)
+        del es
+        b.close()
+    e2e_s = (time.perf_counter() - t0) / max(1, min(args.steps, 2))
+    t0 = time.perf_counter()
+    for sc, n in zip(scenes, need):
+        e = sc.solve(n, rng=rng, options=opt)
+        del e
+    solve_loop_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s, solve_loop_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s, solve_loop_s = float(t[0]), float(t[1])
+        tot = torch.tensor([float(n_total)], device="cuda")
+        dist.all_reduce(tot)
+        n_all = float(tot[0])
+    else:
+        n_all = float(n_total)
+
+    per_step_b = ms_batched / args.steps
+    per_step_p = ms_plain / args.steps
+    value = n_all / (per_step_b * 1e-3) / 1e6
+    agg = {k: bstats[k] for k in ("rays", "node_visits", "triangle_tests",
+                                  "quadric_tests", "bounces", "paths")}
+    peaks = measured_peaks()
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
+    sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = nsm * 128 * 2 * sm_mhz * 1e6 / 1e12
+    # the counters cover the warm-up and timed launches of the batch
+    launches = args.warmup + args.steps
+    achieved = flops_per_run(agg) / launches / (per_step_b * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step_b,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64" if args.fp64 else "f32",
+        "data": "synthetic (seeded sun grid, DNI and budgets)",
+        "config": {"workload": SUNS, "suns": len(suns) * world,
+                   "paths_per_step": int(n_all),
+                   "l2": "flushed: 256 MiB write between steps",
+                   "parallelism": "sun slots per GPU" if world > 1 else "1 GPU",
+                   "launch": {"block": opt.block_size,
+                              "blocks_per_sm_budget": opt.min_blocks_per_sm,
+                              "waves": opt.waves, "bvh_leaf": opt.bvh_leaf_size,
+                              "autotuned": bool(args.autotune)}},
+        "time_to_0.1pct_se_s": {"batched": per_step_b * 1e-3,
+                                "plain_plan_loop": per_step_p * 1e-3,
+                                "ssol_solve_loop": solve_loop_s,
+                                "batch_api_end_to_end": e2e_s},
+        "speedup_batched_vs_plain_plan_loop": per_step_p / per_step_b,
+        "speedup_batched_vs_ssol_solve_loop": solve_loop_s / (per_step_b * 1e-3),
+        "suns_reaching_0.1pct_se": reached,
+        "e2e": {"value": n_all / e2e_s / 1e6, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "timing": "wall clock: batch create + launch + finish per step"},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "work_model": "as the field line"},
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    for sc in scenes:
+        sc.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--config", default="field", choices=["field", "mirror"])
+    p.add_argument("--config", default="field", choices=["field", "mirror", "beamdown", "suns"])
     p.add_argument("--heliostats", type=int, default=1000)
-    p.add_argument("--paths", type=int, default=100_000_000)
+    p.add_argument("--paths", type=int, default=None,
+                   help="realisations per step (field 1e8, beamdown 2e8, mirror 1e6)")
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--fp64", action="store_true")
     p.add_argument("--block", type=int, default=256)
     p.add_argument("--waves", type=int, default=1)
     p.add_argument("--leaf", type=int, default=0)
     p.add_argument("--minb", type=int, default=0)
+    p.add_argument("--no-autotune", dest="autotune", action="store_false",
+                   help="use --block/--minb/--waves/--leaf as given")
+    p.add_argument("--autotune-paths", type=int, default=4_000_000)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--ref-step-seconds", type=float, default=10.0)
     args = p.parse_args()
+    if args.paths is None:
+        args.paths = {"beamdown": 200_000_000, "mirror": 1_000_000}.get(args.config,
+                                                                         100_000_000)
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "suns":
+        run_suns(args)
     else:
         run_b200(args)
 

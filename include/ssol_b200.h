@@ -95,6 +95,17 @@ SSOL_API res_T ssol_b200_plan_finish
 SSOL_API res_T ssol_b200_plan_get_stats
   (const struct ssol_b200_plan* plan, struct ssol_b200_stats* stats);
 
+/* Autotuner: times `trial_paths` realisations of `scn` for every launch
+ * shape in {block 128, 256} x {register budget 1, 2, 3 blocks per SM} x
+ * {1, 2 persistent waves} on each BVH leaf size in {1, 2, 4} (one snapshot
+ * per leaf size), after one untimed launch of each, and writes the fastest
+ * into `options` (its precision and max_segments are kept). `best_ms`, if
+ * not NULL, receives that launch's CUDA-event time. Synchronous; tallies of
+ * the trials are discarded. */
+SSOL_API res_T ssol_b200_autotune
+  (struct ssol_scene* scn, const struct ssp_rng* rng, const uint64_t trial_paths,
+   struct ssol_b200_options* options, double* best_ms);
+
 /* Batches: several scenes (typically one per sun position, each with its own
  * re-aimed field and sun) traced by one persistent kernel launch replayed
  * from a captured CUDA graph, each item with its own budget and tallies */

@@ -1235,7 +1235,7 @@ API res_T ssol_scene_attach_atmosphere(ssol_scene* s, ssol_atmosphere* a)
  ******************************************************************************/
 namespace {
 
-struct OTri { V v0, e1, e2; int sinst; unsigned prim; int gid; };
+struct OTri { V v0, v1, v2; int sinst; unsigned prim; int gid; };
 struct OQuad {
   Affine l2w, w2l; const ssol_shape* shape; int sinst;
 };
@@ -1296,7 +1296,7 @@ void prim_box(const Scene& S, int ref, double lo[3], double hi[3])
 {
   if(ref >= 0) {
     const OTri& t = S.tris[ref];
-    const V p[3] = {t.v0, t.v0 + t.e1, t.v0 + t.e2};
+    const V p[3] = {t.v0, t.v1, t.v2};
     for(int c = 0; c < 3; ++c) {
       const double a = c == 0 ? p[0].x : c == 1 ? p[0].y : p[0].z;
       lo[c] = hi[c] = a;
@@ -1461,14 +1461,14 @@ res_T make_scene(ssol_scene* scn, Scene& S)
           const V p0 = v3(vf[0][0], vf[0][1], vf[0][2]);
           const V p1 = v3(vf[1][0], vf[1][1], vf[1][2]);
           const V p2 = v3(vf[2][0], vf[2][1], vf[2][2]);
-          OTri tr = {p0, p1 - p0, p2 - p0, si, (unsigned)t, first + (int)t};
+          OTri tr = {p0, p1, p2, si, (unsigned)t, first + (int)t};
           S.tris.push_back(tr);
           if(inst->sample) {
-            const V n = cross(tr.e2, tr.e1);
+            const V n = cross(p2 - p0, p1 - p0);
             const double len = std::sqrt(dot(n, n));
             const V nu = len > 0 ? n * (1 / len) : v3(0, 0, 0);
             const V nf = v3((float)nu.x, (float)nu.y, (float)nu.z);
-            OSamp sp = {p0, tr.e1, tr.e2, nf, si, (unsigned)t, tr.gid};
+            OSamp sp = {p0, p1 - p0, p2 - p0, nf, si, (unsigned)t, tr.gid};
             S.samp.push_back(sp);
             area.push_back(0.5 * len);
           }
@@ -1535,26 +1535,53 @@ bool side_ok(const Scene& S, int si, int side, const Self& self)
   return true;
 }
 
-void hit_tri(const Scene& S, int i, V o, V d, double tmin, double eps,
-             const Self& self, OHit& h)
+/* Watertight ray/triangle test (Woop, Benthin and Wald, "Watertight
+ * Ray/Triangle Intersection", JCGT 2(1), 2013), which is what keeps the rays
+ * through a shared edge or vertex (every ray through the focus of
+ * src/test_ssol_solver4.c crosses the diagonal of its targets) from falling
+ * between two triangles. The vertices are sheared into a frame where the ray
+ * runs along +z; the 2D edge functions of an edge shared by two triangles are
+ * then exact negations of each other (this file is compiled without FP
+ * contraction). Ng = e2 x e1 is Star-3D's front face. */
+struct OShear { int kx, ky, kz; double sx, sy, sz; };
+
+OShear make_shear(V d)
+{
+  const double a[3] = {std::fabs(d.x), std::fabs(d.y), std::fabs(d.z)};
+  const int kz = a[0] > a[1] ? (a[0] > a[2] ? 0 : 2) : (a[1] > a[2] ? 1 : 2);
+  int kx = kz == 2 ? 0 : kz + 1, ky = kx == 2 ? 0 : kx + 1;
+  const double dv[3] = {d.x, d.y, d.z};
+  if(dv[kz] < 0) std::swap(kx, ky);
+  return {kx, ky, kz, dv[kx] / dv[kz], dv[ky] / dv[kz], 1 / dv[kz]};
+}
+
+void hit_tri(const Scene& S, int i, V o, V d, const OShear& sh, double tmin,
+             double eps, const Self& self, OHit& h)
 {
   const OTri& T = S.tris[i];
-  const V p = cross(d, T.e2);
-  const double det = dot(T.e1, p);
-  if(det == 0) return;
-  const double inv = 1 / det;
-  const V s = o - T.v0;
-  const double u = dot(s, p) * inv;
-  if(u < 0 || u > 1) return;
-  const V q = cross(s, T.e1);
-  const double v = dot(d, q) * inv;
-  if(v < 0 || u + v > 1) return;
-  const double t = dot(T.e2, q) * inv;
+  const V a = T.v0 - o, b = T.v1 - o, c = T.v2 - o;
+  const double av[3] = {a.x, a.y, a.z}, bv[3] = {b.x, b.y, b.z};
+  const double cv[3] = {c.x, c.y, c.z};
+  const double ax = av[sh.kx] - sh.sx * av[sh.kz], ay = av[sh.ky] - sh.sy * av[sh.kz];
+  const double bx = bv[sh.kx] - sh.sx * bv[sh.kz], by = bv[sh.ky] - sh.sy * bv[sh.kz];
+  const double cx = cv[sh.kx] - sh.sx * cv[sh.kz], cy = cv[sh.ky] - sh.sy * cv[sh.kz];
+  const double U = cx * by - cy * bx;
+  const double Vv = ax * cy - ay * cx;
+  const double W = bx * ay - by * ax;
+  if((U < 0 || Vv < 0 || W < 0) && (U > 0 || Vv > 0 || W > 0)) return;
+  if(U + Vv + W == 0) return;
+  /* Distance from the plane of the triangle, dot(Ng, v0 - o) / dot(Ng, d):
+   * the two triangles of a planar quad then give the same distance, so a
+   * ray that passes through a virtual quad on its shared edge is not
+   * counted twice (it continues from the hit with tmin = next(t)) */
+  const V ng = cross(T.v2 - T.v0, T.v1 - T.v0);
+  const double den = dot(ng, d);
+  const double t = dot(ng, a) / den;
   if(!(t < h.t) || t <= eps || t <= tmin || T.gid == self.gid) return;
-  const int side = det < 0 ? 1 : 2;
+  const int side = den < 0 ? 1 : 2;
   if(!side_ok(S, T.sinst, side, self)) return;
   h.t = t; h.sinst = T.sinst; h.prim = T.prim; h.gid = T.gid;
-  h.n = cross(T.e2, T.e1); h.found = true;
+  h.n = ng; h.found = true;
 }
 
 unsigned grid_prim(const ssol_shape* s, double x, double y)
@@ -1627,6 +1654,7 @@ OHit trace(const Scene& S, V o, V d, double tmin, const Self& self, bool any)
   const V inv = v3(1 / d.x, 1 / d.y, 1 / d.z);
   const double am = std::max(std::fabs(o.x), std::max(std::fabs(o.y), std::fabs(o.z)));
   const double eps = 1e-6 * (1 + am);
+  const OShear sh = make_shear(d);
   int stack[128]; int sp = 0;
   stack[sp++] = 0;
   while(sp) {
@@ -1635,7 +1663,7 @@ OHit trace(const Scene& S, V o, V d, double tmin, const Self& self, bool any)
     if(n.left < 0) {
       for(int k = 0; k < n.count; ++k) {
         const int r = S.order[n.first + k];
-        if(r >= 0) hit_tri(S, r, o, d, tmin, eps, self, h);
+        if(r >= 0) hit_tri(S, r, o, d, sh, tmin, eps, self, h);
         else hit_quad(S, ~r, o, d, tmin, self, h);
         if(any && h.found) return h;
       }

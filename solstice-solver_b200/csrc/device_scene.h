@@ -121,10 +121,11 @@ struct DShadedInst {
   int32_t virtual_mask; /* bit0: front material virtual, bit1: back */
 };
 
-/* World-space triangle, stored as v0 and two edges. The front-face normal
- * follows Star-3D: Ng = (v2 - v0) x (v1 - v0) = e2 x e1. */
+/* World-space triangle, stored as its three vertices (the watertight test
+ * needs the shared vertices of neighbours bit-identical). The front-face
+ * normal follows Star-3D: Ng = (v2 - v0) x (v1 - v0) = e2 x e1. */
 template<typename R> struct alignas(16) DTri {
-  R v0[3]; R e1[3]; R e2[3];
+  R v0[3]; R v1[3]; R v2[3]; /* world vertices, FP32-rounded like Star-3D's */
   int32_t sinst; /* DShadedInst index */
   int32_t prim; /* triangle index inside its shape */
   int32_t gid; /* global triangle index (self-hit test) */

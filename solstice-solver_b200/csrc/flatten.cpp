@@ -423,8 +423,8 @@ static res_T flatten_impl
             /* Vertices go through FP32 like the reference's Star-3D scene */
             const R a = (R)vf[0][c], b = (R)vf[1][c], d = (R)vf[2][c];
             tri.v0[c] = a;
-            tri.e1[c] = b - a;
-            tri.e2[c] = d - a;
+            tri.v1[c] = b;
+            tri.v2[c] = d;
             box.lo[c] = std::min({(double)vf[0][c], (double)vf[1][c],
                                   (double)vf[2][c]});
             box.hi[c] = std::max({(double)vf[0][c], (double)vf[1][c],
@@ -450,8 +450,8 @@ static res_T flatten_impl
             const double len = std::sqrt(n[0]*n[0] + n[1]*n[1] + n[2]*n[2]);
             for(int c = 0; c < 3; ++c) {
               st.v0[c] = tri.v0[c];
-              st.e1[c] = tri.e1[c];
-              st.e2[c] = tri.e2[c];
+              st.e1[c] = tri.v1[c] - tri.v0[c];
+              st.e2[c] = tri.v2[c] - tri.v0[c];
               /* normalised in FP32 like f3_normalize */
               st.n[c] = (R)(float)(len > 0 ? n[c] / len : 0);
             }

@@ -453,34 +453,86 @@ __device__ __forceinline__ bool side_passes
   return true;
 }
 
-/* Mesh rule: reject t <= eps, t <= tmin and the starting triangle */
+/* Products and differences rounded on their own (no FMA contraction): the
+ * edge functions of the watertight test must be exact negations on an edge
+ * shared by two triangles */
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
+/* Per-ray shear of the watertight ray/triangle test (Woop, Benthin and Wald,
+ * "Watertight Ray/Triangle Intersection", JCGT 2(1), 2013): rows that map a
+ * vertex relative to the origin into a frame where the ray runs along +z,
+ * x' = v[kx] - Sx v[kz], y' = v[ky] - Sy v[kz], z' = Sz v[kz], with kz the
+ * dominant axis of the direction and kx, ky swapped when d[kz] < 0 so that
+ * the winding is kept. Applying the rows is deterministic per vertex, which
+ * is all watertightness needs. */
+template<class R> struct Shear { V3<R> rx, ry, rz; };
+
+template<class R>
+__device__ __forceinline__ Shear<R> make_shear(V3<R> d)
+{
+  const R ax = fabs(d.x), ay = fabs(d.y), az = fabs(d.z);
+  const int kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  int kx = kz == 2 ? 0 : kz + 1;
+  int ky = kx == 2 ? 0 : kx + 1;
+  const R dz = kz == 0 ? d.x : kz == 1 ? d.y : d.z;
+  if(dz < R(0)) { const int t = kx; kx = ky; ky = t; }
+  const R dx = kx == 0 ? d.x : kx == 1 ? d.y : d.z;
+  const R dy = ky == 0 ? d.x : ky == 1 ? d.y : d.z;
+  const R sx = dx / dz, sy = dy / dz, sz = R(1) / dz;
+  Shear<R> s;
+  s.rx = mk(kx == 0 ? R(1) : kz == 0 ? -sx : R(0),
+            kx == 1 ? R(1) : kz == 1 ? -sx : R(0),
+            kx == 2 ? R(1) : kz == 2 ? -sx : R(0));
+  s.ry = mk(ky == 0 ? R(1) : kz == 0 ? -sy : R(0),
+            ky == 1 ? R(1) : kz == 1 ? -sy : R(0),
+            ky == 2 ? R(1) : kz == 2 ? -sy : R(0));
+  s.rz = mk(kz == 0 ? sz : R(0), kz == 1 ? sz : R(0), kz == 2 ? sz : R(0));
+  return s;
+}
+
+template<class R>
+__device__ __forceinline__ R shear_row(V3<R> r, V3<R> a)
+{
+  return fma(r.z, a.z, fma(r.y, a.y, mul_rn(r.x, a.x)));
+}
+
+/* Mesh rule: reject t <= eps, t <= tmin and the starting triangle.
+ * Inclusion by the watertight edge functions, so that no ray is lost between
+ * two triangles; distance from the triangle's plane, dot(Ng, v0 - o) /
+ * dot(Ng, d), so that the two triangles of a planar quad give the same t and
+ * a ray crossing a virtual quad on its diagonal is not counted twice.
+ * Ng = e2 x e1 is Star-3D's front face. */
 template<class R>
 __device__ __forceinline__ void test_triangle
-  (const DScene<R>& S, int idx, V3<R> o, V3<R> d, R tmin, R eps,
-   const SelfInfo& self, Hit<R>& best, bool& found)
+  (const DScene<R>& S, int idx, V3<R> o, V3<R> d, const Shear<R>& sh, R tmin,
+   R eps, const SelfInfo& self, Hit<R>& best, bool& found)
 {
-  const DTri<R> T = S.tris[idx];
-  const V3<R> e1 = ld3(T.e1), e2 = ld3(T.e2);
-  const V3<R> p = cross(d, e2);
-  const R det = dot(e1, p);
-  if(det == R(0)) return;
-  const R inv = R(1) / det;
-  const V3<R> s = o - ld3(T.v0);
-  const R u = dot(s, p) * inv;
-  if(u < R(0) || u > R(1)) return;
-  const V3<R> qv = cross(s, e1);
-  const R v = dot(d, qv) * inv;
-  if(v < R(0) || u + v > R(1)) return;
-  const R t = dot(e2, qv) * inv;
+  const DTri<R>& T = S.tris[idx];
+  const V3<R> p0 = ld3(T.v0), p1 = ld3(T.v1), p2 = ld3(T.v2);
+  const V3<R> a = p0 - o, b = p1 - o, c = p2 - o;
+  const R ax = shear_row(sh.rx, a), ay = shear_row(sh.ry, a);
+  const R bx = shear_row(sh.rx, b), by = shear_row(sh.ry, b);
+  const R cx = shear_row(sh.rx, c), cy = shear_row(sh.ry, c);
+  const R u = sub_rn(mul_rn(cx, by), mul_rn(cy, bx));
+  const R v = sub_rn(mul_rn(ax, cy), mul_rn(ay, cx));
+  const R w = sub_rn(mul_rn(bx, ay), mul_rn(by, ax));
+  if((u < R(0) || v < R(0) || w < R(0)) && (u > R(0) || v > R(0) || w > R(0)))
+    return;
+  if(u + v + w == R(0)) return;
+  const V3<R> ng = cross(p2 - p0, p1 - p0);
+  const R den = dot(ng, d);
+  const R t = dot(ng, a) / den;
   if(!(t < best.t) || t <= eps || t <= tmin || T.gid == self.gid) return;
-  /* Ng = e2 x e1, so dot(Ng, d) = det */
-  const int side = det < R(0) ? 1 : 2;
+  const int side = den < R(0) ? 1 : 2;
   if(!side_passes(S, T.sinst, side, self)) return;
   best.t = t;
   best.sinst = T.sinst;
   best.prim = T.prim;
   best.gid = T.gid;
-  best.n = cross(e2, e1);
+  best.n = ng;
   found = true;
 }
 
@@ -581,6 +633,7 @@ __device__ bool trace_ray
    * magnitude of the origin so that it stays above the FP32 resolution */
   const R amax = fmax(fmax(fabs(o.x), fabs(o.y)), fabs(o.z));
   const R eps = R(1e-6) * (R(1) + amax);
+  const Shear<R> sh = make_shear(d);
   best.t = rmax<R>();
   bool found = false;
   int sp = 0;
@@ -603,8 +656,8 @@ __device__ bool trace_ray
           const uint32_t ref = S.primrefs[N.child[k] + p];
           if(primref_kind(ref) == PRIM_TRIANGLE) {
             ++cnt.tris;
-            test_triangle(S, (int)primref_index(ref), o, d, tmin, eps, self,
-                          best, found);
+            test_triangle(S, (int)primref_index(ref), o, d, sh, tmin, eps,
+                          self, best, found);
           } else {
             ++cnt.quads;
             test_quadric(S, (int)primref_index(ref), o, d, tmin, self,
@@ -1194,7 +1247,13 @@ realisation_kernel
     V3<R> pos = p.org, dir = -p.rd;
     if(p.phase == PH_SHADOW) {
       if(found) end = END_SHADOW;
-      else do_interact = true;
+      else {
+        /* The path starts at the sampled point along the sun direction; a
+         * virtual sampled surface pursues that ray (src/ssol_solver.c:
+         * 988-995), not the shadow ray */
+        p.rd = dir;
+        do_interact = true;
+      }
     } else if(p.phase == PH_BOUNCE) {
       if(!found) {
         /* Last segment: the medium the ray leaves into must be the air
@@ -1280,7 +1339,7 @@ batch_kernel
    const unsigned long long* __restrict__ prefix,
    const unsigned long long* __restrict__ firsts, int nitems, uint64_t seed,
    unsigned long long max_segments, unsigned long long* next_path,
-   DStats* stats)
+   DStats* stats, int rcvd)
 {
   extern __shared__ double smem[];
   const int bd = blockDim.x, tid = threadIdx.x;
@@ -1290,6 +1349,18 @@ batch_kernel
   int* stack = reinterpret_cast<int*>(smem + (2 * NGLOBAL + PS_COUNT) * bd) + tid;
   for(int q = 0; q < 2 * NGLOBAL; ++q) acc[q * bd] = 0;
   int acc_item = -1;
+  /* Receiver sums: every path adds to the same few addresses of its item,
+   * so they are gathered per warp in two shared-memory slots tagged with an
+   * item (the warp's current item and the previous one, for the paths still
+   * running across an item boundary) and flushed to the item's tallies when
+   * the warp moves on. Tags change only where the warp is converged. */
+  double* wslots = reinterpret_cast<double*>(
+    reinterpret_cast<int*>(smem + (2 * NGLOBAL + PS_COUNT) * bd) + STACK_SIZE * bd)
+    + (size_t)(tid >> 5) * 2 * rcvd;
+  for(int i = (int)lane; i < 2 * rcvd; i += 32) wslots[i] = 0;
+  __syncwarp();
+  int stag[2] = {-1, -1};
+  int cur = 0;
 
   const unsigned long long count = prefix[nitems];
   Rng rng;
@@ -1339,6 +1410,25 @@ batch_kernel
           ++npaths;
         }
       }
+      if(rcvd) {
+        /* Converged: the newest item fetched becomes the current slot */
+        const bool fetched = (need >> lane) & 1u && !done;
+        const int newest = __reduce_max_sync(0xffffffffu, fetched ? it : -1);
+        if(newest >= 0 && newest != stag[cur]) {
+          const int prv = cur ^ 1;
+          double* sl = wslots + prv * rcvd;
+          __syncwarp();
+          if(stag[prv] >= 0) {
+            double* dst = tallies[stag[prv]].rcv;
+            const int nd = scenes[stag[prv]].nrcv * NRCV_Q * 2;
+            for(int i = (int)lane; i < nd; i += 32) red_add(dst + i, sl[i]);
+          }
+          for(int i = (int)lane; i < rcvd; i += 32) sl[i] = 0;
+          __syncwarp();
+          stag[prv] = newest;
+          cur = prv;
+        }
+      }
     }
     if(!__any_sync(0xffffffffu, p.phase != PH_NONE)) break;
 
@@ -1361,7 +1451,13 @@ batch_kernel
     V3<R> pos = p.org, dir = -p.rd;
     if(p.phase == PH_SHADOW) {
       if(found) end = END_SHADOW;
-      else do_interact = true;
+      else {
+        /* The path starts at the sampled point along the sun direction; a
+         * virtual sampled surface pursues that ray (src/ssol_solver.c:
+         * 988-995), not the shadow ray */
+        p.rd = dir;
+        do_interact = true;
+      }
     } else if(p.phase == PH_BOUNCE) {
       if(!found) {
         if(p.out_medium != S.air_medium) {
@@ -1402,7 +1498,12 @@ batch_kernel
     if(do_interact)
       end = interact(S, rng, p, pos, dir, bounces, max_segments, ps, bd, xr, xp, xv);
     if(end != END_NONE) {
-      commit_path(S, tallies[it], p, end, acc, ps, bd, nullptr, xr, xp, xv);
+      double* rb = nullptr;
+      if(rcvd) {
+        if(it == stag[cur]) rb = wslots + cur * rcvd;
+        else if(it == stag[cur ^ 1]) rb = wslots + (cur ^ 1) * rcvd;
+      }
+      commit_path(S, tallies[it], p, end, acc, ps, bd, rb, xr, xp, xv);
       p.phase = PH_NONE;
     }
   }
@@ -1410,6 +1511,13 @@ batch_kernel
   if(acc_item >= 0) {
     for(int q = 0; q < 2 * NGLOBAL; ++q)
       red_add(tallies[acc_item].global + q, acc[q * bd]);
+  }
+  __syncwarp();
+  for(int k = 0; k < 2 && rcvd; ++k) {
+    if(stag[k] < 0) continue;
+    double* dst = tallies[stag[k]].rcv;
+    const int nd = scenes[stag[k]].nrcv * NRCV_Q * 2;
+    for(int i = (int)lane; i < nd; i += 32) red_add(dst + i, wslots[k * rcvd + i]);
   }
   unsigned long long c[6] = {cnt.rays, cnt.nodes, cnt.tris, cnt.quads,
                              bounces, npaths};
@@ -1487,7 +1595,8 @@ static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg
   const int block = cfg.block_size > 0 ? cfg.block_size : MAX_BLOCK;
   if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
   const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block) * sizeof(double)
-                    + (size_t)STACK_SIZE * block * sizeof(int);
+                    + (size_t)STACK_SIZE * block * sizeof(int)
+                    + (size_t)(block / 32) * 2 * cfg.rcv_doubles * sizeof(double);
   static bool attr_set = false;
   if(!attr_set) {
     cudaFuncSetAttribute(batch_kernel<R, MINB>,
@@ -1504,7 +1613,7 @@ static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg
   cudaMemsetAsync(b.next_path, 0, sizeof(unsigned long long), (cudaStream_t)stream);
   batch_kernel<R, MINB><<<(unsigned)blocks, block, smem, (cudaStream_t)stream>>>
     (b.scenes, b.tallies, b.prefix, b.firsts, b.nitems, b.seed, cfg.max_segments,
-     b.next_path, b.stats);
+     b.next_path, b.stats, cfg.rcv_doubles);
   return (int)cudaGetLastError();
 }
 
@@ -1578,7 +1687,8 @@ static int launch_batch_noalloc_variant
   const int block = cfg.block_size > 0 ? cfg.block_size : MAX_BLOCK;
   if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
   const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block) * sizeof(double)
-                    + (size_t)STACK_SIZE * block * sizeof(int);
+                    + (size_t)STACK_SIZE * block * sizeof(int)
+                    + (size_t)(block / 32) * 2 * cfg.rcv_doubles * sizeof(double);
   cudaFuncSetAttribute(batch_kernel<R, MINB>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
   int per_sm = 0;
@@ -1605,7 +1715,7 @@ static int launch_batch_noalloc_variant
   batch_kernel<R, MINB><<<(unsigned)blocks, block, smem, s>>>
     (scenes, tallies, scratch + NOALLOC_PREFIX, scratch + NOALLOC_FIRSTS, nitems,
      seed, cfg.max_segments, scratch + NOALLOC_NEXT,
-     reinterpret_cast<DStats*>(scratch + NOALLOC_STATS));
+     reinterpret_cast<DStats*>(scratch + NOALLOC_STATS), cfg.rcv_doubles);
   return (int)cudaGetLastError();
 }
 

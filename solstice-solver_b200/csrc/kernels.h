@@ -16,6 +16,9 @@ struct LaunchConfig {
   int waves; /* persistent grid multiplier, 0 => 1 */
   unsigned long long max_segments; /* per path segment budget */
   int min_blocks; /* register budget: 1 (255 regs), 2 (128) or 3 (85) */
+  int rcv_doubles = 0; /* batched launches: largest item receiver-sum array
+                        * (nrcv x 10 x 2); 0 => receiver sums go straight
+                        * to device memory */
 };
 
 /* Enqueue the realisations [first, first + count) of the stream keyed by

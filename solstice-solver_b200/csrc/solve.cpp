@@ -16,6 +16,8 @@
 
 #include <cuda_runtime_api.h>
 
+#include <algorithm>
+#include <cfloat>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -579,6 +581,56 @@ extern "C" res_T ssol_b200_plan_finish
                         p->kernel_ms, p->scene_bytes, max_failed, out);
 }
 
+extern "C" res_T ssol_b200_autotune
+  (ssol_scene* scn, const ssp_rng* rng, const uint64_t trial_paths,
+   ssol_b200_options* options, double* best_ms)
+{
+  if(!scn || !rng || !options || !trial_paths) return RES_BAD_ARG;
+  static const int leaves[] = {1, 2, 4};
+  static const int blocks[] = {128, 256};
+  static const int budgets[] = {1, 2, 3};
+  static const int waves[] = {1, 2};
+  const ssol_b200_options base = *options;
+  ssol_b200_options best_opt = base;
+  double best = DBL_MAX;
+  for(const int leaf : leaves) {
+    ssol_b200_options o = base;
+    o.bvh_leaf_size = leaf;
+    o.grid_blocks = 0;
+    ssol_b200_plan* plan = nullptr;
+    res_T res = ssol_b200_plan_create(scn, &o, &plan);
+    if(res != RES_OK) return res;
+    const cudaStream_t s = plan_stream(plan, nullptr);
+    for(const int blk : blocks)
+      for(const int mb : budgets)
+        for(const int wv : waves) {
+          plan->opt.block_size = blk;
+          plan->opt.min_blocks_per_sm = mb;
+          plan->opt.waves = wv;
+          float ms = 0;
+          for(int k = 0; k < 2 && res == RES_OK; ++k) {
+            res = ssol_b200_plan_launch(plan, rng, 0, trial_paths, s);
+            if(res == RES_OK && cudaStreamSynchronize(s) != cudaSuccess)
+              res = RES_UNKNOWN_ERR;
+            if(res == RES_OK && k == 1
+            && cudaEventElapsedTime(&ms, plan->ev0, plan->ev1) != cudaSuccess)
+              res = RES_UNKNOWN_ERR;
+          }
+          if(res != RES_OK) { ssol_b200_plan_ref_put(plan); return res; }
+          if(ms < best) {
+            best = ms;
+            best_opt = plan->opt;
+          }
+        }
+    ssol_b200_plan_ref_put(plan);
+  }
+  best_opt.precision = base.precision;
+  best_opt.max_segments = base.max_segments;
+  *options = best_opt;
+  if(best_ms) *best_ms = best;
+  return RES_OK;
+}
+
 extern "C" res_T ssol_b200_plan_get_stats
   (const ssol_b200_plan* p, ssol_b200_stats* s)
 {
@@ -801,17 +853,30 @@ extern "C" res_T ssol_b200_batch_reset(ssol_b200_batch* b, void* stream)
 
 /* The captured graph: work-counter reset + the persistent batch kernel. Its
  * parameters are device pointers only, so one capture serves every launch */
-static res_T batch_graph(ssol_b200_batch* b, const ssp_rng* rng, cudaStream_t s)
+/* Launch shape of a batch; receiver sums are gathered per warp in shared
+ * memory when two slots of the largest item fit in 16 KB per block */
+static LaunchConfig batch_config(const ssol_b200_batch* b)
 {
-  if(b->graph_exec && b->graph_stream == s) return RES_OK;
-  if(b->graph_exec) { cudaGraphExecDestroy(b->graph_exec); b->graph_exec = nullptr; }
-  if(b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
   LaunchConfig cfg;
   cfg.block_size = b->opt.block_size;
   cfg.grid_blocks = b->opt.grid_blocks;
   cfg.waves = b->opt.waves;
   cfg.max_segments = b->opt.max_segments;
   cfg.min_blocks = b->opt.min_blocks_per_sm;
+  size_t nrcv = 0;
+  for(const FlatMeta& m : b->meta) nrcv = std::max(nrcv, m.rcv.size());
+  const size_t rcvd = nrcv * NRCV_Q * 2;
+  const size_t warps = (size_t)(cfg.block_size > 0 ? cfg.block_size : 256) / 32;
+  cfg.rcv_doubles = warps * 2 * rcvd * sizeof(double) <= 16 * 1024 ? (int)rcvd : 0;
+  return cfg;
+}
+
+static res_T batch_graph(ssol_b200_batch* b, const ssp_rng* rng, cudaStream_t s)
+{
+  if(b->graph_exec && b->graph_stream == s) return RES_OK;
+  if(b->graph_exec) { cudaGraphExecDestroy(b->graph_exec); b->graph_exec = nullptr; }
+  if(b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+  const LaunchConfig cfg = batch_config(b);
   if(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     return RES_UNKNOWN_ERR;
   int err;
@@ -894,12 +959,7 @@ extern "C" res_T ssol_b200_batch_launch_noalloc
   b->h_prefix[n] = total;
   if(!total) return RES_OK;
   const cudaStream_t s = stream ? (cudaStream_t)stream : (cudaStream_t)b->dev->stream;
-  LaunchConfig cfg;
-  cfg.block_size = b->opt.block_size;
-  cfg.grid_blocks = b->opt.grid_blocks;
-  cfg.waves = b->opt.waves;
-  cfg.max_segments = b->opt.max_segments;
-  cfg.min_blocks = b->opt.min_blocks_per_sm;
+  const LaunchConfig cfg = batch_config(b);
   const int err = b->opt.precision == SSOL_B200_FP32
     ? launch_batch_noalloc_f32((const DScene<float>*)b->d_scenes, b->d_tallies,
                                (int)n, rng->seed, b->h_prefix.data(),

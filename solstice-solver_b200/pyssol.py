@@ -224,6 +224,8 @@ _OPTIONAL = {
     "ssol_b200_batch_launch": [VP, VP, C.POINTER(C.c_uint64), VP],
     "ssol_b200_batch_finish": [VP, VP, C.c_size_t, VP, PVP],
     "ssol_b200_batch_launch_noalloc": [VP, VP, C.POINTER(C.c_uint64), VP],
+    "ssol_b200_autotune": [VP, VP, C.c_uint64, C.POINTER(B200Options),
+                           C.POINTER(C.c_double)],
 }
 
 
@@ -660,6 +662,17 @@ def options(precision=FP32, block_size=256, grid_blocks=0, waves=1, leaf=0,
     o.max_segments = max_segments
     o.min_blocks_per_sm = min_blocks
     return o
+
+
+def autotune(scene, trial_paths=4_000_000, opts=None, seed=0):
+    """Fastest launch shape and BVH leaf size for `scene` (ssol_b200_autotune);
+    returns (options, best_ms)."""
+    o = opts if opts is not None else options()
+    best = C.c_double()
+    rng = scene.rng(seed=seed)
+    scene.lib.call("ssol_b200_autotune", scene.scn, rng, int(trial_paths), C.byref(o),
+                   C.byref(best))
+    return o, best.value
 
 
 def load_product(path=PRODUCT_LIB):

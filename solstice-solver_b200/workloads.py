@@ -193,3 +193,82 @@ def batched_fields(lib, suns, n_helio=1000, receiver_cells=64):
                                receiver_cells=receiver_cells)
         out.append((s, h))
     return out
+
+
+# --------------------------------------------------------------- config 4
+def surround_layout(n=5000, r_min=40.0, spacing=12.0, dr=10.0, height=4.0):
+    """Radial-staggered surround field (full circle), nearest rows first:
+    rows every `dr` metres from r_min, floor(2 pi r / spacing) positions per
+    row, odd rows shifted by half a step, truncated to n positions."""
+    pts = []
+    k = 0
+    rr = r_min
+    while len(pts) < n:
+        m = int(2 * math.pi * rr / spacing)
+        off = 0.5 if k % 2 else 0.0
+        for i in range(m):
+            phi = 2 * math.pi * (i + off) / m
+            pts.append((rr * math.sin(phi), rr * math.cos(phi), height))
+        k += 1
+        rr += dr
+    return pts[:n]
+
+
+def beam_down(lib, n_helio=5000, elevation=60.0, azimuth=180.0, dni=1000.0,
+              sun_sigma=2.5e-3, secondary_height=120.0, image_focal=10.0,
+              secondary_half=20.0, receiver_cells=30):
+    """Beam-down tower: 5000 punched paraboloid heliostats, a hyperboloid
+    secondary and a ground receiver under a glass window.
+
+    Heliostats: 8x8 m punched paraboloids on surround_layout() (r <= 800 m;
+    about 440 m for 5000), focal length = slant range from the heliostat
+    centre to the secondary's vertex, each normal bisecting the to-sun
+    direction and the direction to the hyperboloid's image focus; front:
+    specular mirror reflectivity 0.9, back: absorbing matte.
+    Secondary: punched hyperboloid, vertex at `secondary_height`, real focal
+    length = secondary_height (real focus on the ground at the receiver),
+    image focal length `image_focal` (image focus at 130 m), carved
+    2 secondary_half = 40 m square;
+    front (facing the ground): mirror reflectivity 0.95 with a pillbox
+    microfacet slope distribution of 1.5 mrad; back: absorbing matte.
+    Receiver: 6x6 m on the ground (front up), matte reflectivity 0.1
+    (absorptivity 0.9), receiver_cells^2 quads with per-primitive tallies.
+    Window: 6.5x6.5 m thin dielectric (n 1.5, absorption 20 /m, 5 mm) 0.5 m
+    above the receiver, both sides. Sun: Gaussian sigma 2.5 mrad at
+    (elevation, azimuth), DNI 1000, no atmosphere. Only the heliostats are
+    sampled.
+    """
+    s = P.Scene(lib)
+    sun = to_sun(elevation, azimuth)
+    f2 = (0.0, 0.0, secondary_height + image_focal)
+    vertex = (0.0, 0.0, secondary_height)
+    pts = surround_layout(n_helio)
+    front = s.mirror(0.9, 0.0)
+    back = s.matte(0.0)
+    carve = [(P.SSOL_AND, [(-4, -4), (-4, 4), (4, 4), (4, -4)])]
+    helios = []
+    for p in pts:
+        a = _unit((f2[0] - p[0], f2[1] - p[1], f2[2] - p[2]))
+        n = _unit((sun[0] + a[0], sun[1] + a[1], sun[2] + a[2]))
+        focal = math.sqrt(sum((vertex[c] - p[c]) ** 2 for c in range(3)))
+        shape = s.punched(P.Q_PARABOL, (focal,), carve)
+        helios.append(s.instance(s.object([(shape, front, back)]),
+                                 P.transform_from(frame_z_to(n), p)))
+    q = secondary_half
+    hyp = s.punched(P.Q_HYPERBOL, (image_focal, secondary_height),
+                    [(P.SSOL_AND, [(-q, -q), (-q, q), (q, q), (q, -q)])])
+    sec_mtl = s.mirror(0.95, 1.5e-3, P.PILLBOX)
+    secondary = s.instance(s.object([(hyp, sec_mtl, back)]),
+                           P.transform_from(None, vertex), sample=0)
+    rshape = grid_mesh(s, 6.0, 6.0, receiver_cells, receiver_cells)
+    rmtl = s.matte(0.1)
+    receiver = s.instance(s.object([(rshape, rmtl, rmtl)]), receiver=P.SSOL_FRONT,
+                          per_primitive=1, sample=0)
+    air = s.medium(0.0, 1.0)
+    glass = s.medium(20.0, 1.5)
+    win_mtl = s.thin_dielectric(air, glass, 5e-3)
+    window = s.instance(s.object([(s.rectangle(3.25, 3.25), win_mtl, win_mtl)]),
+                        P.transform_from(None, (0.0, 0.0, 0.5)), sample=0)
+    s.set_sun("gaussian", tuple(-x for x in sun), dni, param=sun_sigma)
+    return s, {"heliostats": helios, "secondary": secondary, "receiver": receiver,
+               "receiver_shape": rshape, "window": window, "positions": pts, "sun": sun}

@@ -49,3 +49,19 @@ def test_batch_matches_plain_solves(product):
     for est, n in zip(again, budgets):
         assert est.count("realisation_count") == n
     batch.close()
+
+
+def test_autotune_picks_a_valid_shape(product):
+    """ssol_b200_autotune returns one of its candidate shapes, and a solve
+    with it agrees with the default shape within 3 combined SE."""
+    s, h = W.heliostat_field(product, n_helio=120, receiver_cells=16)
+    opt, ms = P.autotune(s, 500000)
+    assert ms > 0
+    assert opt.block_size in (128, 256)
+    assert opt.min_blocks_per_sm in (1, 2, 3)
+    assert opt.waves in (1, 2)
+    assert opt.bvh_leaf_size in (1, 2, 4)
+    a = s.solve(2000000, seed=4, options=opt).globals()
+    b = s.solve(2000000, seed=4).globals()
+    for k in b:
+        assert P.combined_ok(a[k], b[k], floor=1e-6 * abs(b[k][0])), k

@@ -19,7 +19,7 @@ import workloads as W
 pytestmark = pytest.mark.gpu
 
 K = 3.0
-REL_FLOOR = 1e-6  # FP32 geometry on zero-variance estimates (north_star: <= 1e-5)
+REL_FLOOR = 1e-6  # FP32 geometry on zero-variance estimates (the stated FP32 bound is 1e-5)
 
 
 def close(a, b):
