@@ -36,6 +36,13 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
             "map, pillbox sun 4.65 mrad el 30 az 180 DNI 900, extinction 1e-4/m")
 
 
+# DRAM bytes per path of the realisation kernel, from ncu captures of 4e6-path
+# launches of the same scenes (dram__bytes_read.sum + dram__bytes_write.sum);
+# the traffic scales with the paths traced (per-thread frames written back)
+DRAM_BYTES_PER_PATH = {"field": (34.2e6 + 349.3e6) / 4e6,
+                       "beamdown": (65.1e6 + 178.1e6) / 4e6}
+
+
 def flops_per_run(st):
     """Algorithmic FP32 work model: 20 FLOP per child slab test (2 per node),
     55 per triangle test, 90 per quadric test, 150 per shaded bounce, 120 per
@@ -232,7 +239,8 @@ def run_b200(args):
     sp = P.C.c_void_p(stream.cuda_stream)
     assert sp.value, "expected a non-default CUDA stream"
     n = args.paths
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = torch.empty(max(1, args.flush_mib) * 1024 * 1024 // 4, dtype=torch.float32,
+                        device="cuda")
 
     def step(k):
         first = (k * world + rank) * n
@@ -240,7 +248,8 @@ def run_b200(args):
 
     for w in range(args.warmup):
         step(w)
-        flush.zero_()
+        if args.flush_mib:
+            flush.zero_()
     lib.call("ssol_b200_plan_reset", plan, sp)
     torch.cuda.synchronize()
     if dist:
@@ -257,7 +266,8 @@ def run_b200(args):
         kev[k][0].record(stream)
         step(args.warmup + k)
         kev[k][1].record(stream)
-        flush.zero_()
+        if args.flush_mib:
+            flush.zero_()
     ev1.record(stream)
     torch.cuda.synchronize()
     if dist:
@@ -316,7 +326,8 @@ def run_b200(args):
         "data": "synthetic (seeded generator, no public scene)",
         "config": {"workload": desc, "paths_per_step": n, "precision":
                    "FP64" if args.fp64 else "FP32 geometry/BSDF, FP64 tallies",
-                   "l2": "flushed: 256 MiB write between steps (scene < 2 MB)",
+                   "l2": ("flushed: %d MiB write between steps (scene < 2 MB)" % args.flush_mib
+                          if args.flush_mib else "not flushed (profiling run)"),
                    "parallelism": "realisation ranges per GPU" if world > 1 else "1 GPU",
                    "launch": launch_shape},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
@@ -325,7 +336,10 @@ def run_b200(args):
         "gpu_launches": args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak else None,
-                     "traffic": None,
+                     "traffic": (DRAM_BYTES_PER_PATH[args.config] * n
+                                 if args.config in DRAM_BYTES_PER_PATH else None),
+                     "traffic_source": "ncu dram__bytes_read+write of a 4e6-path launch, "
+                                       "scaled to paths_per_step (bytes per launch)",
                      "peak_source": "SMs x 128 FP32 lanes x 2 x measured max SM clock "
                                     "(MEASURED_PEAKS.json sm_max_mhz)",
                      "work_model": "20/slab x2 per node + 55/triangle + 90/quadric + "
@@ -398,7 +412,8 @@ def run_suns(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     sp = P.C.c_void_p(stream.cuda_stream)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = torch.empty(max(1, args.flush_mib) * 1024 * 1024 // 4, dtype=torch.float32,
+                        device="cuda")
     rng = scenes[0].rng(seed=args.seed)
 
     # pilot
@@ -545,13 +560,100 @@ def run_suns(args):
         dist.destroy_process_group()
 
 
+ADJOINT = ("aim gradients (ssol_solve_adjoint) on the 1000-heliostat field: 2000 aim "
+           "angles (2 per heliostat), objectives first-bounce absorbed power and spillage "
+           "sum_c (map - uniform target)^2 on a 64x64 map of the 12x12 receiver")
+
+
+def run_adjoint(args):
+    """Adjoint of the field's first-bounce flux map w.r.t. every heliostat's two
+    aim angles. value: Mpaths/s of the two replayed passes (CUDA-event time of
+    the kernels, scene resident); e2e: wall clock of the synchronous call
+    (snapshot, upload, both passes, read-back). Then central finite differences
+    with common random numbers on 32 seeded random parameters, at h = 1e-4
+    and 1e-3 rad, and the relative error of the adjoint against them (the
+    bias of the shadowing, blocking and receiver-edge terms it leaves out)."""
+    import random
+    import torch
+    import pyssol as P
+    import workloads as W
+    import adjoint as A
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    lib = P.load_product()
+    s, h = W.heliostat_field(lib, n_helio=args.heliostats)
+    lower, upper, nx, ny = (-6.0, -6.0), (6.0, 6.0), 64, 64
+    n = args.paths
+    opt = P.options(P.FP64 if args.fp64 else P.FP32)
+    base = A.solve_adjoint(s, h["heliostats"], h["receiver"], lower, upper, nx, ny, 0.0,
+                           n, seed=args.seed, options=opt, want_map=True)
+    target = sum(base["map"]) / len(base["map"])
+    for w in range(args.warmup):
+        A.solve_adjoint(s, h["heliostats"], h["receiver"], lower, upper, nx, ny, target,
+                        n, seed=args.seed + 1 + w, options=opt)
+    clocks = Clocks(local)
+    clocks.start()
+    kms, t0 = 0.0, time.perf_counter()
+    for k in range(args.steps):
+        r = A.solve_adjoint(s, h["heliostats"], h["receiver"], lower, upper, nx, ny, target,
+                            n, seed=args.seed + 100 + k, options=opt)
+        kms += r["kernel_ms"]
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    value = args.steps * n / (kms * 1e-3) / 1e6
+    e2e = args.steps * n / wall / 1e6
+
+    fd = {}
+    if args.fd_params > 0:
+        field = A.AimField(s, h["heliostats"], h["transforms"], h["receiver"], lower, upper,
+                           nx, ny, target, args.fd_paths, seed=args.seed + 7, options=opt)
+        rnd = random.Random(args.seed)
+        params = [(rnd.randrange(len(h["heliostats"])), rnd.randrange(2))
+                  for _ in range(args.fd_params)]
+        for step in (1e-4, 1e-3):
+            _, rows = A.finite_difference_check(field, params, h=step)
+            out = {}
+            for key in ("spillage", "absorbed"):
+                a = [row["adjoint_" + key] for row in rows]
+                b = [row["fd_" + key] for row in rows]
+                nb = math.sqrt(sum(x * x for x in b)) or 1.0
+                na = math.sqrt(sum(x * x for x in a)) or 1.0
+                out[key] = {"rel_l2_error": math.sqrt(sum((x - y) ** 2 for x, y in zip(a, b)))
+                            / nb,
+                            "cosine": sum(x * y for x, y in zip(a, b)) / (na * nb)}
+            fd["h=%g" % step] = out
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": kms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32",
+        "data": "synthetic (seeded generator, no public scene)",
+        "config": {"workload": ADJOINT, "paths_per_step": n, "parameters": 2 * len(
+            h["heliostats"]), "passes": 2, "map": "64x64 over 12x12, bilinear splat",
+            "l2": "not flushed (scene < 2 MB; the map and gradients are rewritten)"},
+        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": (nx * ny + 4 * len(h["heliostats"])) * 8,
+                "timing": "wall clock around the synchronous ssol_solve_adjoint"},
+        "gpu_launches": 2 * args.steps,
+        "objective": {"absorbed_W": base["absorbed"], "spillage": base["spillage"],
+                      "target_W_m2": target},
+        "fd_check": {"params": args.fd_params, "paths": args.fd_paths,
+                     "common_random_numbers": True, **fd},
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--config", default="field", choices=["field", "mirror", "beamdown", "suns"])
+    p.add_argument("--config", default="field",
+                   choices=["field", "mirror", "beamdown", "suns", "adjoint"])
+    p.add_argument("--fd-params", type=int, default=32)
+    p.add_argument("--fd-paths", type=int, default=100_000_000)
     p.add_argument("--heliostats", type=int, default=1000)
     p.add_argument("--paths", type=int, default=None,
                    help="realisations per step (field 1e8, beamdown 2e8, mirror 1e6)")
@@ -564,6 +666,8 @@ def main():
     p.add_argument("--no-autotune", dest="autotune", action="store_false",
                    help="use --block/--minb/--waves/--leaf as given")
     p.add_argument("--autotune-paths", type=int, default=4_000_000)
+    p.add_argument("--flush-mib", type=int, default=256,
+                   help="L2 flush buffer written between steps (profiling: 0)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -576,6 +680,8 @@ def main():
         run_reference(args)
     elif args.config == "suns":
         run_suns(args)
+    elif args.config == "adjoint":
+        run_adjoint(args)
     else:
         run_b200(args)
 

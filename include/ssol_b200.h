@@ -106,6 +106,47 @@ SSOL_API res_T ssol_b200_autotune
   (struct ssol_scene* scn, const struct ssp_rng* rng, const uint64_t trial_paths,
    struct ssol_b200_options* options, double* best_ms);
 
+/* Adjoint (no counterpart in the reference): gradients of a receiver flux
+ * objective with respect to the aim of heliostats.
+ *
+ * Only first-bounce paths count: sampled on a mirror, not shadowed, reflected
+ * once and reaching the `receiver` first on a receiving side with a mirror or
+ * matte material. Their weight w there includes the atmosphere and the
+ * receiver's absorptivity. Objectives:
+ *   absorbed = (1/N) sum w                               (W)
+ *   spillage = sum_c (M_c - target)^2                    (W^2/m^4)
+ * M_c is the flux density of cell c of an nx x ny grid over
+ * [lower, upper] in the receiver's local x, y, each hit splatted with
+ * bilinear weights on the cell centres. Parameters: for each listed
+ * heliostat, rotations theta_x, theta_y about its instance's local x and y
+ * axes through its translation, at theta = 0. Gradients follow the paths
+ * (reparameterised sampling, replayed from the Philox keys of `rng`); the
+ * changes of shadowing, blocking and the receiver's edges are not
+ * differentiated. */
+struct ssol_b200_adjoint_map {
+  struct ssol_instance* receiver; /* a mesh instance */
+  double lower[2], upper[2]; /* receiver-local x, y extent of the grid */
+  unsigned nx, ny;
+  double target; /* uniform target flux density, W/m^2 */
+};
+
+struct ssol_b200_adjoint_result {
+  double absorbed, absorbed_se; /* first-bounce absorbed power and its SE */
+  double spillage;
+  unsigned long long hits; /* first-bounce paths that reached the receiver */
+  double kernel_ms; /* both passes */
+};
+
+/* d_absorbed and d_spillage receive 2 x nheliostats values (theta_x, theta_y
+ * of each listed heliostat, in order) and may be NULL when nheliostats is 0;
+ * flux_map (optional) receives the nx x ny flux densities, row by row. */
+SSOL_API res_T ssol_solve_adjoint
+  (struct ssol_scene* scn, const struct ssp_rng* rng, const size_t realisations_count,
+   struct ssol_instance* const* heliostats, const size_t nheliostats,
+   const struct ssol_b200_adjoint_map* map, const struct ssol_b200_options* options,
+   struct ssol_b200_adjoint_result* result, double* d_absorbed, double* d_spillage,
+   double* flux_map);
+
 /* Batches: several scenes (typically one per sun position, each with its own
  * re-aimed field and sun) traced by one persistent kernel launch replayed
  * from a captured CUDA graph, each item with its own budget and tallies */

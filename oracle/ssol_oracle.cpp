@@ -2107,6 +2107,107 @@ API res_T ssol_solve(ssol_scene* scn, const ssp_rng* rng, const size_t n,
   return RES_OK;
 }
 
+/* Oracle of the primal objective of the B200 library's ssol_solve_adjoint
+ * (no reference counterpart; test infrastructure only): first-bounce paths
+ * sampled on a mirror, not shadowed, reflected once (shade(), scatter event
+ * 0) and reaching `receiver` first on a receiving side whose material is a
+ * mirror or matte; weight w0 x reflectivity x exp(-k t) x (1 - receiver
+ * reflectivity); absorbed = mean of w, flux_map = bilinear splat of w on the
+ * nx x ny cell centres of [lower, upper] in the receiver's local frame,
+ * divided by N and the cell area. */
+API res_T ssol_oracle_first_bounce
+  (ssol_scene* scn, const ssp_rng* rng, const size_t n, const ssol_instance* receiver,
+   const double lower[2], const double upper[2], const unsigned nx, const unsigned ny,
+   double* absorbed, double* absorbed_se, unsigned long long* hits, double* flux_map)
+{
+  if(!scn || !rng || !n || !receiver || !lower || !upper || !nx || !ny || !absorbed
+  || !absorbed_se || !hits || !flux_map) return RES_BAD_ARG;
+  Scene S;
+  res_T res = make_scene(scn, S);
+  if(res != RES_OK) return res;
+  Affine rxf, rinv;
+  rxf = receiver->xf;
+  if(!inverse(rxf, rinv)) return RES_BAD_ARG;
+  const double cw = (upper[0] - lower[0]) / nx, ch = (upper[1] - lower[1]) / ny;
+  const int nth = (int)scn->dev->nthreads;
+  std::vector<std::vector<double>> maps(nth, std::vector<double>((size_t)nx * ny, 0.0));
+  std::vector<double> sw(nth, 0.0), sw2(nth, 0.0), sh(nth, 0.0);
+  const int64_t N = (int64_t)n;
+  #pragma omp parallel for schedule(static) num_threads(nth)
+  for(int64_t i = 0; i < N; ++i) {
+    const int th = omp_get_thread_num();
+    const PathRng rg = {rng->pos + (uint64_t)i, rng->seed};
+    const Block r0 = rg.get(0, DOM_PRIMARY);
+    int k = (int)(((uint64_t)(r0.x[0] >> 8) * (uint64_t)S.samp.size()) >> 24);
+    if(!((float)unif(r0.x[1]) < S.aprob[k])) k = S.aidx[k];
+    const OSamp& st = S.samp[k];
+    const double sa = std::sqrt(unif(r0.x[2]));
+    const double b2 = sa * unif(r0.x[3]), b1 = sa - b2;
+    V pos = st.v0 + st.e1 * b1 + st.e2 * b2;
+    const Block r1 = rg.get(1, DOM_PRIMARY);
+    const V dir = sun_dir(S, rg, r1);
+    const double wl = wl_sample(S, unif(r1.x[2]));
+    const OSInst* o = &S.sinst[st.sinst];
+    V N = st.n;
+    if(o->punched) {
+      const OQuad& Q = S.quads[o->quad];
+      V pl = xpoint(Q.w2l, pos);
+      pl.z = qz(o->shape->quad.type, o->shape->q, pl.x, pl.y);
+      N = unit(xvec_t(Q.w2l, qgrad(o->shape->quad.type, o->shape->q, pl)));
+      pos = xpoint(Q.l2w, pl);
+    }
+    int side = 1;
+    if(!(dot(N, dir) < 0)) { side = 2; N = -N; }
+    const ssol_material* mtl = o->mtl[side - 1];
+    if(mtl->type != SSOL_MATERIAL_MIRROR) continue;
+    const double spc = o->punched ? std::fabs(dot(st.n, N)) : 1.0;
+    double w = S.sun->dni * S.area_proxy
+      * std::fabs(dot(N, dir) / (spc * dot(S.sun_dir, dir)));
+    const Self self = {st.gid, st.sinst, side, true, true};
+    if(trace(S, pos, -dir, 0, self, true).found) continue;
+    ssol_medium in = S.air, out = S.air;
+    double prop; V rd = dir; int type;
+    if(!shade(S, rg, 0, mtl, in, out, wl, -dir, N, prop, rd, type) || !(prop > 0)) continue;
+    w *= prop;
+    const Self s2 = {st.gid, st.sinst, side, false, false};
+    const OHit h = trace(S, pos, rd, 0, s2, false);
+    if(!h.found) continue;
+    const OSInst& hs = S.sinst[h.sinst];
+    if(hs.inst != receiver || hs.punched) continue;
+    const int hside = dot(rd, h.n) < 0 ? 1 : 2;
+    if(!(receiver->mask & hside)) continue;
+    const ssol_material* hm = hs.mtl[hside - 1];
+    if(hm->type != SSOL_MATERIAL_MIRROR && hm->type != SSOL_MATERIAL_MATTE) continue;
+    const double kext = data_value(S.air.extinction, wl);
+    if(kext > 0) w *= std::exp(-kext * h.t);
+    w *= 1 - shader(S, hm, 0, wl);
+    sw[th] += w; sw2[th] += w * w; sh[th] += 1;
+    const V p = pos + rd * h.t;
+    const V pl = xpoint(rinv, p);
+    const double fx = (pl.x - lower[0]) / cw - 0.5, fy = (pl.y - lower[1]) / ch - 0.5;
+    const int i0 = (int)std::floor(fx), j0 = (int)std::floor(fy);
+    const double tx = fx - i0, ty = fy - j0;
+    for(int dj = 0; dj < 2; ++dj)
+      for(int di = 0; di < 2; ++di) {
+        const int ci = i0 + di, cj = j0 + dj;
+        if(ci < 0 || cj < 0 || ci >= (int)nx || cj >= (int)ny) continue;
+        maps[th][(size_t)cj * nx + ci] += w * (di ? tx : 1 - tx) * (dj ? ty : 1 - ty);
+      }
+  }
+  double a = 0, a2 = 0, hh = 0;
+  for(int t = 0; t < nth; ++t) { a += sw[t]; a2 += sw2[t]; hh += sh[t]; }
+  const double mean = a / (double)n;
+  *absorbed = mean;
+  *absorbed_se = std::sqrt(std::max(0.0, a2 / (double)n - mean * mean) / (double)n);
+  *hits = (unsigned long long)hh;
+  for(size_t c = 0; c < (size_t)nx * ny; ++c) {
+    double v = 0;
+    for(int t = 0; t < nth; ++t) v += maps[t][c];
+    flux_map[c] = v / ((double)n * cw * ch);
+  }
+  return RES_OK;
+}
+
 /*******************************************************************************
  * Estimator read-out (src/ssol_estimator.c, src/ssol_mc_receiver.c)
  ******************************************************************************/

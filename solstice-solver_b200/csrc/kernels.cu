@@ -1763,4 +1763,6 @@ int launch_realisations_f64
    uint64_t count, const LaunchConfig& cfg, void* stream)
 { return launch_impl<double>(S, T, seed, first, count, cfg, stream); }
 
+#include "adjoint.cuh"
+
 } /* namespace ssolb */

@@ -67,6 +67,36 @@ int launch_batch_noalloc_f64
 int launch_batch_f64(const BatchLaunch<double>& b, const LaunchConfig& cfg,
                      void* stream);
 
+/* Arguments of the adjoint passes (adjoint.cuh). Device pointers: inst_slot
+ * (parameter slot per instance, -1 if none), axes (per slot: centre, e_x,
+ * e_y), map (nx * ny cell sums of pass 0, read by pass 1), sums (sum w,
+ * sum w^2, hits), grad_abs and grad_spill (2 per slot), counters (rays,
+ * nodes, triangles, quadrics). */
+struct AdjointArgs {
+  const int* inst_slot;
+  const double* axes;
+  int rcv_instance;
+  double w2l[8]; /* rows x and y of the receiver's world -> local transform */
+  double lower[2], inv_cell[2];
+  int nx, ny;
+  double* map;
+  double* sums;
+  double* grad_abs;
+  double* grad_spill;
+  unsigned long long* counters;
+  double target; /* uniform target flux density */
+  double inv_n; /* 1 / realisations */
+  double map_scale; /* 1 / (realisations x cell area) */
+};
+
+/* One adjoint pass (0: objective and map, 1: gradients) */
+int launch_adjoint_f32
+  (const DScene<float>& S, const AdjointArgs& A, uint64_t seed, uint64_t first,
+   uint64_t count, int pass, void* stream);
+int launch_adjoint_f64
+  (const DScene<double>& S, const AdjointArgs& A, uint64_t seed, uint64_t first,
+   uint64_t count, int pass, void* stream);
+
 } /* namespace ssolb */
 
 #endif /* SSOL_B200_KERNELS_H */

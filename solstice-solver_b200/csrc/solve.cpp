@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -628,6 +629,156 @@ extern "C" res_T ssol_b200_autotune
   best_opt.max_segments = base.max_segments;
   *options = best_opt;
   if(best_ms) *best_ms = best;
+  return RES_OK;
+}
+
+/* Affine inverse of a 3x4 column-major transform (rotation/scale + translation) */
+static bool invert_affine(const double* T, double* W)
+{
+  const double a = T[0], b = T[3], c = T[6];
+  const double d = T[1], e = T[4], f = T[7];
+  const double g = T[2], h = T[5], i = T[8];
+  const double det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+  if(!(std::fabs(det) > 0)) return false;
+  const double inv[9] = {(e * i - f * h) / det, (c * h - b * i) / det, (b * f - c * e) / det,
+                         (f * g - d * i) / det, (a * i - c * g) / det, (c * d - a * f) / det,
+                         (d * h - e * g) / det, (b * g - a * h) / det, (a * e - b * d) / det};
+  /* W row-major 3x4: local = inv (x - t) */
+  for(int r = 0; r < 3; ++r) {
+    W[4 * r + 0] = inv[3 * r + 0];
+    W[4 * r + 1] = inv[3 * r + 1];
+    W[4 * r + 2] = inv[3 * r + 2];
+    W[4 * r + 3] = -(inv[3 * r + 0] * T[9] + inv[3 * r + 1] * T[10] + inv[3 * r + 2] * T[11]);
+  }
+  return true;
+}
+
+extern "C" res_T ssol_solve_adjoint
+  (ssol_scene* scn, const ssp_rng* rng, const size_t n,
+   ssol_instance* const* helios, const size_t nh, const ssol_b200_adjoint_map* map,
+   const ssol_b200_options* options, ssol_b200_adjoint_result* result,
+   double* d_absorbed, double* d_spillage, double* flux_map)
+{
+  if(!scn || !rng || !n || !map || !map->receiver || !result) return RES_BAD_ARG;
+  if(nh && (!helios || !d_absorbed || !d_spillage)) return RES_BAD_ARG;
+  if(!map->nx || !map->ny || !(map->upper[0] > map->lower[0])
+  || !(map->upper[1] > map->lower[1]))
+    return RES_BAD_ARG;
+  /* Instance indices in attach order, as the device scene numbers them */
+  const std::vector<ssol_instance*>& insts = scn->instances;
+  int rcv_index = -1;
+  std::vector<int> slot(insts.size(), -1);
+  for(size_t i = 0; i < insts.size(); ++i)
+    if(insts[i] == map->receiver) rcv_index = (int)i;
+  if(rcv_index < 0) return RES_BAD_ARG;
+  std::vector<double> axes(9 * nh);
+  for(size_t k = 0; k < nh; ++k) {
+    size_t i = 0;
+    while(i < insts.size() && insts[i] != helios[k]) ++i;
+    if(i == insts.size() || slot[i] >= 0 || (int)i == rcv_index) return RES_BAD_ARG;
+    slot[i] = (int)k;
+    const double* T = helios[k]->transform;
+    double* a = axes.data() + 9 * k;
+    a[0] = T[9]; a[1] = T[10]; a[2] = T[11];
+    for(int c = 0; c < 2; ++c) {
+      const double* col = T + 3 * c;
+      const double len = std::sqrt(col[0] * col[0] + col[1] * col[1] + col[2] * col[2]);
+      if(!(len > 0)) return RES_BAD_ARG;
+      for(int q = 0; q < 3; ++q) a[3 + 3 * c + q] = col[q] / len;
+    }
+  }
+  double W[12];
+  if(!invert_affine(map->receiver->transform, W)) return RES_BAD_ARG;
+
+  ssol_b200_plan* plan = nullptr;
+  res_T res = ssol_b200_plan_create(scn, options, &plan);
+  if(res != RES_OK) return res;
+  const cudaStream_t s = plan_stream(plan, nullptr);
+  const size_t ncell = (size_t)map->nx * map->ny;
+  const size_t bytes = (insts.size() * sizeof(int) + 255) / 256 * 256
+    + (9 * nh + ncell + 3 + 4 * nh) * sizeof(double) + 4 * sizeof(unsigned long long);
+  char* dbuf = nullptr;
+  if(cudaMalloc((void**)&dbuf, bytes) != cudaSuccess) {
+    ssol_b200_plan_ref_put(plan);
+    return RES_MEM_ERR;
+  }
+  int* d_slot = reinterpret_cast<int*>(dbuf);
+  double* d_axes = reinterpret_cast<double*>(dbuf + (insts.size() * sizeof(int) + 255) / 256 * 256);
+  double* d_map = d_axes + 9 * nh;
+  double* d_sums = d_map + ncell;
+  double* d_gabs = d_sums + 3;
+  double* d_gspill = d_gabs + 2 * nh;
+  unsigned long long* d_cnt = reinterpret_cast<unsigned long long*>(d_gspill + 2 * nh);
+
+  AdjointArgs A;
+  A.inst_slot = d_slot;
+  A.axes = d_axes;
+  A.rcv_instance = rcv_index;
+  for(int q = 0; q < 8; ++q) A.w2l[q] = W[q];
+  const double cw = (map->upper[0] - map->lower[0]) / map->nx;
+  const double ch = (map->upper[1] - map->lower[1]) / map->ny;
+  A.lower[0] = map->lower[0];
+  A.lower[1] = map->lower[1];
+  A.inv_cell[0] = 1.0 / cw;
+  A.inv_cell[1] = 1.0 / ch;
+  A.nx = (int)map->nx;
+  A.ny = (int)map->ny;
+  A.map = d_map;
+  A.sums = d_sums;
+  A.grad_abs = d_gabs;
+  A.grad_spill = d_gspill;
+  A.counters = d_cnt;
+  A.target = map->target;
+  A.inv_n = 1.0 / (double)n;
+  A.map_scale = 1.0 / ((double)n * cw * ch);
+
+  std::vector<double> h_map(ncell), h_sums(3);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  bool ok = cudaMemsetAsync(dbuf, 0, bytes, s) == cudaSuccess
+    && cudaMemcpyAsync(d_slot, slot.data(), insts.size() * sizeof(int),
+                       cudaMemcpyHostToDevice, s) == cudaSuccess
+    && (!nh || cudaMemcpyAsync(d_axes, axes.data(), 9 * nh * sizeof(double),
+                               cudaMemcpyHostToDevice, s) == cudaSuccess)
+    && cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess
+    && cudaEventRecord(e0, s) == cudaSuccess;
+  const bool f32 = plan->opt.precision == SSOL_B200_FP32;
+  for(int pass = 0; ok && pass < (nh ? 2 : 1); ++pass) {
+    const int err = f32
+      ? launch_adjoint_f32(plan->s32, A, rng->seed, rng->position, n, pass, s)
+      : launch_adjoint_f64(plan->s64, A, rng->seed, rng->position, n, pass, s);
+    ok = err == 0;
+  }
+  ok = ok && cudaEventRecord(e1, s) == cudaSuccess
+    && cudaMemcpyAsync(h_map.data(), d_map, ncell * sizeof(double),
+                       cudaMemcpyDeviceToHost, s) == cudaSuccess
+    && cudaMemcpyAsync(h_sums.data(), d_sums, 3 * sizeof(double),
+                       cudaMemcpyDeviceToHost, s) == cudaSuccess
+    && (!nh || (cudaMemcpyAsync(d_absorbed, d_gabs, 2 * nh * sizeof(double),
+                                cudaMemcpyDeviceToHost, s) == cudaSuccess
+             && cudaMemcpyAsync(d_spillage, d_gspill, 2 * nh * sizeof(double),
+                                cudaMemcpyDeviceToHost, s) == cudaSuccess))
+    && cudaStreamSynchronize(s) == cudaSuccess;
+  float ms = 0;
+  if(ok) cudaEventElapsedTime(&ms, e0, e1);
+  if(e0) cudaEventDestroy(e0);
+  if(e1) cudaEventDestroy(e1);
+  cudaFree(dbuf);
+  ssol_b200_plan_ref_put(plan);
+  if(!ok) return RES_UNKNOWN_ERR;
+
+  const double mean = h_sums[0] / (double)n;
+  const double var = std::max(0.0, h_sums[1] / (double)n - mean * mean);
+  result->absorbed = mean;
+  result->absorbed_se = std::sqrt(var / (double)n);
+  result->hits = (unsigned long long)h_sums[2];
+  result->kernel_ms = ms;
+  double spill = 0;
+  for(size_t c = 0; c < ncell; ++c) {
+    const double m = h_map[c] * A.map_scale;
+    spill += (m - map->target) * (m - map->target);
+    if(flux_map) flux_map[c] = m;
+  }
+  result->spillage = spill;
   return RES_OK;
 }
 

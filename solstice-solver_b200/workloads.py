@@ -142,11 +142,12 @@ def heliostat_field(lib, n_helio=1000, elevation=30.0, azimuth=180.0, dni=900.0,
     front = s.mirror(0.9, slope_error, P.BECKMANN)
     back = s.matte(0.0)
     hobj = s.object([(helio_shape, front, back)])
-    helios = []
+    helios, xfs = [], []
     for p in pts:
         a = _unit((aim[0] - p[0], aim[1] - p[1], aim[2] - p[2]))
         n = _unit((sun[0] + a[0], sun[1] + a[1], sun[2] + a[2]))
-        helios.append(s.instance(hobj, P.transform_from(frame_z_to(n), p)))
+        xfs.append(P.transform_from(frame_z_to(n), p))
+        helios.append(s.instance(hobj, xfs[-1]))
     cx = sum(p[0] for p in pts) / len(pts)
     cy = sum(p[1] for p in pts) / len(pts)
     cz = sum(p[2] for p in pts) / len(pts)
@@ -159,8 +160,8 @@ def heliostat_field(lib, n_helio=1000, elevation=30.0, azimuth=180.0, dni=900.0,
     s.set_sun("pillbox", tuple(-x for x in sun), dni, param=4.65e-3)
     if extinction:
         s.atmosphere(extinction)
-    return s, {"heliostats": helios, "receiver": rcv, "receiver_shape": rshape,
-               "positions": pts, "sun": sun}
+    return s, {"heliostats": helios, "transforms": xfs, "receiver": rcv,
+               "receiver_shape": rshape, "positions": pts, "sun": sun}
 
 
 # --------------------------------------------------------------- config 3
