@@ -1891,8 +1891,19 @@ McRcv1& rcv_side(std::map<const ssol_instance*, McRcv>& m, const ssol_instance* 
 { return m[i].side[side == 1 ? 0 : 1]; }
 
 /* One realisation (trace_radiative_path, src/ssol_solver.c:873-1127) */
-res_T realisation(const Scene& S, Ctx& ctx, size_t ireal, const PathRng& rng)
+/* Tracked-path lengths after the defaults (src/ssol_solver.c:1211-1220) */
+struct TrackLen { double sun, inf; };
+
+res_T realisation(const Scene& S, Ctx& ctx, size_t ireal, const PathRng& rng,
+                  const TrackLen* track = nullptr, OPath* path = nullptr)
 {
+  bool hit_rcv = false;
+  auto vtx = [&](V p, double w) {
+    if(!path) return;
+    ssol_path_vertex v;
+    v.pos[0] = p.x; v.pos[1] = p.y; v.pos[2] = p.z; v.weight = w;
+    path->v.push_back(v);
+  };
   /* point_init */
   const Block r0 = rng.get(0, DOM_PRIMARY);
   int k = (int)(((uint64_t)(r0.x[0] >> 8) * (uint64_t)S.samp.size()) >> 24);
@@ -1932,6 +1943,11 @@ res_T realisation(const Scene& S, Ctx& ctx, size_t ireal, const PathRng& rng)
     ssol_medium_copy(&in, side == 1 ? &mtl->in : &mtl->out);
   else ssol_medium_copy(&in, &S.air);
 
+  /* Tracked path: the sun end, then the sampled point (src/ssol_solver.c:909-922) */
+  if(path) {
+    if(track->sun > 0) vtx(pos - dir * track->sun, S.sun->dni);
+    vtx(pos, w0);
+  }
   Self self = {gid, si, side, true, true};
   OHit h = trace(S, pos, -dir, 0, self, true);
   int score = 0;
@@ -1940,6 +1956,7 @@ res_T realisation(const Scene& S, Ctx& ctx, size_t ireal, const PathRng& rng)
   if(h.found) {
     ms.shadow.add(ireal, w0);
     ctx.g[2].add(ireal, w0);
+    if(path) path->type = SSOL_PATH_SHADOW;
   } else {
     double prev[3] = {w0, w0, w0}, inc[3], outw[3] = {0, 0, 0};
     double hit_t = 0, tmin = 0;
@@ -1973,6 +1990,7 @@ res_T realisation(const Scene& S, Ctx& ctx, size_t ireal, const PathRng& rng)
         if(type) dir = nd;
       }
       if(is_rcv) {
+        hit_rcv = true;
         /* update_mc (src/ssol_solver.c:708-785) */
         ctx.g[1].add(ireal, inc[0] - outw[0]);
         const double w[10] = {inc[0], inc[1], inc[2], inc[2] - inc[0], inc[1] - inc[0],
@@ -1997,6 +2015,7 @@ res_T realisation(const Scene& S, Ctx& ctx, size_t ireal, const PathRng& rng)
         Self s2 = {gid, si, side, false, false};
         h = trace(S, org, rd, tmin, s2, false);
         if(!h.found) {
+          if(path && track->inf > 0) vtx(pos + rd * track->inf, outw[0]);
           last = true;
           if(!media_ceq(out, S.air)) { res = RES_BAD_OP; break; }
         }
@@ -2018,6 +2037,7 @@ res_T realisation(const Scene& S, Ctx& ctx, size_t ireal, const PathRng& rng)
       si = h.sinst; o = &S.sinst[si]; prim = h.prim; gid = h.gid;
       N = unit(h.n);
       pos = org + rd * h.t;
+      vtx(pos, outw[0]);
       side = dot(rd, N) < 0 ? 1 : 2;
       if(side == 2) N = -N;
       mtl = o->mtl[side - 1];
@@ -2025,7 +2045,10 @@ res_T realisation(const Scene& S, Ctx& ctx, size_t ireal, const PathRng& rng)
       ssol_medium_copy(&in, &out);
     }
     if(res == RES_OK && !killed) ctx.g[3].add(ireal, outw[0]);
+    if(path) path->type = hit_rcv ? SSOL_PATH_SUCCESS : SSOL_PATH_MISSING;
   }
+  if(path && res != RES_OK) path->type = SSOL_PATH_ERROR;
+  if(path && killed) path->v.clear(), path->type = (ssol_path_type)-1;
   ssol_medium_clear(&in);
   ssol_medium_clear(&out);
   if(res != RES_OK) return res;
@@ -2054,7 +2077,7 @@ void merge_rcv(McRcv& dst, McRcv& src, const ssol_instance* inst)
 
 /* ssol_solve (src/ssol_solver.c:1132-1361) */
 API res_T ssol_solve(ssol_scene* scn, const ssp_rng* rng, const size_t n,
-                     const size_t max_failed, const ssol_path_tracker*,
+                     const size_t max_failed, const ssol_path_tracker* tracker,
                      ssol_estimator** out)
 {
   if(!scn || !rng || !n || !out) return RES_BAD_ARG;
@@ -2066,12 +2089,26 @@ API res_T ssol_solve(ssol_scene* scn, const ssp_rng* rng, const size_t n,
   std::atomic<size_t> nfail{0};
   std::atomic<int> stop{0};
   const int64_t N = (int64_t)n;
+  /* Path tracking (src/ssol_solver.c:1211-1220): negative lengths default to
+   * 0.75 x the largest extent of the scene's bounding box. The first
+   * min(N, 2^20) realisations are tracked, in realisation order. */
+  TrackLen tl = {0, 0};
+  std::vector<OPath> paths;
+  if(tracker) {
+    double ext = 0;
+    for(int c = 0; c < 3; ++c) ext = std::max(ext, S.nodes[0].hi[c] - S.nodes[0].lo[c]);
+    ext *= 0.75;
+    tl.sun = tracker->sun_ray_length < 0 ? ext : tracker->sun_ray_length;
+    tl.inf = tracker->infinite_ray_length < 0 ? ext : tracker->infinite_ray_length;
+    paths.resize((size_t)std::min<int64_t>(N, int64_t(1) << 20));
+  }
   #pragma omp parallel for schedule(static) num_threads(nth)
   for(int64_t i = 0; i < N; ++i) {
     if(stop.load()) continue;
     Ctx& c = ctx[omp_get_thread_num()];
     PathRng pr = {rng->pos + (uint64_t)i, rng->seed};
-    const res_T r = realisation(S, c, (size_t)i, pr);
+    OPath* pp = (size_t)i < paths.size() ? &paths[(size_t)i] : nullptr;
+    const res_T r = realisation(S, c, (size_t)i, pr, &tl, pp);
     if(r != RES_OK) {
       apply_factor(c, (size_t)i, 0);
       if(r == RES_BAD_OP) {
@@ -2100,6 +2137,8 @@ API res_T ssol_solve(ssol_scene* scn, const ssp_rng* rng, const size_t n,
     }
   }
   e->sampled_area = S.area_rt;
+  for(OPath& p : paths)
+    if((int)p.type >= 0 && !p.v.empty()) e->paths.push_back(std::move(p));
   e->rng = new ssp_rng();
   e->rng->type = rng->type; e->rng->seed = rng->seed; e->rng->pos = rng->pos + n;
   *out = e;
@@ -2294,6 +2333,34 @@ API res_T ssol_estimator_get_rng_state(const ssol_estimator* e, const ssp_rng** 
 { if(!e || !r) return RES_BAD_ARG; *r = e->rng; return RES_OK; }
 API res_T ssol_estimator_get_tracked_paths_count(const ssol_estimator* e, size_t* n)
 { if(!e || !n) return RES_BAD_ARG; *n = e->paths.size(); return RES_OK; }
+/* src/ssol_estimator.c:280-322 */
+API res_T ssol_estimator_get_tracked_path(const ssol_estimator* e, const size_t i,
+                                          ssol_path* p)
+{
+  if(!e || i >= e->paths.size() || !p) return RES_BAD_ARG;
+  p->path__ = &e->paths[i];
+  return RES_OK;
+}
+API res_T ssol_path_get_vertices_count(const ssol_path* p, size_t* n)
+{
+  if(!p || !n) return RES_BAD_ARG;
+  *n = static_cast<const OPath*>(p->path__)->v.size();
+  return RES_OK;
+}
+API res_T ssol_path_get_vertex(const ssol_path* p, const size_t i, ssol_path_vertex* v)
+{
+  if(!p || !v) return RES_BAD_ARG;
+  const OPath* o = static_cast<const OPath*>(p->path__);
+  if(i >= o->v.size()) return RES_BAD_ARG;
+  *v = o->v[i];
+  return RES_OK;
+}
+API res_T ssol_path_get_type(const ssol_path* p, ssol_path_type* t)
+{
+  if(!p || !t) return RES_BAD_ARG;
+  *t = static_cast<const OPath*>(p->path__)->type;
+  return RES_OK;
+}
 API res_T ssol_mc_receiver_get_mc_shape(ssol_mc_receiver* rcv, const ssol_shape* s,
                                         ssol_mc_shape* mc)
 {

@@ -240,6 +240,25 @@ struct DTallies {
   DStats* stats;
 };
 
+/* Path tracking (ssol_path_tracker): the realisations of launch index
+ * below npaths record their vertices, each appended through a counter with
+ * its path slot and its rank in the path; the host groups them back */
+struct TrackVertex {
+  uint32_t slot, seq;
+  double pos[3];
+  double weight;
+};
+
+struct DTrack {
+  TrackVertex* verts;
+  unsigned long long* nverts; /* vertices appended (may exceed cap) */
+  unsigned long long cap; /* capacity of verts */
+  int32_t* path_type; /* per slot: ssol_path_type, -1 if not registered */
+  int32_t* path_nv; /* per slot: vertices the path produced */
+  unsigned long long npaths; /* tracked launch indices [0, npaths) */
+  double sun_len, inf_len; /* lengths of the sun and infinite segments */
+};
+
 } /* namespace ssolb */
 
 #endif /* SSOL_B200_DEVICE_SCENE_H */

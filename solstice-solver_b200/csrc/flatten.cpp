@@ -5,6 +5,7 @@
 #include "tessellate.h"
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <limits>
 #include <map>
@@ -596,6 +597,17 @@ static res_T flatten_impl
   if(!has_receiver) dev->log_warning("No receiver is defined.\n");
 
   build_alias(samp_area, out.alias_prob, out.alias_idx);
+  /* Bounding box of the ray-traced geometry (src/ssol_solver.c:563-570 uses
+   * the scene view's box for the tracked segments to and from infinity) */
+  for(int c = 0; c < 3; ++c) {
+    out.meta.aabb_lo[c] = boxes.empty() ? 0.0 : DBL_MAX;
+    out.meta.aabb_hi[c] = boxes.empty() ? 0.0 : -DBL_MAX;
+  }
+  for(const PrimBox& b : boxes)
+    for(int c = 0; c < 3; ++c) {
+      out.meta.aabb_lo[c] = std::min(out.meta.aabb_lo[c], b.lo[c]);
+      out.meta.aabb_hi[c] = std::max(out.meta.aabb_hi[c], b.hi[c]);
+    }
   build_bvh(boxes, bvh_params, out.bvh);
   out.nodes = bvh_nodes<R>(out.bvh);
   return RES_OK;

@@ -37,6 +37,7 @@ struct FlatMeta {
   double sampled_area = 0;
   double sampled_area_proxy = 0;
   size_t scene_bytes = 0; /* bytes uploaded to the device */
+  double aabb_lo[3] = {0, 0, 0}, aabb_hi[3] = {0, 0, 0}; /* ray-traced geometry */
 };
 
 template<class R> struct FlatScene {

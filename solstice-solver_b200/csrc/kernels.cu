@@ -875,6 +875,8 @@ __device__ __noinline__ void commit10(double* dst, const double v[6], double f)
 template<class R> struct PathState {
   int phase;
   int samp;
+  int tslot; /* tracked path slot, -1 if not tracked */
+  uint32_t tseq; /* vertices recorded so far */
   /* current point / ray: the point is org (+ rd t after a hit) */
   int sinst, side, prim, gid, medium, out_medium;
   V3<R> N, org, rd;
@@ -1168,12 +1170,32 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 constexpr int SMEM_RCV_MAX = 16;
 constexpr int MAX_BLOCK = 256;
 
-template<class R, int MINB>
+/* Append one vertex of a tracked path (src/ssol_solver.c:909-922, 1014-1019,
+ * 1080-1083: the sun end, the sampled point, every hit and the end at
+ * infinity, each with the flux carried to it) */
+template<class R>
+__device__ __forceinline__ void track_vertex
+  (const DTrack& tr, PathState<R>& p, V3<R> x, double w)
+{
+  const unsigned long long k = atomicAdd(tr.nverts, 1ull);
+  if(k < tr.cap) {
+    TrackVertex& v = tr.verts[k];
+    v.slot = (uint32_t)p.tslot;
+    v.seq = p.tseq;
+    v.pos[0] = (double)x.x;
+    v.pos[1] = (double)x.y;
+    v.pos[2] = (double)x.z;
+    v.weight = w;
+  }
+  ++p.tseq;
+}
+
+template<class R, int MINB, bool TRACK>
 __global__ void __launch_bounds__(MAX_BLOCK, MINB)
 realisation_kernel
   (const DScene<R> S, const DTallies T, uint64_t seed, uint64_t first,
    uint64_t count, unsigned long long max_segments,
-   unsigned long long* next_path)
+   unsigned long long* next_path, const DTrack tr)
 {
   /* Shared memory: per-thread FP64 global sums [12][blockDim], per-thread
    * path sums [10][blockDim], the receiver-side sums, the per-thread
@@ -1223,6 +1245,15 @@ realisation_kernel
           rng.i_hi = (uint32_t)(id >> 32);
           init_path(S, rng, p, ps, bd);
           ++npaths;
+          if(TRACK) {
+            p.tslot = idx < tr.npaths ? (int)idx : -1;
+            p.tseq = 0;
+            if(p.tslot >= 0) {
+              if(tr.sun_len > 0)
+                track_vertex(tr, p, p.org + p.rd * (R)tr.sun_len, S.dni);
+              track_vertex(tr, p, p.org, p.prev[0]);
+            }
+          }
         }
       }
     }
@@ -1256,6 +1287,10 @@ realisation_kernel
       }
     } else if(p.phase == PH_BOUNCE) {
       if(!found) {
+        if(TRACK && p.tslot >= 0 && tr.inf_len > 0) {
+          const V3<R> last = p.virt ? p.org + p.rd * p.hit_t : p.org;
+          track_vertex(tr, p, last + p.rd * (R)tr.inf_len, p.virt ? p.inc0 : p.prev[0]);
+        }
         /* Last segment: the medium the ray leaves into must be the air
          * (src/ssol_solver.c:1012-1032) */
         if(p.out_medium != S.air_medium) {
@@ -1287,6 +1322,8 @@ realisation_kernel
           dir = p.rd;
           p.N = normalize(h.n);
           pos = p.org + p.rd * h.t;
+          if(TRACK && p.tslot >= 0)
+            track_vertex(tr, p, pos, p.virt ? p.inc0 : p.prev[0]);
           p.side = dot(p.rd, p.N) < R(0) ? 1 : 2;
           if(p.side == 2) p.N = -p.N;
           p.hit_t = h.t;
@@ -1298,6 +1335,13 @@ realisation_kernel
     if(do_interact)
       end = interact(S, rng, p, pos, dir, bounces, max_segments, ps, bd, xr, xp, xv);
     if(end != END_NONE) {
+      if(TRACK && p.tslot >= 0 && end != END_KILL) {
+        /* src/ssol_solver.c:931, 1092-1094, 1122-1125; killed paths are not
+         * registered (1111) */
+        tr.path_type[p.tslot] = end == END_SHADOW ? 1
+          : (end == END_FAIL || p.overflow) ? 3 : (p.nent > 0 ? 2 : 0);
+        tr.path_nv[p.tslot] = (int32_t)p.tseq;
+      }
       commit_path(S, T, p, end, acc, ps, bd, smem_rcv, xr, xp, xv);
       p.phase = PH_NONE;
     }
@@ -1531,10 +1575,10 @@ batch_kernel
 /*******************************************************************************
  * Host launchers
  ******************************************************************************/
-template<class R, int MINB>
+template<class R, int MINB, bool TRACK>
 static int launch_variant
   (const DScene<R>& S, const DTallies& T, uint64_t seed, uint64_t first,
-   uint64_t count, const LaunchConfig& cfg, void* stream)
+   uint64_t count, const LaunchConfig& cfg, void* stream, const DTrack& tr)
 {
   int dev = 0;
   cudaGetDevice(&dev);
@@ -1548,13 +1592,13 @@ static int launch_variant
                     + (size_t)STACK_SIZE * block * sizeof(int);
   static bool attr_set = false;
   if(!attr_set) {
-    cudaFuncSetAttribute(realisation_kernel<R, MINB>,
+    cudaFuncSetAttribute(realisation_kernel<R, MINB, TRACK>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
     attr_set = true;
   }
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor
-    (&per_sm, realisation_kernel<R, MINB>, block, smem);
+    (&per_sm, realisation_kernel<R, MINB, TRACK>, block, smem);
   if(per_sm < 1) per_sm = 1;
   uint64_t blocks = cfg.grid_blocks > 0
     ? (uint64_t)cfg.grid_blocks
@@ -1565,9 +1609,9 @@ static int launch_variant
   /* Work counter of this launch: counters[3] */
   cudaMemsetAsync(T.counters + 3, 0, sizeof(unsigned long long),
                   (cudaStream_t)stream);
-  realisation_kernel<R, MINB><<<(unsigned)blocks, block, smem,
-                                (cudaStream_t)stream>>>
-    (S, T, seed, first, count, cfg.max_segments, T.counters + 3);
+  realisation_kernel<R, MINB, TRACK><<<(unsigned)blocks, block, smem,
+                                       (cudaStream_t)stream>>>
+    (S, T, seed, first, count, cfg.max_segments, T.counters + 3, tr);
   return (int)cudaGetLastError();
 }
 
@@ -1575,12 +1619,14 @@ static int launch_variant
 template<class R>
 static int launch_impl
   (const DScene<R>& S, const DTallies& T, uint64_t seed, uint64_t first,
-   uint64_t count, const LaunchConfig& cfg, void* stream)
+   uint64_t count, const LaunchConfig& cfg, void* stream, const DTrack* track)
 {
+  if(track) return launch_variant<R, 2, true>(S, T, seed, first, count, cfg, stream, *track);
+  const DTrack none = {};
   switch(cfg.min_blocks) {
-    case 1: return launch_variant<R, 1>(S, T, seed, first, count, cfg, stream);
-    case 3: return launch_variant<R, 3>(S, T, seed, first, count, cfg, stream);
-    default: return launch_variant<R, 2>(S, T, seed, first, count, cfg, stream);
+    case 1: return launch_variant<R, 1, false>(S, T, seed, first, count, cfg, stream, none);
+    case 3: return launch_variant<R, 3, false>(S, T, seed, first, count, cfg, stream, none);
+    default: return launch_variant<R, 2, false>(S, T, seed, first, count, cfg, stream, none);
   }
 }
 
@@ -1755,13 +1801,13 @@ int launch_batch_noalloc_f64
 
 int launch_realisations_f32
   (const DScene<float>& S, const DTallies& T, uint64_t seed, uint64_t first,
-   uint64_t count, const LaunchConfig& cfg, void* stream)
-{ return launch_impl<float>(S, T, seed, first, count, cfg, stream); }
+   uint64_t count, const LaunchConfig& cfg, void* stream, const DTrack* track)
+{ return launch_impl<float>(S, T, seed, first, count, cfg, stream, track); }
 
 int launch_realisations_f64
   (const DScene<double>& S, const DTallies& T, uint64_t seed, uint64_t first,
-   uint64_t count, const LaunchConfig& cfg, void* stream)
-{ return launch_impl<double>(S, T, seed, first, count, cfg, stream); }
+   uint64_t count, const LaunchConfig& cfg, void* stream, const DTrack* track)
+{ return launch_impl<double>(S, T, seed, first, count, cfg, stream, track); }
 
 #include "adjoint.cuh"
 

@@ -22,14 +22,17 @@ struct LaunchConfig {
 };
 
 /* Enqueue the realisations [first, first + count) of the stream keyed by
- * `seed` on `stream` (a cudaStream_t); tallies accumulate into T. Returns a
- * cudaError_t value. */
+ * `seed` on `stream` (a cudaStream_t); tallies accumulate into T; `track`
+ * (may be NULL) records the paths of the first track->npaths of them.
+ * Returns a cudaError_t value. */
 int launch_realisations_f32
   (const DScene<float>& S, const DTallies& T, uint64_t seed, uint64_t first,
-   uint64_t count, const LaunchConfig& cfg, void* stream);
+   uint64_t count, const LaunchConfig& cfg, void* stream,
+   const DTrack* track = nullptr);
 int launch_realisations_f64
   (const DScene<double>& S, const DTallies& T, uint64_t seed, uint64_t first,
-   uint64_t count, const LaunchConfig& cfg, void* stream);
+   uint64_t count, const LaunchConfig& cfg, void* stream,
+   const DTrack* track = nullptr);
 
 /* Batched launch: device arrays of per-item scenes and tallies, the item
  * budgets as an inclusive prefix (nitems + 1 entries; the last one is the

@@ -521,9 +521,9 @@ extern "C" res_T ssol_b200_plan_reset(ssol_b200_plan* p, void* stream)
   return RES_OK;
 }
 
-extern "C" res_T ssol_b200_plan_launch
+static res_T plan_launch
   (ssol_b200_plan* p, const ssp_rng* rng, const uint64_t first,
-   const uint64_t count, void* stream)
+   const uint64_t count, void* stream, const DTrack* track)
 {
   if(!p || !rng) return RES_BAD_ARG;
   if(!count) return RES_OK;
@@ -537,8 +537,8 @@ extern "C" res_T ssol_b200_plan_launch
   const uint64_t start = rng->position + first;
   cudaEventRecord(p->ev0, s);
   const int err = p->opt.precision == SSOL_B200_FP32
-    ? launch_realisations_f32(p->s32, p->t, rng->seed, start, count, cfg, s)
-    : launch_realisations_f64(p->s64, p->t, rng->seed, start, count, cfg, s);
+    ? launch_realisations_f32(p->s32, p->t, rng->seed, start, count, cfg, s, track)
+    : launch_realisations_f64(p->s64, p->t, rng->seed, start, count, cfg, s, track);
   cudaEventRecord(p->ev1, s);
   if(err != 0) {
     p->dev->log_error("kernel launch failed: %s\n",
@@ -547,6 +547,13 @@ extern "C" res_T ssol_b200_plan_launch
   }
   p->timing_valid = true;
   return RES_OK;
+}
+
+extern "C" res_T ssol_b200_plan_launch
+  (ssol_b200_plan* p, const ssp_rng* rng, const uint64_t first,
+   const uint64_t count, void* stream)
+{
+  return plan_launch(p, rng, first, count, stream, nullptr);
 }
 
 static void fill_sums(double dst[10][2], const double* src)
@@ -1171,16 +1178,90 @@ extern "C" res_T ssol_solve_ex
    const size_t max_failed, const ssol_path_tracker* tracker,
    const ssol_b200_options* options, ssol_estimator** out)
 {
-  (void)tracker;
   if(!scn || !rng || !n || !out) return RES_BAD_ARG;
+  *out = nullptr;
   if(n > (size_t)INT64_MAX || max_failed > (size_t)INT64_MAX)
     return RES_BAD_ARG;
   ssol_b200_plan* plan = nullptr;
   res_T res = ssol_b200_plan_create(scn, options, &plan);
   if(res != RES_OK) return res;
-  res = ssol_b200_plan_launch(plan, rng, 0, n, nullptr);
-  if(res == RES_OK)
-    res = ssol_b200_plan_finish(plan, rng, n, max_failed, nullptr, out);
+  if(!tracker) {
+    res = ssol_b200_plan_launch(plan, rng, 0, n, nullptr);
+    if(res == RES_OK)
+      res = ssol_b200_plan_finish(plan, rng, n, max_failed, nullptr, out);
+    ssol_b200_plan_ref_put(plan);
+    return res;
+  }
+
+  /* Path tracking (src/ssol_solver.c:1211-1220, 898-1126): the first
+   * min(N, 2^20) realisations record their paths on the device; negative
+   * lengths default to 0.75 x the largest extent of the scene's box */
+  double ext = 0;
+  for(int c = 0; c < 3; ++c)
+    ext = std::max(ext, plan->meta.aabb_hi[c] - plan->meta.aabb_lo[c]);
+  ext *= 0.75;
+  DTrack tr = {};
+  tr.npaths = std::min<unsigned long long>(n, 1ull << 20);
+  tr.cap = std::min<unsigned long long>(tr.npaths * 16 + 64, 1ull << 22);
+  tr.sun_len = tracker->sun_ray_length < 0 ? ext : tracker->sun_ray_length;
+  tr.inf_len = tracker->infinite_ray_length < 0 ? ext : tracker->infinite_ray_length;
+  const size_t vbytes = (size_t)tr.cap * sizeof(TrackVertex);
+  const size_t bytes = vbytes + 256 + (size_t)tr.npaths * 2 * sizeof(int32_t);
+  char* d = nullptr;
+  if(cudaMalloc((void**)&d, bytes) != cudaSuccess) {
+    ssol_b200_plan_ref_put(plan);
+    return RES_MEM_ERR;
+  }
+  tr.verts = reinterpret_cast<TrackVertex*>(d);
+  tr.nverts = reinterpret_cast<unsigned long long*>(d + vbytes);
+  tr.path_type = reinterpret_cast<int32_t*>(d + vbytes + 256);
+  tr.path_nv = tr.path_type + tr.npaths;
+  const cudaStream_t s = plan_stream(plan, nullptr);
+  if(cudaMemsetAsync(tr.nverts, 0, sizeof(unsigned long long), s) != cudaSuccess
+  || cudaMemsetAsync(tr.path_type, 0xff, (size_t)tr.npaths * sizeof(int32_t), s)
+       != cudaSuccess)
+    res = RES_UNKNOWN_ERR;
+  if(res == RES_OK) res = plan_launch(plan, rng, 0, n, s, &tr);
+  if(res == RES_OK) res = ssol_b200_plan_finish(plan, rng, n, max_failed, s, out);
+  if(*out) {
+    unsigned long long nv = 0;
+    std::vector<int32_t> types(tr.npaths), counts(tr.npaths);
+    bool ok = cudaMemcpy(&nv, tr.nverts, sizeof(nv), cudaMemcpyDeviceToHost) == cudaSuccess
+      && cudaMemcpy(types.data(), tr.path_type, tr.npaths * sizeof(int32_t),
+                    cudaMemcpyDeviceToHost) == cudaSuccess
+      && cudaMemcpy(counts.data(), tr.path_nv, tr.npaths * sizeof(int32_t),
+                    cudaMemcpyDeviceToHost) == cudaSuccess;
+    std::vector<TrackVertex> hv(ok ? (size_t)std::min(nv, tr.cap) : 0);
+    ok = ok && (hv.empty() || cudaMemcpy(hv.data(), tr.verts, hv.size() * sizeof(TrackVertex),
+                                         cudaMemcpyDeviceToHost) == cudaSuccess);
+    if(!ok) {
+      res = RES_UNKNOWN_ERR;
+    } else {
+      std::vector<TrackedPath> paths(tr.npaths);
+      std::vector<int32_t> got(tr.npaths, 0);
+      for(size_t k = 0; k < tr.npaths; ++k)
+        if(types[k] >= 0) paths[k].vertices.resize((size_t)counts[k]);
+      for(const TrackVertex& v : hv) {
+        if(v.slot >= tr.npaths || types[v.slot] < 0 || (int32_t)v.seq >= counts[v.slot])
+          continue;
+        ssol_path_vertex& pv = paths[v.slot].vertices[v.seq];
+        pv.pos[0] = v.pos[0]; pv.pos[1] = v.pos[1]; pv.pos[2] = v.pos[2];
+        pv.weight = v.weight;
+        ++got[v.slot];
+      }
+      size_t dropped = 0;
+      for(size_t k = 0; k < tr.npaths; ++k) {
+        if(types[k] < 0) continue;
+        if(got[k] != counts[k]) { ++dropped; continue; }
+        paths[k].type = (ssol_path_type)types[k];
+        (*out)->paths.push_back(std::move(paths[k]));
+      }
+      if(dropped)
+        scn->dev->log_warning("path tracking: %zu paths dropped, the vertex buffer "
+                              "holds %llu vertices.\n", dropped, tr.cap);
+    }
+  }
+  cudaFree(d);
   ssol_b200_plan_ref_put(plan);
   return res;
 }

@@ -55,6 +55,22 @@ GLOBAL_FIELDS = ("cos_factor", "absorbed_by_receivers", "shadowed", "missing",
                  "extinguished_by_atmosphere", "other_absorbed")
 
 
+class PathTracker(C.Structure):
+    """struct ssol_path_tracker (src/ssol.h:359-364); negative => default"""
+    _fields_ = [("sun_ray_length", C.c_double), ("infinite_ray_length", C.c_double)]
+
+
+class PathVertex(C.Structure):
+    _fields_ = [("pos", C.c_double * 3), ("weight", C.c_double)]
+
+
+class SsolPath(C.Structure):
+    _fields_ = [("path__", C.c_void_p)]
+
+
+PATH_TYPES = {0: "missing", 1: "shadow", 2: "success", 3: "error"}
+
+
 class McReceiver(C.Structure):
     _fields_ = [(n, McResult) for n in RCV_FIELDS] + [
         ("N__", C.c_size_t), ("mc__", C.c_void_p), ("instance__", C.c_void_p)]
@@ -195,6 +211,11 @@ _SIGS = {
     "ssol_atmosphere_create": [VP, PVP], "ssol_atmosphere_ref_put": [VP],
     "ssol_atmosphere_set_extinction": [VP, C.POINTER(Data)],
     "ssol_solve": [VP, VP, C.c_size_t, C.c_size_t, VP, PVP],
+    "ssol_estimator_get_tracked_paths_count": [VP, C.POINTER(C.c_size_t)],
+    "ssol_estimator_get_tracked_path": [VP, C.c_size_t, C.POINTER(SsolPath)],
+    "ssol_path_get_vertices_count": [C.POINTER(SsolPath), C.POINTER(C.c_size_t)],
+    "ssol_path_get_vertex": [C.POINTER(SsolPath), C.c_size_t, C.POINTER(PathVertex)],
+    "ssol_path_get_type": [C.POINTER(SsolPath), C.POINTER(C.c_int)],
     "ssol_estimator_ref_put": [VP],
     "ssol_estimator_get_mc_global": [VP, C.POINTER(McGlobal)],
     "ssol_estimator_get_mc_receiver": [VP, VP, C.c_int, C.POINTER(McReceiver)],
@@ -316,6 +337,25 @@ class Estimator:
             p = McPrimitive()
             self.lib.call("ssol_mc_shape_get_mc_primitive", C.byref(ms), i, C.byref(p))
             out.append({k: mc(getattr(p, k)) for k in RCV_FIELDS})
+        return out
+
+    def paths(self):
+        """Tracked paths: [(type, [((x, y, z), weight), ...]), ...]"""
+        n = C.c_size_t()
+        self.lib.call("ssol_estimator_get_tracked_paths_count", self.h, C.byref(n))
+        out = []
+        for i in range(n.value):
+            p = SsolPath()
+            self.lib.call("ssol_estimator_get_tracked_path", self.h, i, C.byref(p))
+            nv, t = C.c_size_t(), C.c_int()
+            self.lib.call("ssol_path_get_vertices_count", C.byref(p), C.byref(nv))
+            self.lib.call("ssol_path_get_type", C.byref(p), C.byref(t))
+            verts = []
+            for k in range(nv.value):
+                v = PathVertex()
+                self.lib.call("ssol_path_get_vertex", C.byref(p), k, C.byref(v))
+                verts.append((tuple(v.pos), v.weight))
+            out.append((PATH_TYPES.get(t.value, t.value), verts))
         return out
 
     def count(self, what):
@@ -591,15 +631,21 @@ class Scene:
             self.lib.call("ssp_rng_discard", h, position)
         return h
 
-    def solve(self, n, seed=0, max_failed=0, rng=None, options=None, check=True):
+    def solve(self, n, seed=0, max_failed=0, rng=None, options=None, check=True,
+              tracker=None):
+        """tracker: None, or (sun_ray_length, infinite_ray_length)"""
         if rng is None:
             rng = self.rng(seed)
         est = C.c_void_p()
+        tr = None
+        if tracker is not None:
+            tr = PathTracker(float(tracker[0]), float(tracker[1]))
+            tr = C.byref(tr)
         if options is not None:
-            res = self.lib.raw("ssol_solve_ex", self.scn, rng, n, max_failed, None,
+            res = self.lib.raw("ssol_solve_ex", self.scn, rng, n, max_failed, tr,
                                C.byref(options), C.byref(est))
         else:
-            res = self.lib.raw("ssol_solve", self.scn, rng, n, max_failed, None,
+            res = self.lib.raw("ssol_solve", self.scn, rng, n, max_failed, tr,
                                C.byref(est))
         if check and res not in (RES_OK,):
             if est:

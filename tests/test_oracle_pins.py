@@ -117,3 +117,26 @@ def test_solver10_12_flat_exact(oracle, kind, param):
         3 * g["absorbed_by_receivers"][2]
     assert est.count("failed_count") == 0
     del geom2
+
+
+def test_oracle_tracked_paths(oracle):
+    """src/test_ssol_solver1.c:177-207: a tracked solve of one realisation
+    records one path with vertices; the sun and infinite segments follow the
+    tracker lengths (negative: 0.75 x the scene's largest extent)."""
+    s, h = R.solver1_base(oracle)
+    e = s.solve(1, seed=0, tracker=(-1, -1))
+    paths = e.paths()
+    assert len(paths) == 1 and len(paths[0][1]) != 0
+    e = s.solve(200, seed=3, tracker=(2.0, 5.0))
+    paths = e.paths()
+    assert len(paths) == 200
+    for kind, verts in paths:
+        (x0, w0), (x1, w1) = verts[0], verts[1]
+        assert w0 == 1000.0  # the sun end carries the DNI
+        assert math.dist(x0, x1) == pytest.approx(2.0, rel=1e-9)
+        if kind == "shadow":
+            assert len(verts) == 2
+        else:
+            assert kind in ("success", "missing")
+            xl, _ = verts[-1]
+            assert math.dist(xl, verts[-2][0]) == pytest.approx(5.0, rel=1e-9)
