@@ -33,6 +33,7 @@ struct ssol_device {
   int verbose = 0;
   int cuda_device = -1; /* bound lazily on the first solve */
   void* stream = nullptr; /* cudaStream_t, created lazily */
+  void* mem_cache = nullptr; /* device blocks kept for reuse (solve.cpp) */
   void log_error(const char* fmt, ...) const;
   void log_warning(const char* fmt, ...) const;
 };

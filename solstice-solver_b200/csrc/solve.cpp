@@ -22,6 +22,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 
 using namespace ssolb;
 
@@ -46,8 +47,70 @@ static res_T device_bind(ssol_device* dev)
   return RES_OK;
 }
 
+/* Device blocks released by plans and batches are kept for the next solve
+ * on the same device: cudaFree unmaps memory and its cost varies by tens of
+ * milliseconds, which a loop of ssol_solve calls would pay every time. A
+ * released block is reused by a request of at most its size and at least a
+ * quarter of it; at most 8 blocks and 4 GiB are kept. */
+namespace {
+struct MemCache {
+  std::mutex lock;
+  std::vector<std::pair<void*, size_t>> blocks;
+};
+constexpr size_t CACHE_BLOCKS = 8;
+constexpr size_t CACHE_BYTES = size_t(4) << 30;
+}
+
+static cudaError_t dev_alloc(ssol_device* dev, void** p, size_t bytes)
+{
+  MemCache* c = dev ? static_cast<MemCache*>(dev->mem_cache) : nullptr;
+  if(c) {
+    std::lock_guard<std::mutex> g(c->lock);
+    size_t best = c->blocks.size();
+    for(size_t i = 0; i < c->blocks.size(); ++i) {
+      const size_t cap = c->blocks[i].second;
+      if(cap >= bytes && cap / 4 <= bytes
+      && (best == c->blocks.size() || cap < c->blocks[best].second))
+        best = i;
+    }
+    if(best < c->blocks.size()) {
+      *p = c->blocks[best].first;
+      c->blocks.erase(c->blocks.begin() + (long)best);
+      return cudaSuccess;
+    }
+  }
+  return cudaMalloc(p, bytes);
+}
+
+/* Work still queued on the block finishes first (a cudaFree would have
+ * synchronised too) */
+static void dev_free(ssol_device* dev, void* p, size_t bytes)
+{
+  if(!p) return;
+  if(!dev) { cudaFree(p); return; }
+  cudaDeviceSynchronize();
+  if(!dev->mem_cache) dev->mem_cache = new (std::nothrow) MemCache();
+  MemCache* c = static_cast<MemCache*>(dev->mem_cache);
+  if(!c) { cudaFree(p); return; }
+  std::lock_guard<std::mutex> g(c->lock);
+  c->blocks.emplace_back(p, bytes);
+  size_t total = 0;
+  for(const auto& b : c->blocks) total += b.second;
+  while(c->blocks.size() > CACHE_BLOCKS || total > CACHE_BYTES) {
+    total -= c->blocks.front().second;
+    cudaFree(c->blocks.front().first);
+    c->blocks.erase(c->blocks.begin());
+  }
+}
+
 void ssolb_device_release_gpu(ssol_device* dev)
 {
+  if(dev->mem_cache) {
+    MemCache* c = static_cast<MemCache*>(dev->mem_cache);
+    for(const auto& b : c->blocks) cudaFree(b.first);
+    delete c;
+    dev->mem_cache = nullptr;
+  }
   if(dev->stream) {
     cudaStreamDestroy((cudaStream_t)dev->stream);
     dev->stream = nullptr;
@@ -89,6 +152,7 @@ struct ssol_b200_plan {
   void* d_scene = nullptr;
   void* d_tally = nullptr;
   size_t scene_bytes = 0;
+  size_t scene_alloc = 0;
   TallyLayout tl{};
   DScene<float> s32{};
   DScene<double> s64{};
@@ -398,7 +462,8 @@ static res_T upload(ssol_b200_plan* p, const FlatScene<R>& f, DScene<R>& S)
   b.add(f.wl_pdf);
   b.add(f.wl_cdf);
   const size_t bytes = b.host.size() + 256;
-  if(cudaMalloc(&p->d_scene, bytes) != cudaSuccess) return RES_MEM_ERR;
+  if(dev_alloc(p->dev, &p->d_scene, bytes) != cudaSuccess) return RES_MEM_ERR;
+  p->scene_alloc = bytes;
   if(cudaMemcpyAsync(p->d_scene, b.host.data(), b.host.size(),
                      cudaMemcpyHostToDevice,
                      (cudaStream_t)p->dev->stream) != cudaSuccess)
@@ -410,8 +475,8 @@ static res_T upload(ssol_b200_plan* p, const FlatScene<R>& f, DScene<R>& S)
 
 static void plan_release(ssol_b200_plan* p)
 {
-  if(p->d_scene) cudaFree(p->d_scene);
-  if(p->d_tally) cudaFree(p->d_tally);
+  dev_free(p->dev, p->d_scene, p->scene_alloc);
+  dev_free(p->dev, p->d_tally, p->tl.total);
   if(p->ev0) cudaEventDestroy(p->ev0);
   if(p->ev1) cudaEventDestroy(p->ev1);
   if(p->scn) ssol_scene_ref_put(p->scn);
@@ -494,7 +559,7 @@ extern "C" res_T ssol_b200_plan_create
 
   /* Tallies: FP64 sums, then integer counters */
   p->tl = tally_layout(p->nrcv, p->nsampled, p->meta.nprim_slots);
-  if(cudaMalloc(&p->d_tally, p->tl.total) != cudaSuccess) {
+  if(dev_alloc(p->dev, &p->d_tally, p->tl.total) != cudaSuccess) {
     plan_release(p);
     return RES_MEM_ERR;
   }
