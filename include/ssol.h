@@ -7,7 +7,7 @@
  * written against the reference compiles unchanged. Everything in here is
  * plain C: no CUDA or C++ type crosses this boundary.
  *
- * What differs from the reference ("Boundary"):
+ * What differs from the reference:
  *  - `res_T` and its codes are defined here (the reference takes them from
  *    RSys, which is not part of the reference tree); source compatibility is
  *    the target, not binary compatibility with RSys-built callers.

@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(MAX_BLOCK, 1)
 adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t first,
                uint64_t count)
 {
-  __shared__ int stack_sm[STACK_SIZE * MAX_BLOCK];
+  __shared__ int stack_sm[SMEM_STACK * MAX_BLOCK];
   int* stack = stack_sm + threadIdx.x;
   const int stride = blockDim.x;
   Counters cnt = {0, 0, 0, 0};

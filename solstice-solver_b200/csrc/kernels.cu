@@ -609,12 +609,15 @@ __device__ __forceinline__ bool slab
 }
 
 /* The builder bounds the BVH depth to 30, so a traversal never holds more
- * than 30 deferred nodes */
+ * than 30 deferred nodes. The first SMEM_STACK entries live in shared
+ * memory; the rare deeper ones in a per-thread array (local memory), which
+ * leaves shared memory to the L1 cache that holds the BVH. */
 constexpr int STACK_SIZE = 32;
+constexpr int SMEM_STACK = 8;
 
 /* Closest accepted hit, or the first accepted hit when `any` (shadow rays).
- * The deferred-node stack lives in shared memory: entry i of this thread is
- * stack[i * stride]. */
+ * Deferred node i < SMEM_STACK of this thread is stack[i * stride] in shared
+ * memory, deeper ones go to `spill`. */
 template<class R>
 __device__ bool trace_ray
   (const DScene<R>& S, V3<R> o, V3<R> d, R tmin, const SelfInfo& self,
@@ -636,6 +639,7 @@ __device__ bool trace_ray
   const Shear<R> sh = make_shear(d);
   best.t = rmax<R>();
   bool found = false;
+  int spill[STACK_SIZE - SMEM_STACK];
   int sp = 0;
   int node = 0;
   for(;;) {
@@ -647,8 +651,6 @@ __device__ bool trace_ray
         && N.count[0] >= 0;
     h[1] = slab(N.lo[1], N.hi[1], inv, oinv, tmin, best.t, te[1])
         && N.count[1] >= 0;
-    int next[2];
-    int nnext = 0;
     for(int k = 0; k < 2; ++k) {
       if(!h[k]) continue;
       if(N.count[k] > 0) {
@@ -665,26 +667,29 @@ __device__ bool trace_ray
           }
           if(any && found) return true;
         }
-      } else {
-        next[nnext++] = k;
       }
     }
-    if(nnext == 2) {
-      const int nearer = te[0] <= te[1] ? 0 : 1;
-      if(sp < STACK_SIZE) stack[(sp++) * stride] = N.child[1 - nearer];
-      node = N.child[nearer];
-    } else if(nnext == 1) {
-      node = N.child[next[0]];
+    const bool in0 = h[0] && N.count[0] == 0, in1 = h[1] && N.count[1] == 0;
+    if(in0 && in1) {
+      const bool first0 = te[0] <= te[1];
+      const int far = first0 ? N.child[1] : N.child[0];
+      if(sp < SMEM_STACK) stack[(sp++) * stride] = far;
+      else if(sp < STACK_SIZE) spill[(sp++) - SMEM_STACK] = far;
+      node = first0 ? N.child[0] : N.child[1];
+    } else if(in0 || in1) {
+      node = in0 ? N.child[0] : N.child[1];
     } else {
       if(sp == 0) break;
-      node = stack[(--sp) * stride];
+      --sp;
+      node = sp < SMEM_STACK ? stack[sp * stride] : spill[sp - SMEM_STACK];
     }
   }
   return found;
 }
 
 /*******************************************************************************
- * BSDF sampling (Star-SF restated from published optics)
+ * BSDF sampling (Star-SF's BSDFs restated from published optics: Fresnel
+ * equations, Walter et al. 2007 microfacet sampling, thin-slab series)
  ******************************************************************************/
 enum { BXDF_REFLECTION = 1, BXDF_TRANSMISSION = 2 };
 
@@ -1103,11 +1108,13 @@ __device__ __noinline__ void commit_path
   g[G_MISSING] = end == END_MISS ? (p.virt ? p.inc0 : p.prev[0]) : 0.0;
   g[G_ATM] = ps[PS_ATM * stride];
   g[G_OTHER] = ps[PS_OTHER * stride];
+  if(acc) {
 #pragma unroll
-  for(int q = 0; q < NGLOBAL; ++q) {
-    const double w = f * g[q];
-    acc[(2 * q) * stride] += w;
-    acc[(2 * q + 1) * stride] += w * w;
+    for(int q = 0; q < NGLOBAL; ++q) {
+      const double w = f * g[q];
+      acc[(2 * q) * stride] += w;
+      acc[(2 * q + 1) * stride] += w * w;
+    }
   }
   {
     const double wc = f * g[G_COS], ws = f * g[G_SHADOW];
@@ -1198,8 +1205,9 @@ realisation_kernel
    unsigned long long* next_path, const DTrack tr)
 {
   /* Shared memory: per-thread FP64 global sums [12][blockDim], per-thread
-   * path sums [10][blockDim], the receiver-side sums, the per-thread
-   * traversal stacks [32][blockDim] */
+   * path sums [10][blockDim], the receiver-side sums, the first traversal
+   * stack entries [8][blockDim]; shared memory left unused goes to the L1
+   * cache */
   extern __shared__ double smem[];
   __shared__ double red[MAX_BLOCK / 32][2 * NGLOBAL];
   const int bd = blockDim.x, tid = threadIdx.x;
@@ -1399,7 +1407,7 @@ batch_kernel
    * running across an item boundary) and flushed to the item's tallies when
    * the warp moves on. Tags change only where the warp is converged. */
   double* wslots = reinterpret_cast<double*>(
-    reinterpret_cast<int*>(smem + (2 * NGLOBAL + PS_COUNT) * bd) + STACK_SIZE * bd)
+    reinterpret_cast<int*>(smem + (2 * NGLOBAL + PS_COUNT) * bd) + SMEM_STACK * bd)
     + (size_t)(tid >> 5) * 2 * rcvd;
   for(int i = (int)lane; i < 2 * rcvd; i += 32) wslots[i] = 0;
   __syncwarp();
@@ -1589,7 +1597,7 @@ static int launch_variant
   const int rcv_doubles = S.nrcv <= SMEM_RCV_MAX ? S.nrcv * NRCV_Q * 2 : 0;
   const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block + rcv_doubles)
                       * sizeof(double)
-                    + (size_t)STACK_SIZE * block * sizeof(int);
+                    + (size_t)SMEM_STACK * block * sizeof(int);
   static bool attr_set = false;
   if(!attr_set) {
     cudaFuncSetAttribute(realisation_kernel<R, MINB, TRACK>,
@@ -1641,7 +1649,7 @@ static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg
   const int block = cfg.block_size > 0 ? cfg.block_size : MAX_BLOCK;
   if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
   const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block) * sizeof(double)
-                    + (size_t)STACK_SIZE * block * sizeof(int)
+                    + (size_t)SMEM_STACK * block * sizeof(int)
                     + (size_t)(block / 32) * 2 * cfg.rcv_doubles * sizeof(double);
   static bool attr_set = false;
   if(!attr_set) {
@@ -1733,7 +1741,7 @@ static int launch_batch_noalloc_variant
   const int block = cfg.block_size > 0 ? cfg.block_size : MAX_BLOCK;
   if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
   const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block) * sizeof(double)
-                    + (size_t)STACK_SIZE * block * sizeof(int)
+                    + (size_t)SMEM_STACK * block * sizeof(int)
                     + (size_t)(block / 32) * 2 * cfg.rcv_doubles * sizeof(double);
   cudaFuncSetAttribute(batch_kernel<R, MINB>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
