@@ -239,7 +239,10 @@ template<class R> std::vector<DNode<R>> bvh_nodes(const BvhResult& b)
           nodes[i].hi[k][c] = round_up<R>(hi);
         }
       }
-      nodes[i].child[k] = b.child[s];
+      /* A one-primitive leaf holds its prim reference itself (no indirection
+       * through primrefs on the device) */
+      nodes[i].child[k] = b.count[s] == 1 ? (int32_t)b.primrefs[(size_t)b.child[s]]
+                                          : b.child[s];
       nodes[i].count[k] = b.count[s];
     }
   }

@@ -154,8 +154,8 @@ struct DCarving {
 };
 
 /* Binary BVH node holding its children's boxes. count == 0: child is a node
- * index; count > 0: child is the first prim reference of a leaf; count < 0:
- * empty slot. */
+ * index; count == 1: child is the leaf's prim reference itself; count > 1:
+ * child is the leaf's first entry in primrefs; count < 0: empty slot. */
 template<typename R> struct alignas(16) DNode {
   R lo[2][3];
   R hi[2][3];

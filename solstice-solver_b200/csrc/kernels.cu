@@ -655,7 +655,8 @@ __device__ bool trace_ray
       if(!h[k]) continue;
       if(N.count[k] > 0) {
         for(int p = 0; p < N.count[k]; ++p) {
-          const uint32_t ref = S.primrefs[N.child[k] + p];
+          const uint32_t ref = N.count[k] == 1 ? (uint32_t)N.child[k]
+                                               : S.primrefs[N.child[k] + p];
           if(primref_kind(ref) == PRIM_TRIANGLE) {
             ++cnt.tris;
             test_triangle(S, (int)primref_index(ref), o, d, sh, tmin, eps,

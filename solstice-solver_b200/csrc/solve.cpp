@@ -351,6 +351,11 @@ static bool validate(const FlatScene<R>& f)
     for(int k = 0; k < 2; ++k) {
       if(n.count[k] == 0) {
         if(n.child[k] <= 0 || n.child[k] >= nnodes) return false;
+      } else if(n.count[k] == 1) {
+        const uint32_t ref = (uint32_t)n.child[k];
+        const uint32_t i = primref_index(ref);
+        if(primref_kind(ref) == PRIM_TRIANGLE ? i >= f.tris.size() : i >= f.quads.size())
+          return false;
       } else if(n.count[k] > 0) {
         if(n.child[k] < 0 || (int64_t)n.child[k] + n.count[k] > nrefs) return false;
       }
