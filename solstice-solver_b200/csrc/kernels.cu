@@ -909,7 +909,7 @@ enum : int { PS_V0 = 0, PS_ABS = 6, PS_ATM = 7, PS_OTHER = 8, PS_COS = 9,
 
 /* point_init (src/ssol_solver.c:207-352) up to the shadow ray */
 template<class R>
-__device__ __noinline__ void init_path
+__device__ __forceinline__ void init_path
   (const DScene<R>& S, const Rng& rng, PathState<R>& p, double* ps, int stride)
 {
   const U32x4 r0 = rng.get(0u, RNG_PRIMARY);
