@@ -509,6 +509,60 @@ def run_suns(args):
     else:
         n_all = float(n_total)
 
+    # (e) from scratch: each approach runs a pilot of 1e5 realisations per
+    # sun, reads its estimates back, and traces the realisations each sun
+    # still needs for 0.1 % SE; wall clock, scene snapshots included. The
+    # plain loop does this sun by sun, as a caller running every sun to a
+    # target SE with the plain kernel must.
+    budgets = [100000 for _ in suns]
+
+    def needed(est, done_n):
+        a = est.globals()["absorbed_by_receivers"]
+        rse = a[2] / a[0] if a[0] > 0 else 1.0
+        return int(min(max(done_n * (rse / target) ** 2, done_n), 1e8))
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bt = P.Batch(lib, scenes, opt)
+    bt.launch(rng, budgets, sp)
+    es = bt.finish(rng, 0, sp)
+    more = [needed(e, b) - b for e, b in zip(es, budgets)]
+    del es
+    bt.launch(rng, more, sp)
+    es = bt.finish(rng, 0, sp)
+    del es
+    bt.close()
+    scratch_batched = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for sc, b in zip(scenes, budgets):
+        pl = P.C.c_void_p()
+        lib.call("ssol_b200_plan_create", sc.scn, P.C.byref(opt), P.C.byref(pl))
+        lib.call("ssol_b200_plan_launch", pl, rng, 0, b, sp)
+        est = P.C.c_void_p()
+        lib.raw("ssol_b200_plan_finish", pl, rng, b, 0, sp, P.C.byref(est))
+        e = P.Estimator(sc, est, 0)
+        tot = needed(e, b)
+        del e
+        if tot > b:
+            lib.call("ssol_b200_plan_launch", pl, rng, b, tot - b, sp)
+            est = P.C.c_void_p()
+            lib.raw("ssol_b200_plan_finish", pl, rng, tot, 0, sp, P.C.byref(est))
+            lib.raw("ssol_estimator_ref_put", est)
+        lib.raw("ssol_b200_plan_ref_put", pl)
+    scratch_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for sc, b in zip(scenes, budgets):
+        r1 = sc.rng(seed=args.seed + 5)
+        e = sc.solve(b, rng=r1, options=opt)
+        tot = needed(e, b)
+        if tot > b:
+            state = P.C.c_void_p()
+            lib.call("ssol_estimator_get_rng_state", e.h, P.C.byref(state))
+            e2 = sc.solve(tot - b, rng=state, options=opt)
+            del e2
+        del e
+    scratch_solve = time.perf_counter() - t0
+
     per_step_b = ms_batched / args.steps
     per_step_p = ms_plain / args.steps
     value = n_all / (per_step_b * 1e-3) / 1e6
@@ -539,6 +593,14 @@ def run_suns(args):
                                 "plain_plan_loop": per_step_p * 1e-3,
                                 "ssol_solve_loop": solve_loop_s,
                                 "batch_api_end_to_end": e2e_s},
+        "time_to_0.1pct_se_from_scratch_s": {
+            "batched": scratch_batched, "plain_plan_loop_per_sun": scratch_plain,
+            "ssol_solve_loop_per_sun": scratch_solve,
+            "what": "pilot of 1e5 per sun + read-back + the rest, per approach, "
+                    "scene snapshots included; the per-sun loops synchronise once "
+                    "per pilot"},
+        "speedup_from_scratch_vs_plain_plan_loop": scratch_plain / scratch_batched,
+        "speedup_from_scratch_vs_ssol_solve_loop": scratch_solve / scratch_batched,
         "speedup_batched_vs_plain_plan_loop": per_step_p / per_step_b,
         "speedup_batched_vs_ssol_solve_loop": solve_loop_s / (per_step_b * 1e-3),
         "suns_reaching_0.1pct_se": reached,

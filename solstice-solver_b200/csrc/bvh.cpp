@@ -6,6 +6,7 @@
 #include "bvh.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <limits>
 
@@ -55,9 +56,11 @@ Box bounds(const std::vector<PrimBox>& p, int b, int e)
 double centroid(const PrimBox& p, int axis)
 { return 0.5 * (p.lo[axis] + p.hi[axis]); }
 
-/* Returns the split position in [b, e) or -1 to make a leaf */
-int split(std::vector<PrimBox>& p, int b, int e, const BvhBuildParams& prm,
-          int depth)
+/* Returns the split position in [b, e) or -1 to make a leaf. One pass
+ * bins the centroids of [b, e) on all three axes at once (centroids are
+ * precomputed in `c`, kept in the order of `p`). */
+int split(std::vector<PrimBox>& p, std::vector<std::array<double, 3>>& c, int b, int e,
+          const BvhBuildParams& prm, int depth)
 {
   const int n = e - b;
   if(n <= prm.max_leaf) return -1;
@@ -65,46 +68,50 @@ int split(std::vector<PrimBox>& p, int b, int e, const BvhBuildParams& prm,
   if(depth >= prm.max_depth - 1) return -1;
   Box cb;
   cb.reset();
-  for(int i = b; i < e; ++i) {
-    double c[3];
-    for(int k = 0; k < 3; ++k) c[k] = centroid(p[i], k);
-    cb.grow(c, c);
-  }
+  for(int i = b; i < e; ++i) cb.grow(c[i].data(), c[i].data());
   const bool force_median = depth >= prm.max_depth - 10;
   double best_cost = std::numeric_limits<double>::max();
   int best_axis = -1, best_bin = -1;
-  const int nb = prm.bins;
+  constexpr int MAX_BINS = 64;
+  const int nb = std::min(std::max(prm.bins, 2), MAX_BINS);
+  double scale[3];
+  for(int a = 0; a < 3; ++a) {
+    const double ext = cb.hi[a] - cb.lo[a];
+    scale[a] = ext > 0 ? nb / ext : 0;
+  }
   if(!force_median) {
-    for(int axis = 0; axis < 3; ++axis) {
-      const double ext = cb.hi[axis] - cb.lo[axis];
-      if(!(ext > 0)) continue;
-      std::vector<Box> bin(nb);
-      std::vector<int> cnt(nb, 0);
-      for(Box& x : bin) x.reset();
-      for(int i = b; i < e; ++i) {
-        int k = (int)((centroid(p[i], axis) - cb.lo[axis]) / ext * nb);
+    Box bin[3][MAX_BINS];
+    int cnt[3][MAX_BINS];
+    for(int a = 0; a < 3; ++a)
+      for(int k = 0; k < nb; ++k) { bin[a][k].reset(); cnt[a][k] = 0; }
+    for(int i = b; i < e; ++i) {
+      for(int a = 0; a < 3; ++a) {
+        int k = (int)((c[i][a] - cb.lo[a]) * scale[a]);
         k = std::min(std::max(k, 0), nb - 1);
-        bin[k].grow(p[i].lo, p[i].hi);
-        ++cnt[k];
+        bin[a][k].grow(p[i].lo, p[i].hi);
+        ++cnt[a][k];
       }
-      std::vector<double> right_area(nb, 0);
-      std::vector<int> right_cnt(nb, 0);
+    }
+    for(int axis = 0; axis < 3; ++axis) {
+      if(!(scale[axis] > 0)) continue;
+      double right_area[MAX_BINS] = {};
+      int right_cnt[MAX_BINS] = {};
       Box acc;
       acc.reset();
-      int c = 0;
+      int m = 0;
       for(int k = nb - 1; k > 0; --k) {
-        acc.grow(bin[k].lo, bin[k].hi);
-        c += cnt[k];
+        acc.grow(bin[axis][k].lo, bin[axis][k].hi);
+        m += cnt[axis][k];
         right_area[k] = acc.area();
-        right_cnt[k] = c;
+        right_cnt[k] = m;
       }
       acc.reset();
-      c = 0;
+      m = 0;
       for(int k = 0; k < nb - 1; ++k) {
-        acc.grow(bin[k].lo, bin[k].hi);
-        c += cnt[k];
-        if(!c || !right_cnt[k + 1]) continue;
-        const double cost = acc.area() * c + right_area[k + 1] * right_cnt[k + 1];
+        acc.grow(bin[axis][k].lo, bin[axis][k].hi);
+        m += cnt[axis][k];
+        if(!m || !right_cnt[k + 1]) continue;
+        const double cost = acc.area() * m + right_area[k + 1] * right_cnt[k + 1];
         if(cost < best_cost) {
           best_cost = cost;
           best_axis = axis;
@@ -113,16 +120,21 @@ int split(std::vector<PrimBox>& p, int b, int e, const BvhBuildParams& prm,
       }
     }
   }
+  /* Partition p and c together */
+  auto swap_items = [&](int x, int y) {
+    std::swap(p[x], p[y]);
+    std::swap(c[x], c[y]);
+  };
   if(best_axis >= 0) {
-    const double ext = cb.hi[best_axis] - cb.lo[best_axis];
-    auto mid = std::partition(p.begin() + b, p.begin() + e,
-      [&](const PrimBox& x) {
-        int k = (int)((centroid(x, best_axis) - cb.lo[best_axis]) / ext * nb);
-        k = std::min(std::max(k, 0), nb - 1);
-        return k <= best_bin;
-      });
-    const int m = (int)(mid - p.begin());
-    if(m > b && m < e) return m;
+    const double lo = cb.lo[best_axis], sc = scale[best_axis];
+    int l = b, r = e - 1;
+    while(l <= r) {
+      int k = (int)((c[l][best_axis] - lo) * sc);
+      k = std::min(std::max(k, 0), nb - 1);
+      if(k <= best_bin) ++l;
+      else swap_items(l, r--);
+    }
+    if(l > b && l < e) return l;
   }
   /* Median split along the largest centroid extent */
   int axis = 0;
@@ -131,10 +143,15 @@ int split(std::vector<PrimBox>& p, int b, int e, const BvhBuildParams& prm,
     if(cb.hi[k] - cb.lo[k] > ext) { ext = cb.hi[k] - cb.lo[k]; axis = k; }
   }
   const int m = b + n / 2;
-  std::nth_element(p.begin() + b, p.begin() + m, p.begin() + e,
-    [&](const PrimBox& x, const PrimBox& y) {
-      return centroid(x, axis) < centroid(y, axis);
-    });
+  std::vector<int> order(n);
+  for(int i = 0; i < n; ++i) order[i] = b + i;
+  std::nth_element(order.begin(), order.begin() + n / 2, order.end(),
+    [&](int x, int y) { return c[x][axis] < c[y][axis]; });
+  std::vector<PrimBox> tp(n);
+  std::vector<std::array<double, 3>> tc(n);
+  for(int i = 0; i < n; ++i) { tp[i] = p[order[i]]; tc[i] = c[order[i]]; }
+  std::copy(tp.begin(), tp.end(), p.begin() + b);
+  std::copy(tc.begin(), tc.end(), c.begin() + b);
   return m;
 }
 
@@ -172,8 +189,11 @@ void build_bvh(std::vector<PrimBox> prims, const BvhBuildParams& prm,
     out.primrefs.push_back(0);
     return;
   }
+  std::vector<std::array<double, 3>> cent(prims.size());
+  for(size_t i = 0; i < prims.size(); ++i)
+    for(int a = 0; a < 3; ++a) cent[i][a] = centroid(prims[i], a);
   std::vector<Task> stack;
-  int m = split(prims, 0, n, prm, 0);
+  int m = split(prims, cent, 0, n, prm, 0);
   if(m < 0) {
     /* Whole scene in one leaf; the second slot is an empty box */
     Box empty;
@@ -194,7 +214,7 @@ void build_bvh(std::vector<PrimBox> prims, const BvhBuildParams& prm,
     stack.pop_back();
     out.depth = std::max(out.depth, t.depth + 1);
     const Box b = bounds(prims, t.begin, t.end);
-    const int s = split(prims, t.begin, t.end, prm, t.depth);
+    const int s = split(prims, cent, t.begin, t.end, prm, t.depth);
     if(s < 0) {
       const int first = (int)refs.size();
       for(int i = t.begin; i < t.end; ++i) refs.push_back(prims[i].ref);

@@ -23,6 +23,8 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <atomic>
+#include <thread>
 
 using namespace ssolb;
 
@@ -45,6 +47,24 @@ static res_T device_bind(ssol_device* dev)
     return RES_UNKNOWN_ERR;
   dev->stream = s;
   return RES_OK;
+}
+
+/* Runs f(0..n-1) on the host's hardware threads (the calling thread
+ * included); used for per-item host work of batches */
+template<class F> static void parallel_for(size_t n, F&& f)
+{
+  const unsigned hw = std::thread::hardware_concurrency();
+  const size_t nt = std::max<size_t>(1, std::min<size_t>(hw ? hw : 1, n));
+  if(nt <= 1) { for(size_t i = 0; i < n; ++i) f(i); return; }
+  std::atomic<size_t> next{0};
+  auto work = [&]() {
+    for(size_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) f(i);
+  };
+  std::vector<std::thread> pool;
+  pool.reserve(nt - 1);
+  for(size_t t = 1; t < nt; ++t) pool.emplace_back(work);
+  work();
+  for(std::thread& t : pool) t.join();
 }
 
 /* Device blocks released by plans and batches are kept for the next solve
@@ -902,6 +922,7 @@ struct ssol_b200_batch {
   double kernel_ms = 0;
   bool timing_valid = false;
   uint64_t h_seed = 0;
+  void* h_tally = nullptr; /* pinned tally read-back, allocated on first finish */
 };
 
 static void batch_release(ssol_b200_batch* b)
@@ -910,6 +931,7 @@ static void batch_release(ssol_b200_batch* b)
   if(b->graph) cudaGraphDestroy(b->graph);
   if(b->d_scene) cudaFree(b->d_scene);
   if(b->d_tally) cudaFree(b->d_tally);
+  if(b->h_tally) cudaFreeHost(b->h_tally);
   if(b->ev0) cudaEventDestroy(b->ev0);
   if(b->ev1) cudaEventDestroy(b->ev1);
   for(ssol_scene* s : b->scenes) ssol_scene_ref_put(s);
@@ -998,22 +1020,24 @@ extern "C" res_T ssol_b200_batch_create
   res_T res;
   std::vector<FlatScene<float>> f32;
   std::vector<FlatScene<double>> f64;
+  /* Snapshots of the items in parallel on the host threads */
+  std::vector<res_T> item_res(nscenes, RES_OK);
   if(opt.precision == SSOL_B200_FP32) {
     f32.resize(nscenes);
-    for(size_t i = 0; i < nscenes; ++i) {
-      res = flatten_scene(scenes[i], bp, f32[i]);
-      if(res == RES_OK && !validate(f32[i])) res = RES_UNKNOWN_ERR;
-      if(res != RES_OK) { batch_release(b); return res; }
-      b->meta.push_back(f32[i].meta);
-    }
+    parallel_for(nscenes, [&](size_t i) {
+      item_res[i] = flatten_scene(scenes[i], bp, f32[i]);
+      if(item_res[i] == RES_OK && !validate(f32[i])) item_res[i] = RES_UNKNOWN_ERR;
+    });
   } else {
     f64.resize(nscenes);
-    for(size_t i = 0; i < nscenes; ++i) {
-      res = flatten_scene(scenes[i], bp, f64[i]);
-      if(res == RES_OK && !validate(f64[i])) res = RES_UNKNOWN_ERR;
-      if(res != RES_OK) { batch_release(b); return res; }
-      b->meta.push_back(f64[i].meta);
-    }
+    parallel_for(nscenes, [&](size_t i) {
+      item_res[i] = flatten_scene(scenes[i], bp, f64[i]);
+      if(item_res[i] == RES_OK && !validate(f64[i])) item_res[i] = RES_UNKNOWN_ERR;
+    });
+  }
+  for(size_t i = 0; i < nscenes; ++i) {
+    if(item_res[i] != RES_OK) { batch_release(b); return item_res[i]; }
+    b->meta.push_back(f32.empty() ? f64[i].meta : f32[i].meta);
   }
   res = device_bind(dev);
   if(res == RES_OK)
@@ -1212,9 +1236,14 @@ extern "C" res_T ssol_b200_batch_finish
 {
   if(!b || !rng || !out) return RES_BAD_ARG;
   const cudaStream_t s = stream ? (cudaStream_t)stream : (cudaStream_t)b->dev->stream;
-  std::vector<unsigned char> h(b->tally_total);
+  /* Pinned read-back buffer, kept with the batch */
+  if(!b->h_tally && cudaMallocHost(&b->h_tally, b->tally_total) != cudaSuccess) {
+    b->h_tally = nullptr;
+    return RES_MEM_ERR;
+  }
+  unsigned char* h = static_cast<unsigned char*>(b->h_tally);
   DStats st;
-  if(cudaMemcpyAsync(h.data(), b->d_tally, b->tally_total, cudaMemcpyDeviceToHost, s)
+  if(cudaMemcpyAsync(h, b->d_tally, b->tally_total, cudaMemcpyDeviceToHost, s)
      != cudaSuccess
   || cudaMemcpyAsync(&st, b->d_stats, sizeof(DStats), cudaMemcpyDeviceToHost, s)
      != cudaSuccess)
@@ -1224,18 +1253,22 @@ extern "C" res_T ssol_b200_batch_finish
     b->dev->log_error("device error: %s\n", cudaGetErrorString(err));
     return RES_UNKNOWN_ERR;
   }
-  res_T worst = RES_OK;
-  for(size_t i = 0; i < b->scenes.size(); ++i) {
-    out[i] = nullptr;
-    const res_T r = make_estimator(b->dev, b->scenes[i], b->meta[i], b->tl[i],
-      h.data() + b->tally_off[i], b->done[i], rng, b->done[i], &st, b->kernel_ms,
+  const size_t n = b->scenes.size();
+  std::vector<res_T> item_res(n, RES_OK);
+  for(size_t i = 0; i < n; ++i) out[i] = nullptr;
+  parallel_for(n, [&](size_t i) {
+    item_res[i] = make_estimator(b->dev, b->scenes[i], b->meta[i], b->tl[i],
+      h + b->tally_off[i], b->done[i], rng, b->done[i], &st, b->kernel_ms,
       b->scene_bytes, max_failed, &out[i]);
-    if(r != RES_OK && r != RES_BAD_OP) {
-      for(size_t k = 0; k <= i; ++k)
+  });
+  res_T worst = RES_OK;
+  for(size_t i = 0; i < n; ++i) {
+    if(item_res[i] != RES_OK && item_res[i] != RES_BAD_OP) {
+      for(size_t k = 0; k < n; ++k)
         if(out[k]) { ssol_estimator_ref_put(out[k]); out[k] = nullptr; }
-      return r;
+      return item_res[i];
     }
-    if(r == RES_BAD_OP) worst = RES_BAD_OP;
+    if(item_res[i] == RES_BAD_OP) worst = RES_BAD_OP;
   }
   return worst;
 }
