@@ -1441,12 +1441,20 @@ batch_kernel
         if(g >= count) {
           done = true;
         } else {
-          int lo = 0, hi = nitems; /* prefix[lo] <= g < prefix[hi] */
-          while(hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if(prefix[mid] <= g) lo = mid; else hi = mid;
+          /* The work index only grows, so the item follows from the lane's
+           * previous one, usually in zero or one step; a binary search
+           * covers long jumps. prefix[it] <= g < prefix[it + 1]. */
+          if(prefix[it] > g) it = 0;
+          int steps = 0;
+          while(prefix[it + 1] <= g && steps < 4) { ++it; ++steps; }
+          if(prefix[it + 1] <= g) {
+            int lo = it, hi = nitems;
+            while(hi - lo > 1) {
+              const int mid = (lo + hi) >> 1;
+              if(prefix[mid] <= g) lo = mid; else hi = mid;
+            }
+            it = lo;
           }
-          it = lo;
           if(it != acc_item) {
             if(acc_item >= 0) {
               for(int q = 0; q < 2 * NGLOBAL; ++q) {
