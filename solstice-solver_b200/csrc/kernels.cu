@@ -1402,15 +1402,19 @@ batch_kernel
   int* stack = reinterpret_cast<int*>(smem + (2 * NGLOBAL + PS_COUNT) * bd) + tid;
   for(int q = 0; q < 2 * NGLOBAL; ++q) acc[q * bd] = 0;
   int acc_item = -1;
-  /* Receiver sums: every path adds to the same few addresses of its item,
-   * so they are gathered per warp in two shared-memory slots tagged with an
-   * item (the warp's current item and the previous one, for the paths still
-   * running across an item boundary) and flushed to the item's tallies when
-   * the warp moves on. Tags change only where the warp is converged. */
+  /* Global and receiver sums: every path adds to the same few addresses of
+   * its item, so they are gathered per warp in two shared-memory slots
+   * tagged with an item (the warp's current item and the previous one, for
+   * the paths still running across an item boundary) and flushed to the
+   * item's tallies when the warp moves on: one device atomic per warp and
+   * address for each item instead of one per thread. A slot holds the
+   * 2 x NGLOBAL global sums, then `rcvd` receiver sums. Tags change only
+   * where the warp is converged. */
+  const int ss = 2 * NGLOBAL + rcvd;
   double* wslots = reinterpret_cast<double*>(
     reinterpret_cast<int*>(smem + (2 * NGLOBAL + PS_COUNT) * bd) + SMEM_STACK * bd)
-    + (size_t)(tid >> 5) * 2 * rcvd;
-  for(int i = (int)lane; i < 2 * rcvd; i += 32) wslots[i] = 0;
+    + (size_t)(tid >> 5) * 2 * ss;
+  for(int i = (int)lane; i < 2 * ss; i += 32) wslots[i] = 0;
   __syncwarp();
   int stag[2] = {-1, -1};
   int cur = 0;
@@ -1457,8 +1461,14 @@ batch_kernel
           }
           if(it != acc_item) {
             if(acc_item >= 0) {
+              double* sl = acc_item == stag[cur] ? wslots + cur * ss
+                : acc_item == stag[cur ^ 1] ? wslots + (cur ^ 1) * ss : nullptr;
               for(int q = 0; q < 2 * NGLOBAL; ++q) {
-                red_add(tallies[acc_item].global + q, acc[q * bd]);
+                const double v = acc[q * bd];
+                if(v != 0.0) {
+                  if(sl) atomicAdd(sl + q, v);
+                  else red_add(tallies[acc_item].global + q, v);
+                }
                 acc[q * bd] = 0;
               }
             }
@@ -1471,20 +1481,21 @@ batch_kernel
           ++npaths;
         }
       }
-      if(rcvd) {
+      {
         /* Converged: the newest item fetched becomes the current slot */
         const bool fetched = (need >> lane) & 1u && !done;
         const int newest = __reduce_max_sync(0xffffffffu, fetched ? it : -1);
         if(newest >= 0 && newest != stag[cur]) {
           const int prv = cur ^ 1;
-          double* sl = wslots + prv * rcvd;
+          double* sl = wslots + prv * ss;
           __syncwarp();
           if(stag[prv] >= 0) {
+            if((int)lane < 2 * NGLOBAL) red_add(tallies[stag[prv]].global + lane, sl[lane]);
             double* dst = tallies[stag[prv]].rcv;
-            const int nd = scenes[stag[prv]].nrcv * NRCV_Q * 2;
-            for(int i = (int)lane; i < nd; i += 32) red_add(dst + i, sl[i]);
+            const int nd = rcvd ? scenes[stag[prv]].nrcv * NRCV_Q * 2 : 0;
+            for(int i = (int)lane; i < nd; i += 32) red_add(dst + i, sl[2 * NGLOBAL + i]);
           }
-          for(int i = (int)lane; i < rcvd; i += 32) sl[i] = 0;
+          for(int i = (int)lane; i < ss; i += 32) sl[i] = 0;
           __syncwarp();
           stag[prv] = newest;
           cur = prv;
@@ -1561,8 +1572,8 @@ batch_kernel
     if(end != END_NONE) {
       double* rb = nullptr;
       if(rcvd) {
-        if(it == stag[cur]) rb = wslots + cur * rcvd;
-        else if(it == stag[cur ^ 1]) rb = wslots + (cur ^ 1) * rcvd;
+        if(it == stag[cur]) rb = wslots + cur * ss + 2 * NGLOBAL;
+        else if(it == stag[cur ^ 1]) rb = wslots + (cur ^ 1) * ss + 2 * NGLOBAL;
       }
       commit_path(S, tallies[it], p, end, acc, ps, bd, rb, xr, xp, xv);
       p.phase = PH_NONE;
@@ -1570,15 +1581,22 @@ batch_kernel
   }
 
   if(acc_item >= 0) {
-    for(int q = 0; q < 2 * NGLOBAL; ++q)
-      red_add(tallies[acc_item].global + q, acc[q * bd]);
+    double* sl = acc_item == stag[cur] ? wslots + cur * ss
+      : acc_item == stag[cur ^ 1] ? wslots + (cur ^ 1) * ss : nullptr;
+    for(int q = 0; q < 2 * NGLOBAL; ++q) {
+      const double v = acc[q * bd];
+      if(v == 0.0) continue;
+      if(sl) atomicAdd(sl + q, v);
+      else red_add(tallies[acc_item].global + q, v);
+    }
   }
   __syncwarp();
-  for(int k = 0; k < 2 && rcvd; ++k) {
+  for(int k = 0; k < 2; ++k) {
     if(stag[k] < 0) continue;
+    if((int)lane < 2 * NGLOBAL) red_add(tallies[stag[k]].global + lane, wslots[k * ss + lane]);
     double* dst = tallies[stag[k]].rcv;
-    const int nd = scenes[stag[k]].nrcv * NRCV_Q * 2;
-    for(int i = (int)lane; i < nd; i += 32) red_add(dst + i, wslots[k * rcvd + i]);
+    const int nd = rcvd ? scenes[stag[k]].nrcv * NRCV_Q * 2 : 0;
+    for(int i = (int)lane; i < nd; i += 32) red_add(dst + i, wslots[k * ss + 2 * NGLOBAL + i]);
   }
   unsigned long long c[6] = {cnt.rays, cnt.nodes, cnt.tris, cnt.quads,
                              bounces, npaths};
@@ -1659,7 +1677,7 @@ static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg
   if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
   const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block) * sizeof(double)
                     + (size_t)SMEM_STACK * block * sizeof(int)
-                    + (size_t)(block / 32) * 2 * cfg.rcv_doubles * sizeof(double);
+                    + (size_t)(block / 32) * 2 * (2 * NGLOBAL + cfg.rcv_doubles) * sizeof(double);
   static bool attr_set = false;
   if(!attr_set) {
     cudaFuncSetAttribute(batch_kernel<R, MINB>,
@@ -1751,7 +1769,7 @@ static int launch_batch_noalloc_variant
   if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
   const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block) * sizeof(double)
                     + (size_t)SMEM_STACK * block * sizeof(int)
-                    + (size_t)(block / 32) * 2 * cfg.rcv_doubles * sizeof(double);
+                    + (size_t)(block / 32) * 2 * (2 * NGLOBAL + cfg.rcv_doubles) * sizeof(double);
   cudaFuncSetAttribute(batch_kernel<R, MINB>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
   int per_sm = 0;
