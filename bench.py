@@ -114,6 +114,19 @@ def measured_peaks():
         return {}
 
 
+def shard_first(step, rank, world, n):
+    """First realisation (relative to the RNG position) of `rank`'s share of
+    step `step`: every step hands each rank a disjoint range of n
+    realisation ids, so the ranks together trace exactly the ids a single
+    GPU would trace in world x more steps."""
+    return (step * world + rank) * n
+
+
+def shard_suns(suns, rank, world):
+    """Sun slots of `rank` in the batched form: every world-th sun."""
+    return suns[rank::world]
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -243,7 +256,7 @@ def run_b200(args):
                         device="cuda")
 
     def step(k):
-        first = (k * world + rank) * n
+        first = shard_first(k, rank, world, n)
         lib.call("ssol_b200_plan_launch", plan, rng, first, n, sp)
 
     for w in range(args.warmup):
@@ -400,7 +413,7 @@ def run_suns(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     lib = P.load_product()
-    suns = W.sun_grid()[rank::world]
+    suns = shard_suns(W.sun_grid(), rank, world)
     built = W.batched_fields(lib, suns, n_helio=args.heliostats)
     scenes = [b[0] for b in built]
     rcv = [b[1]["receiver"] for b in built]
