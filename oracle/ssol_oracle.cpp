@@ -191,6 +191,7 @@ struct OCarving { int op; std::vector<double> xy; };
 struct ssol_shape {
   Ref ref; ssol_device* dev; bool punched; bool ready = false;
   std::vector<float> pos; /* RT positions, shape space */
+  std::vector<float> nrm, uv; /* optional vertex normals and texcoords */
   std::vector<unsigned> ids;
   double rt_area = 0, samp_area = 0;
   /* punched */
@@ -665,9 +666,23 @@ API res_T ssol_mesh_setup(ssol_shape* s, const unsigned ntris,
     return RES_BAD_ARG;
   if(nattribs > SSOL_ATTRIBS_COUNT__) return RES_MEM_ERR;
   const ssol_vertex_data* pos = nullptr;
-  for(unsigned i = 0; i < nattribs; ++i)
+  const ssol_vertex_data* nrm = nullptr;
+  const ssol_vertex_data* tex = nullptr;
+  for(unsigned i = 0; i < nattribs; ++i) {
     if(attribs[i].usage == SSOL_POSITION) pos = &attribs[i];
+    else if(attribs[i].usage == SSOL_NORMAL) nrm = &attribs[i];
+    else if(attribs[i].usage == SSOL_TEXCOORD) tex = &attribs[i];
+  }
   if(!pos || !pos->get) return RES_BAD_ARG;
+  s->nrm.clear(); s->uv.clear();
+  if(nrm && nrm->get) {
+    s->nrm.resize(nverts * 3);
+    for(unsigned v = 0; v < nverts; ++v) nrm->get(v, &s->nrm[v * 3], data);
+  }
+  if(tex && tex->get) {
+    s->uv.resize(nverts * 2);
+    for(unsigned v = 0; v < nverts; ++v) tex->get(v, &s->uv[v * 2], data);
+  }
   std::vector<unsigned> ids(ntris * 3);
   for(unsigned t = 0; t < ntris; ++t) {
     get_ids(t, &ids[t * 3], data);
@@ -1235,7 +1250,17 @@ API res_T ssol_scene_attach_atmosphere(ssol_scene* s, ssol_atmosphere* a)
  ******************************************************************************/
 namespace {
 
-struct OTri { V v0, v1, v2; int sinst; unsigned prim; int gid; };
+struct OTri { V v0, v1, v2; int sinst; unsigned prim; int gid; int attr = -1; };
+/* Fragment inputs of a mesh triangle (src/ssol_material.c:551-655): world
+ * vertex normals through the inverse transpose of the instance, texcoords
+ * (or Star-3D's default (1,0), (0,1), (0,0)), dP/du and dP/dv, and per side
+ * the material whose shaders vary over the shape (evaluated per fragment) */
+struct OTriAttr {
+  bool has_n = false; V n[3];
+  double uv[3][2];
+  V dpdu, dpdv;
+  const ssol_material* vary[2] = {nullptr, nullptr};
+};
 struct OQuad {
   Affine l2w, w2l; const ssol_shape* shape; int sinst;
 };
@@ -1266,6 +1291,7 @@ struct Scene {
    * spectrum nodes: callbacks are host functions, evaluated once per solve
    * (the same wavelength-only rule as the device library) */
   std::map<const ssol_material*, std::vector<double>> shade_tab;
+  std::vector<OTriAttr> tattr;
 };
 
 /* Same deterministic Vose construction as the device library */
@@ -1388,6 +1414,108 @@ double buie_chi(double c)
 
 void tabulate(Scene& S, const ssol_material* m);
 
+/* Fragment of a mesh point (surface_fragment_setup, src/ssol_material.c:
+ * 551-655): P, dir, Ng (unit, facing the incoming dir), uv and Ns
+ * interpolated with the barycentric weights (1 - b1 - b2, b1, b2), Ns turned
+ * toward -dir, dP/du and dP/dv of the triangle */
+ssol_surface_fragment mesh_fragment(const OTriAttr& a, V P, V dir, V Ng, double b1,
+                                    double b2)
+{
+  ssol_surface_fragment f = SSOL_SURFACE_FRAGMENT_NULL;
+  const double b0 = 1 - b1 - b2;
+  f.P[0] = P.x; f.P[1] = P.y; f.P[2] = P.z;
+  f.dir[0] = dir.x; f.dir[1] = dir.y; f.dir[2] = dir.z;
+  f.Ng[0] = Ng.x; f.Ng[1] = Ng.y; f.Ng[2] = Ng.z;
+  V ns = Ng;
+  if(a.has_n) {
+    const V m = a.n[0] * b0 + a.n[1] * b1 + a.n[2] * b2;
+    const double l = std::sqrt(dot(m, m));
+    if(l > 0) {
+      ns = m * (1 / l);
+      if(dot(dir, ns) > 0) ns = -ns;
+    }
+  }
+  f.Ns[0] = ns.x; f.Ns[1] = ns.y; f.Ns[2] = ns.z;
+  f.uv[0] = a.uv[0][0] * b0 + a.uv[1][0] * b1 + a.uv[2][0] * b2;
+  f.uv[1] = a.uv[0][1] * b0 + a.uv[1][1] * b1 + a.uv[2][1] * b2;
+  f.dPdu[0] = a.dpdu.x; f.dPdu[1] = a.dpdu.y; f.dPdu[2] = a.dpdu.z;
+  f.dPdv[0] = a.dpdv.x; f.dPdv[1] = a.dpdv.y; f.dPdv[2] = a.dpdv.z;
+  return f;
+}
+
+/* Attributes of mesh triangle t of shape s under instance transform xf */
+OTriAttr tri_attr(const ssol_shape* s, unsigned t, const Affine& xf)
+{
+  OTriAttr a;
+  V p[3];
+  for(int k = 0; k < 3; ++k) {
+    const unsigned id = s->ids[t * 3 + k];
+    p[k] = xpoint(xf, v3(s->pos[id * 3], s->pos[id * 3 + 1], s->pos[id * 3 + 2]));
+    if(!s->uv.empty()) { a.uv[k][0] = s->uv[id * 2]; a.uv[k][1] = s->uv[id * 2 + 1]; }
+    else { a.uv[k][0] = k == 0 ? 1 : 0; a.uv[k][1] = k == 1 ? 1 : 0; }
+  }
+  Affine inv;
+  if(!s->nrm.empty() && inverse(xf, inv)) {
+    a.has_n = true;
+    for(int k = 0; k < 3; ++k) {
+      const unsigned id = s->ids[t * 3 + k];
+      /* inverse transpose of the instance's linear part */
+      a.n[k] = xvec_t(inv, v3(s->nrm[id * 3], s->nrm[id * 3 + 1], s->nrm[id * 3 + 2]));
+    }
+  }
+  const V e1 = p[1] - p[0], e2 = p[2] - p[0];
+  const double du1 = a.uv[1][0] - a.uv[0][0], dv1 = a.uv[1][1] - a.uv[0][1];
+  const double du2 = a.uv[2][0] - a.uv[0][0], dv2 = a.uv[2][1] - a.uv[0][1];
+  const double det = du1 * dv2 - dv1 * du2;
+  if(det == 0) {
+    V n = cross(e2, e1);
+    const double l = std::sqrt(dot(n, n));
+    n = l > 0 ? n * (1 / l) : v3(0, 0, 1);
+    onb(n, a.dpdu, a.dpdv);
+  } else {
+    a.dpdu = (e1 * dv2 - e2 * dv1) * (1 / det);
+    a.dpdv = (e2 * du1 - e1 * du2) * (1 / det);
+  }
+  return a;
+}
+
+/* Whether a mirror or matte material gives other shader values at the
+ * vertices of triangles t0 and t1 of a shape (seen from `side`) than at the
+ * reference fragment of the per-material table: the same probe as the B200
+ * library's, so that both evaluate the same materials per fragment */
+bool varies_over(const ssol_material* m, const ssol_shape* s, const Affine& xf,
+                 int side, double wl)
+{
+  if(m->type != SSOL_MATERIAL_MIRROR && m->type != SSOL_MATERIAL_MATTE) return false;
+  ssol_surface_fragment ref = SSOL_SURFACE_FRAGMENT_NULL;
+  ref.dir[2] = -1; ref.Ng[2] = 1; ref.Ns[2] = 1; ref.dPdu[0] = 1; ref.dPdv[1] = 1;
+  double r0 = 0, g0 = 0;
+  if(m->refl) m->refl(m->dev, m->buf, wl, &ref, &r0);
+  if(m->rough) m->rough(m->dev, m->buf, wl, &ref, &g0);
+  const unsigned nt = (unsigned)(s->ids.size() / 3);
+  const unsigned probe[2] = {0, nt - 1};
+  for(unsigned t : probe) {
+    const OTriAttr a = tri_attr(s, t, xf);
+    V p[3];
+    for(int k = 0; k < 3; ++k) {
+      const unsigned id = s->ids[t * 3 + k];
+      p[k] = xpoint(xf, v3(s->pos[id * 3], s->pos[id * 3 + 1], s->pos[id * 3 + 2]));
+    }
+    V ng = cross(p[2] - p[0], p[1] - p[0]);
+    const double l = std::sqrt(dot(ng, ng));
+    ng = (l > 0 ? ng * (1 / l) : v3(0, 0, 1)) * (side == 0 ? 1.0 : -1.0);
+    for(int k = 0; k < 3; ++k) {
+      const double b1 = k == 1 ? 1 : 0, b2 = k == 2 ? 1 : 0;
+      const ssol_surface_fragment f = mesh_fragment(a, p[k], -ng, ng, b1, b2);
+      double r = 0, g = 0;
+      if(m->refl) m->refl(m->dev, m->buf, wl, &f, &r);
+      if(m->rough) m->rough(m->dev, m->buf, wl, &f, &g);
+      if(r != r0 || g != g0) return true;
+    }
+  }
+  return false;
+}
+
 res_T make_scene(ssol_scene* scn, Scene& S)
 {
   if(!scn->sun || !scn->sun->spec || scn->sun->spec->wl.empty() || scn->sun->dni <= 0)
@@ -1432,6 +1560,7 @@ res_T make_scene(ssol_scene* scn, Scene& S)
   }
   std::vector<double> area;
   bool sampled = false;
+  std::map<std::pair<const ssol_material*, const ssol_shape*>, bool> varies;
   for(ssol_instance* inst : scn->inst) {
     if(inst->sample) {
       sampled = true;
@@ -1462,6 +1591,21 @@ res_T make_scene(ssol_scene* scn, Scene& S)
           const V p1 = v3(vf[1][0], vf[1][1], vf[1][2]);
           const V p2 = v3(vf[2][0], vf[2][1], vf[2][2]);
           OTri tr = {p0, p1, p2, si, (unsigned)t, first + (int)t};
+          const ssol_material* vary[2] = {nullptr, nullptr};
+          for(int sd = 0; sd < 2; ++sd) {
+            const ssol_material* m = sd == 0 ? sh.front : sh.back;
+            const auto key = std::make_pair(m, (const ssol_shape*)s);
+            auto f = varies.find(key);
+            if(f == varies.end())
+              f = varies.emplace(key, varies_over(m, s, inst->xf, sd, S.wl[0])).first;
+            if(f->second) vary[sd] = m;
+          }
+          if(!s->nrm.empty() || vary[0] || vary[1]) {
+            OTriAttr a = tri_attr(s, (unsigned)t, inst->xf);
+            a.vary[0] = vary[0]; a.vary[1] = vary[1];
+            tr.attr = (int)S.tattr.size();
+            S.tattr.push_back(a);
+          }
           S.tris.push_back(tr);
           if(inst->sample) {
             const V n = cross(p2 - p0, p1 - p0);
@@ -1522,7 +1666,7 @@ res_T make_scene(ssol_scene* scn, Scene& S)
 
 /* Ray query with the reference hit filter (src/ssol_scene.c:439-535) */
 struct Self { int gid; int sinst; int side; bool discard_virtual, reversed; };
-struct OHit { double t; int sinst; unsigned prim; int gid; V n; bool found; };
+struct OHit { double t; int sinst; unsigned prim; int gid; V n; bool found; double b1, b2; };
 
 bool side_ok(const Scene& S, int si, int side, const Self& self)
 {
@@ -1582,6 +1726,7 @@ void hit_tri(const Scene& S, int i, V o, V d, const OShear& sh, double tmin,
   if(!side_ok(S, T.sinst, side, self)) return;
   h.t = t; h.sinst = T.sinst; h.prim = T.prim; h.gid = T.gid;
   h.n = ng; h.found = true;
+  h.b1 = Vv / (U + Vv + W); h.b2 = W / (U + Vv + W);
 }
 
 unsigned grid_prim(const ssol_shape* s, double x, double y)
@@ -1629,6 +1774,7 @@ void hit_quad(const Scene& S, int i, V o, V d, double tmin, const Self& self, OH
     if(Q.sinst == self.sinst && side != self.side) continue;
     if(!side_ok(S, Q.sinst, side, self)) continue;
     h.t = t; h.sinst = Q.sinst; h.gid = -1; h.n = nw; h.found = true;
+    h.b1 = h.b2 = 0;
     h.prim = s->gexact ? grid_prim(s, pl.x, pl.y) : 0;
     break;
   }
@@ -1802,9 +1948,18 @@ double fresnel(double ci, double ct, double ei, double et)
 
 /* point_shade (src/ssol_solver.c:419-494); returns false on RES_BAD_OP */
 bool shade(const Scene& S, const PathRng& rng, uint32_t j, const ssol_material* m,
-           const ssol_medium& in, ssol_medium& out, double wl, V wo, V N,
-           double& prop, V& dir, int& type)
+           const ssol_medium& in, ssol_medium& out, double wl, V wo, V Ng,
+           double& prop, V& dir, int& type, V N, const ssol_surface_fragment* frag)
 {
+  /* N: shading normal (the fragment's Ns), Ng: geometric normal; shaders
+   * of a material that varies over its mesh are evaluated at the fragment */
+  auto sv = [&](int which) {
+    if(!frag) return shader(S, m, which, wl);
+    double v = 0;
+    ssol_shader_getter_T f = which == 0 ? m->refl : m->rough;
+    if(f) f(m->dev, m->buf, wl, frag, &v);
+    return v;
+  };
   prop = 0; type = 0;
   ssol_medium_copy(&out, &in);
   if(m->type == SSOL_MATERIAL_DIELECTRIC && !media_ceq(in, m->out)) return false;
@@ -1814,7 +1969,7 @@ bool shade(const Scene& S, const PathRng& rng, uint32_t j, const ssol_material* 
   V b1, b2;
   switch(m->type) {
     case SSOL_MATERIAL_MIRROR: {
-      const double R = shader(S, m, 0, wl), a = shader(S, m, 1, wl);
+      const double R = sv(0), a = sv(1);
       type = 1;
       if(a == 0) { dir = N * (2 * ci) - wo; prop = R; }
       else {
@@ -1843,7 +1998,7 @@ bool shade(const Scene& S, const PathRng& rng, uint32_t j, const ssol_material* 
       const double ph = 2 * M_PI * unif(r.x[1]);
       onb(N, b1, b2);
       dir = b1 * (rad * std::cos(ph)) + b2 * (rad * std::sin(ph)) + N * std::sqrt(1 - u0);
-      prop = shader(S, m, 0, wl);
+      prop = sv(0);
       type = 1;
       break;
     }
@@ -1882,13 +2037,26 @@ bool shade(const Scene& S, const PathRng& rng, uint32_t j, const ssol_material* 
     }
     default: break;
   }
-  const double c = dot(N, dir);
+  const double c = dot(Ng, dir);
   if((c > 0 && type == 2) || (c < 0 && type == 1)) prop = 0;
   return true;
 }
 
 McRcv1& rcv_side(std::map<const ssol_instance*, McRcv>& m, const ssol_instance* i, int side)
 { return m[i].side[side == 1 ? 0 : 1]; }
+
+/* Shading inputs of the point on triangle gid (or a quadric when gid < 0):
+ * the shading normal, and the fragment when the side's material varies */
+V shading_inputs(const Scene& S, int gid, int side, V pos, V dir, V N, double b1,
+                 double b2, ssol_surface_fragment& frag, bool& use_frag)
+{
+  use_frag = false;
+  if(gid < 0 || S.tris[gid].attr < 0) return N;
+  const OTriAttr& a = S.tattr[S.tris[gid].attr];
+  frag = mesh_fragment(a, pos, dir, N, b1, b2);
+  use_frag = a.vary[side - 1] != nullptr;
+  return v3(frag.Ns[0], frag.Ns[1], frag.Ns[2]);
+}
 
 /* One realisation (trace_radiative_path, src/ssol_solver.c:873-1127) */
 /* Tracked-path lengths after the defaults (src/ssol_solver.c:1211-1220) */
@@ -1912,6 +2080,7 @@ res_T realisation(const Scene& S, Ctx& ctx, size_t ireal, const PathRng& rng,
   const double sa = std::sqrt(unif(r0.x[2]));
   const double b2 = sa * unif(r0.x[3]), b1 = sa - b2;
   V pos = st.v0 + st.e1 * b1 + st.e2 * b2;
+  double cb1 = b1, cb2 = b2; /* barycentric weights of the current point */
   const Block r1 = rng.get(1, DOM_PRIMARY);
   V dir = sun_dir(S, rng, r1);
   const double wl = wl_sample(S, unif(r1.x[2]));
@@ -1981,7 +2150,11 @@ res_T realisation(const Scene& S, Ctx& ctx, size_t ireal, const PathRng& rng,
         ssol_medium_copy(&out, &in);
       } else {
         double prop; V nd = dir; int type;
-        if(!shade(S, rng, j++, mtl, in, out, wl, -dir, N, prop, nd, type)) {
+        ssol_surface_fragment frag;
+        bool use_frag;
+        const V Ns = shading_inputs(S, gid, side, pos, dir, N, cb1, cb2, frag, use_frag);
+        if(!shade(S, rng, j++, mtl, in, out, wl, -dir, N, prop, nd, type, Ns,
+                  use_frag ? &frag : nullptr)) {
           res = RES_BAD_OP; break;
         }
         kabs = 1 - prop;
@@ -2035,6 +2208,7 @@ res_T realisation(const Scene& S, Ctx& ctx, size_t ireal, const PathRng& rng,
       if(seg >= 1000000) { res = RES_BAD_OP; break; }
       /* point_update_from_hit */
       si = h.sinst; o = &S.sinst[si]; prim = h.prim; gid = h.gid;
+      cb1 = h.b1; cb2 = h.b2;
       N = unit(h.n);
       pos = org + rd * h.t;
       vtx(pos, outw[0]);
@@ -2206,7 +2380,11 @@ API res_T ssol_oracle_first_bounce
     if(trace(S, pos, -dir, 0, self, true).found) continue;
     ssol_medium in = S.air, out = S.air;
     double prop; V rd = dir; int type;
-    if(!shade(S, rg, 0, mtl, in, out, wl, -dir, N, prop, rd, type) || !(prop > 0)) continue;
+    ssol_surface_fragment frag;
+    bool use_frag;
+    const V Ns = shading_inputs(S, st.gid, side, pos, dir, N, b1, b2, frag, use_frag);
+    if(!shade(S, rg, 0, mtl, in, out, wl, -dir, N, prop, rd, type, Ns,
+              use_frag ? &frag : nullptr) || !(prop > 0)) continue;
     w *= prop;
     const Self s2 = {st.gid, st.sinst, side, false, false};
     const OHit h = trace(S, pos, rd, 0, s2, false);

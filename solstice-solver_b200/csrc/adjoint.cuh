@@ -153,10 +153,27 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
     if(dot(N, dir) >= R(0)) { side = 2; N = -N; }
     const DMaterial m = S.mtls[si.mtl[side - 1]];
     if(m.type != MTL_MIRROR) continue;
-    if(!(dot(-dir, N) > R(0))) continue;
+    /* Shading normal and baked shader values at the sampled point, as in
+     * shade() */
+    V3<R> Ns = N;
+    int bake = -1;
+    if(S.tshade && st.gid >= 0) {
+      const DTriShade<R>& ts = S.tshade[st.gid];
+      bake = ts.bake[side - 1];
+      if(!isnan(ts.n[0])) {
+        const V3<R> v = ld3(ts.n) * (R(1) - b1 - b2) + ld3(ts.n + 3) * b1
+                      + ld3(ts.n + 6) * b2;
+        const R l2 = dot(v, v);
+        if(l2 > R(0)) {
+          Ns = v * rsq(l2);
+          if(dot(Ns, -dir) < R(0)) Ns = -Ns;
+        }
+      }
+    }
+    if(!(dot(-dir, Ns) > R(0))) continue;
 
-    /* Point and normal with their tangents (zero for other instances) */
-    DV x = dv(vd(pos)), n = dv(vd(N));
+    /* Point and normals with their tangents (zero for other instances) */
+    DV x = dv(vd(pos)), n = dv(vd(N)), ns = dv(vd(Ns));
     if(slot >= 0) {
       const double* ax = A.axes + 9 * slot;
       const V3<double> c = mk(ax[0], ax[1], ax[2]);
@@ -165,6 +182,7 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
       x = with_tangents(vd(pos) - c, ex, ey);
       x.x.v += c.x; x.y.v += c.y; x.z.v += c.z;
       n = with_tangents(vd(N), ex, ey);
+      ns = with_tangents(vd(Ns), ex, ey);
     }
     const V3<double> sdir = vd(dir);
     const V3<R> sun0 = ld3(S.sun_dir);
@@ -183,12 +201,14 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
     if(trace_ray(S, pos, -dir, R(0), self, true, h, cnt, stack, stride)) continue;
 
     /* Mirror reflection with the draws of shade() (scatter event 0) */
-    const R refl = shader_value(S, m, 0, wl);
-    const R rough = shader_value(S, m, 1, wl);
+    const R refl = bake >= 0 ? baked_value(S, bake, 0, wl, b1, b2)
+                             : shader_value(S, m, 0, wl);
+    const R rough = bake >= 0 ? baked_value(S, bake, 1, wl, b1, b2)
+                              : shader_value(S, m, 1, wl);
     const V3<double> wo = -sdir;
     DV out;
     if(rough == R(0)) {
-      out = n * (2.0 * ddot(n, wo));
+      out = ns * (2.0 * ddot(ns, wo));
       out.x = out.x - wo.x; out.y = out.y - wo.y; out.z = out.z - wo.z;
     } else {
       bool ok = false;
@@ -203,13 +223,13 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
         const R stn = sq_rt(tan2) * ct;
         R sp, cp; sincos2pi(uni<R>(rr.v[1]), &sp, &cp);
         DV e1, e2;
-        donb(n, e1, e2);
-        const DV hh = e1 * (double)(cp * stn) + e2 * (double)(sp * stn) + n * (double)ct;
+        donb(ns, e1, e2);
+        const DV hh = e1 * (double)(cp * stn) + e2 * (double)(sp * stn) + ns * (double)ct;
         const Dd wh = ddot(hh, wo);
         if(!(wh.v > 0.0)) continue;
         out = hh * (2.0 * wh);
         out.x = out.x - wo.x; out.y = out.y - wo.y; out.z = out.z - wo.z;
-        ok = ddot(out, n).v > 0.0;
+        ok = ddot(out, ns).v > 0.0;
       }
       if(!ok) continue;
     }
@@ -227,7 +247,11 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
     if(!(hs.receiver_mask & hside)) continue;
     const DMaterial hm = S.mtls[hs.mtl[hside - 1]];
     if(hm.type != MTL_MIRROR && hm.type != MTL_MATTE) continue;
-    const double kabs = 1.0 - (double)shader_value(S, hm, 0, wl);
+    const int hbake = S.tshade ? S.tshade[h.gid].bake[hside - 1] : -1;
+    float2 huv = make_float2(0.f, 0.f);
+    if(hbake >= 0) huv = tri_uv(S, h.gid, pos + rd * h.t);
+    const double kabs = 1.0 - (double)(hbake >= 0
+      ? baked_value(S, hbake, 0, wl, (R)huv.x, (R)huv.y) : shader_value(S, hm, 0, wl));
 
     /* Distance to the hit triangle's plane and hit point, with tangents */
     const DTri<R>& T = S.tris[h.gid];

@@ -131,6 +131,16 @@ template<typename R> struct alignas(16) DTri {
   int32_t gid; /* global triangle index (self-hit test) */
 };
 
+/* Shading attributes of a mesh triangle, present only in scenes that need
+ * them: world-space vertex normals (n[0] is NaN when the mesh has none) and,
+ * per side (front, back), the offset in DScene::bake_tab of shader values
+ * baked at the three vertices (-1: the material's tabulated constants).
+ * A baked block is [vertex 0..2][wavelength node][reflectivity, roughness]. */
+template<typename R> struct alignas(16) DTriShade {
+  R n[9];
+  int32_t bake[2];
+};
+
 /* Analytic punched quadric patch */
 template<typename R> struct alignas(16) DQuadric {
   R w2l[12]; /* world -> local: rows 0..2 of a 3x4 affine map (row major) */
@@ -222,6 +232,9 @@ template<typename R> struct DScene {
   int32_t air_medium;
   double area_proxy; /* sampled_area_proxy */
   double area_rt; /* sampled_area */
+
+  const DTriShade<R>* tshade; /* per triangle, or nullptr */
+  const R* bake_tab; /* baked per-vertex shader values */
 
   int32_t nrcv; /* receiver-side slots */
   int32_t nsampled; /* sampled instances */

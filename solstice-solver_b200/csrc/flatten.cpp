@@ -10,6 +10,8 @@
 #include <limits>
 #include <map>
 
+void ssolb_d33_invtrans(double out[9], const double m[9]); /* objects.cpp */
+
 namespace ssolb {
 
 namespace {
@@ -206,6 +208,108 @@ void tabulate_shaders(FlatScene<R>& out, ssol_material* m, ssol_device* dev)
   }
 }
 
+/* Fragments of the three vertices of mesh triangle t seen from `side`
+ * (0 front, 1 back), with the fields of surface_fragment_setup
+ * (src/ssol_material.c:551-655): P the vertex, Ng the side's unit normal, dir
+ * = -Ng, uv the vertex texcoord or Star-3D's default (1,0), (0,1), (0,0), Ns
+ * the vertex normal through the inverse transpose of the instance (or Ng),
+ * turned toward -dir, dPdu and dPdv of the triangle. */
+void vertex_fragments(const ssol_shape* shape, int t, const double T[12],
+                      const double Rn[9], int side, ssol_surface_fragment f[3])
+{
+  double v[3][3];
+  for(int k = 0; k < 3; ++k) {
+    const uint32_t id = shape->ids[(size_t)t * 3 + k];
+    const double p[3] = {shape->pos[id * 3 + 0], shape->pos[id * 3 + 1],
+                         shape->pos[id * 3 + 2]};
+    apply(T, p, v[k]);
+  }
+  double e1[3], e2[3], n[3];
+  for(int c = 0; c < 3; ++c) { e1[c] = v[1][c] - v[0][c]; e2[c] = v[2][c] - v[0][c]; }
+  n[0] = e2[1] * e1[2] - e2[2] * e1[1];
+  n[1] = e2[2] * e1[0] - e2[0] * e1[2];
+  n[2] = e2[0] * e1[1] - e2[1] * e1[0];
+  double len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  if(!(len > 0)) len = 1;
+  const double sgn = side == 0 ? 1.0 : -1.0;
+  double ng[3];
+  for(int c = 0; c < 3; ++c) ng[c] = sgn * n[c] / len;
+  double uv[3][2] = {{1, 0}, {0, 1}, {0, 0}};
+  if(!shape->uv.empty())
+    for(int k = 0; k < 3; ++k) {
+      const uint32_t id = shape->ids[(size_t)t * 3 + k];
+      uv[k][0] = shape->uv[id * 2 + 0];
+      uv[k][1] = shape->uv[id * 2 + 1];
+    }
+  const double duv1[2] = {uv[1][0] - uv[0][0], uv[1][1] - uv[0][1]};
+  const double duv2[2] = {uv[2][0] - uv[0][0], uv[2][1] - uv[0][1]};
+  const double det = duv1[0] * duv2[1] - duv1[1] * duv2[0];
+  double dpdu[3], dpdv[3];
+  if(det == 0) {
+    /* any orthonormal tangents of Ng (Duff et al. basis) */
+    const double s2 = ng[2] >= 0 ? 1.0 : -1.0;
+    const double a = -1.0 / (s2 + ng[2]), b = ng[0] * ng[1] * a;
+    dpdu[0] = 1 + s2 * ng[0] * ng[0] * a; dpdu[1] = s2 * b; dpdu[2] = -s2 * ng[0];
+    dpdv[0] = b; dpdv[1] = s2 + ng[1] * ng[1] * a; dpdv[2] = -ng[1];
+  } else {
+    for(int c = 0; c < 3; ++c) {
+      dpdu[c] = (e1[c] * duv2[1] - e2[c] * duv1[1]) / det;
+      dpdv[c] = (e2[c] * duv1[0] - e1[c] * duv2[0]) / det;
+    }
+  }
+  for(int k = 0; k < 3; ++k) {
+    ssol_surface_fragment& fr = f[k];
+    fr = SSOL_SURFACE_FRAGMENT_NULL;
+    for(int c = 0; c < 3; ++c) {
+      fr.P[c] = v[k][c];
+      fr.Ng[c] = ng[c];
+      fr.dir[c] = -ng[c];
+      fr.Ns[c] = ng[c];
+      fr.dPdu[c] = dpdu[c];
+      fr.dPdv[c] = dpdv[c];
+    }
+    fr.uv[0] = uv[k][0];
+    fr.uv[1] = uv[k][1];
+    if(!shape->nrm.empty()) {
+      const uint32_t id = shape->ids[(size_t)t * 3 + k];
+      const double m[3] = {shape->nrm[id * 3 + 0], shape->nrm[id * 3 + 1],
+                           shape->nrm[id * 3 + 2]};
+      double w[3], l = 0;
+      for(int c = 0; c < 3; ++c) {
+        w[c] = Rn[c] * m[0] + Rn[3 + c] * m[1] + Rn[6 + c] * m[2];
+        l += w[c] * w[c];
+      }
+      l = std::sqrt(l);
+      if(l > 0) {
+        double d = 0;
+        for(int c = 0; c < 3; ++c) { w[c] /= l; d += fr.dir[c] * w[c]; }
+        for(int c = 0; c < 3; ++c) fr.Ns[c] = d > 0 ? -w[c] : w[c];
+      }
+    }
+  }
+}
+
+/* Whether a mirror or matte material's shaders give other values at the
+ * vertex fragments of a shape than at the reference fragment used for the
+ * per-material table (then they are baked per vertex) */
+bool material_varies(ssol_material* m, const ssol_surface_fragment* f, int nf,
+                     double wl, ssol_device* dev)
+{
+  if(m->type != SSOL_MATERIAL_MIRROR && m->type != SSOL_MATERIAL_MATTE) return false;
+  ssol_surface_fragment ref = SSOL_SURFACE_FRAGMENT_NULL;
+  ref.dir[2] = -1; ref.Ng[2] = 1; ref.Ns[2] = 1; ref.dPdu[0] = 1; ref.dPdv[1] = 1;
+  double r0 = 0, g0 = 0;
+  if(m->reflectivity) m->reflectivity(dev, m->buf, wl, &ref, &r0);
+  if(m->roughness) m->roughness(dev, m->buf, wl, &ref, &g0);
+  for(int i = 0; i < nf; ++i) {
+    double r = 0, g = 0;
+    if(m->reflectivity) m->reflectivity(dev, m->buf, wl, &f[i], &r);
+    if(m->roughness) m->roughness(dev, m->buf, wl, &f[i], &g);
+    if(r != r0 || g != g0) return true;
+  }
+  return false;
+}
+
 /* Quadric patch bounds: local z range over the carving AABB */
 void quadric_z_range(const ssol_shape* s, double& zlo, double& zhi)
 {
@@ -352,6 +456,11 @@ static res_T flatten_impl
   /* Receivers and sampled instances, in attach order */
   bool has_sampled = false, has_receiver = false;
   std::vector<PrimBox> boxes;
+  /* Shading attributes (vertex normals, baked spatially varying shaders),
+   * one record per triangle, kept only if some triangle needs one */
+  std::vector<DTriShade<R>> tsh;
+  bool need_tshade = false;
+  std::map<std::pair<const ssol_material*, const ssol_shape*>, bool> varies;
   std::vector<double> samp_area;
   for(size_t ii = 0; ii < scn->instances.size(); ++ii) {
     ssol_instance* inst = scn->instances[ii];
@@ -408,6 +517,29 @@ static res_T flatten_impl
 
       if(shape->kind == SHAPE_MESH) {
         const int first_gid = (int)out.tris.size();
+        /* Normals go through the inverse transpose of the instance
+         * (src/ssol_material.c:632-646); a side's shaders are baked per vertex
+         * when they vary over the shape */
+        double Rn[9];
+        ssolb_d33_invtrans(Rn, T);
+        ssol_material* side_mtl[2] = {ss.front, ss.back};
+        bool bake_side[2] = {false, false};
+        for(int sd = 0; sd < 2; ++sd) {
+          const auto key = std::make_pair((const ssol_material*)side_mtl[sd],
+                                          (const ssol_shape*)shape);
+          auto found = varies.find(key);
+          if(found == varies.end()) {
+            ssol_surface_fragment fr[6];
+            vertex_fragments(shape, 0, T, Rn, sd, fr);
+            vertex_fragments(shape, ntris - 1, T, Rn, sd, fr + 3);
+            found = varies.emplace(key, material_varies(side_mtl[sd], fr, 6,
+                                                        out.shader_wl[0], dev)).first;
+          }
+          bake_side[sd] = found->second;
+        }
+        const bool has_n = !shape->nrm.empty();
+        const bool attrs = has_n || bake_side[0] || bake_side[1];
+        if(attrs) need_tshade = true;
         for(int t = 0; t < ntris; ++t) {
           double v[3][3];
           float vf[3][3];
@@ -437,6 +569,35 @@ static res_T flatten_impl
           box.ref = primref_make(PRIM_TRIANGLE, (uint32_t)out.tris.size());
           out.tris.push_back(tri);
           boxes.push_back(box);
+          DTriShade<R> ts;
+          for(int c = 0; c < 9; ++c) ts.n[c] = R(0);
+          ts.n[0] = std::numeric_limits<R>::quiet_NaN();
+          ts.bake[0] = ts.bake[1] = -1;
+          if(has_n) {
+            for(int k = 0; k < 3; ++k) {
+              const uint32_t id = shape->ids[(size_t)t * 3 + k];
+              const double m[3] = {shape->nrm[id * 3 + 0], shape->nrm[id * 3 + 1],
+                                   shape->nrm[id * 3 + 2]};
+              for(int c = 0; c < 3; ++c)
+                ts.n[3 * k + c] = (R)(Rn[c] * m[0] + Rn[3 + c] * m[1] + Rn[6 + c] * m[2]);
+            }
+          }
+          for(int sd = 0; sd < 2 && attrs; ++sd) {
+            if(!bake_side[sd]) continue;
+            ssol_surface_fragment fr[3];
+            vertex_fragments(shape, t, T, Rn, sd, fr);
+            ts.bake[sd] = (int32_t)out.bake_tab.size();
+            ssol_material* m = side_mtl[sd];
+            for(int k = 0; k < 3; ++k)
+              for(double wl : out.shader_wl) {
+                double refl = 0, rough = 0;
+                if(m->reflectivity) m->reflectivity(dev, m->buf, wl, &fr[k], &refl);
+                if(m->roughness) m->roughness(dev, m->buf, wl, &fr[k], &rough);
+                out.bake_tab.push_back((R)refl);
+                out.bake_tab.push_back((R)rough);
+              }
+          }
+          tsh.push_back(ts);
           if(inst->sample) {
             DSampTri<R> st;
             double n[3], e1[3], e2[3];
@@ -597,6 +758,8 @@ static res_T flatten_impl
   if(!has_receiver) dev->log_warning("No receiver is defined.\n");
 
   build_alias(samp_area, out.alias_prob, out.alias_idx);
+  if(need_tshade) out.tshade = std::move(tsh);
+
   /* Bounding box of the ray-traced geometry (src/ssol_solver.c:563-570 uses
    * the scene view's box for the tracked segments to and from infinity) */
   for(int c = 0; c < 3; ++c) {

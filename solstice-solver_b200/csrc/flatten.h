@@ -55,6 +55,8 @@ template<class R> struct FlatScene {
   std::vector<double> spec_wl, spec_val;
   std::vector<R> shader_tab;
   std::vector<double> shader_wl;
+  std::vector<DTriShade<R>> tshade; /* empty when no triangle needs it */
+  std::vector<R> bake_tab;
   std::vector<DSampTri<R>> samp;
   std::vector<float> alias_prob;
   std::vector<int32_t> alias_idx;

@@ -140,10 +140,9 @@ __device__ __forceinline__ double data_value
 /* Shader value of a material at wavelength wl: index 0 reflectivity,
  * 1 roughness */
 template<class R>
-__device__ __forceinline__ R shader_value
-  (const DScene<R>& S, const DMaterial& m, int which, double wl)
+__device__ __forceinline__ R shader_lerp
+  (const DScene<R>& S, const R* tab, int which, double wl)
 {
-  const R* tab = S.shader_tab + m.table;
   const int n = S.shader_nodes;
   if(n == 1) return tab[which];
   const double* w = S.shader_wl;
@@ -156,6 +155,26 @@ __device__ __forceinline__ R shader_value
   if(lo == 0) return tab[which];
   const double a = tab[2 * (lo - 1) + which], b = tab[2 * lo + which];
   return (R)(a + (wl - w[lo - 1]) * (b - a) / (w[lo] - w[lo - 1]));
+}
+
+template<class R>
+__device__ __forceinline__ R shader_value
+  (const DScene<R>& S, const DMaterial& m, int which, double wl)
+{ return shader_lerp(S, S.shader_tab + m.table, which, wl); }
+
+/* Shader value baked at the vertices of a triangle side (offset `bake` in
+ * bake_tab), interpolated in wavelength then with the barycentric weights
+ * (1 - b1 - b2, b1, b2) of the point */
+template<class R>
+__device__ __forceinline__ R baked_value
+  (const DScene<R>& S, int bake, int which, double wl, R b1, R b2)
+{
+  const R* tab = S.bake_tab + bake;
+  const int stride = 2 * S.shader_nodes;
+  const R v0 = shader_lerp(S, tab, which, wl);
+  const R v1 = shader_lerp(S, tab + stride, which, wl);
+  const R v2 = shader_lerp(S, tab + 2 * stride, which, wl);
+  return v0 * (R(1) - b1 - b2) + v1 * b1 + v2 * b2;
 }
 
 /*******************************************************************************
@@ -688,6 +707,40 @@ __device__ bool trace_ray
   return found;
 }
 
+/* Per-thread FP64 path sums kept in shared memory (column `tid`, stride
+ * blockDim): the first receiver entry's 6 values, the 3 global quantities
+ * accumulated along the path and the cosine factor */
+enum : int { PS_V0 = 0, PS_ABS = 6, PS_ATM = 7, PS_OTHER = 8, PS_COS = 9,
+             PS_UV = 10, PS_COUNT = 11 };
+
+/* Barycentric weights (b1, b2) of vertices 1 and 2 of triangle gid at the
+ * point x of its plane */
+template<class R>
+__device__ __forceinline__ float2 tri_uv(const DScene<R>& S, int gid, V3<R> x)
+{
+  const DTri<R>& T = S.tris[gid];
+  const V3<R> a = ld3(T.v0);
+  const V3<R> e1 = ld3(T.v1) - a, e2 = ld3(T.v2) - a, q = x - a;
+  const R d11 = dot(e1, e1), d12 = dot(e1, e2), d22 = dot(e2, e2);
+  const R q1 = dot(q, e1), q2 = dot(q, e2);
+  const R den = d11 * d22 - d12 * d12;
+  if(!(den != R(0))) return make_float2(0.f, 0.f);
+  return make_float2((float)((d22 * q1 - d12 * q2) / den),
+                     (float)((d11 * q2 - d12 * q1) / den));
+}
+
+/* Barycentric weights (b1, b2) of the current point, kept as two floats in
+ * the PS_UV slot when the scene has shading attributes */
+__device__ __forceinline__ void put_uv(double* ps, int stride, float b1, float b2)
+{
+  float2* q = reinterpret_cast<float2*>(ps + PS_UV * stride);
+  *q = make_float2(b1, b2);
+}
+__device__ __forceinline__ float2 get_uv(const double* ps, int stride)
+{
+  return *reinterpret_cast<const float2*>(ps + PS_UV * stride);
+}
+
 /*******************************************************************************
  * BSDF sampling (Star-SF's BSDFs restated from published optics: Fresnel
  * equations, Walter et al. 2007 microfacet sampling, thin-slab series)
@@ -715,8 +768,8 @@ __device__ __forceinline__ V3<R> local_to(V3<R> n, R x, R y, R z)
 template<class R>
 __device__ __noinline__ bool shade
   (const DScene<R>& S, const Rng& rng, uint32_t scatter, int mtl_idx,
-   int medium, double wl, V3<R> wo, V3<R> N, R& prop, V3<R>& out,
-   int& type, int& next_medium)
+   int medium, double wl, V3<R> wo, V3<R> Ng, R& prop, V3<R>& out,
+   int& type, int& next_medium, int gid, int side, const double* ps, int stride)
 {
   const DMaterial m = S.mtls[mtl_idx];
   prop = R(0);
@@ -724,13 +777,37 @@ __device__ __noinline__ bool shade
   next_medium = medium;
   /* src/ssol_material.c:97-101 */
   if(m.type == MTL_DIELECTRIC && medium != m.out_medium) return false;
+  /* Shading normal: the interpolated vertex normal turned toward the
+   * incoming side, else Ng (src/ssol_material.c:630-654); shader values
+   * baked per vertex where the material varies over the mesh */
+  V3<R> N = Ng;
+  int bake = -1;
+  R b1 = R(0), b2 = R(0);
+  if(S.tshade && gid >= 0) {
+    const float2 uv = get_uv(ps, stride);
+    b1 = (R)uv.x;
+    b2 = (R)uv.y;
+    const DTriShade<R>& ts = S.tshade[gid];
+    bake = ts.bake[side - 1];
+    if(!isnan(ts.n[0])) {
+      const V3<R> ns = ld3(ts.n) * (R(1) - b1 - b2) + ld3(ts.n + 3) * b1
+                     + ld3(ts.n + 6) * b2;
+      const R l2 = dot(ns, ns);
+      if(l2 > R(0)) {
+        N = ns * rsq(l2);
+        if(dot(N, wo) < R(0)) N = -N;
+      }
+    }
+  }
   const R cos_i = dot(wo, N);
   if(!(cos_i > R(0))) return true;
   const U32x4 r = rng.get(scatter, RNG_SCATTER);
   switch(m.type) {
     case MTL_MIRROR: {
-      const R refl = shader_value(S, m, 0, wl);
-      const R rough = shader_value(S, m, 1, wl);
+      const R refl = bake >= 0 ? baked_value(S, bake, 0, wl, b1, b2)
+                               : shader_value(S, m, 0, wl);
+      const R rough = bake >= 0 ? baked_value(S, bake, 1, wl, b1, b2)
+                                : shader_value(S, m, 1, wl);
       type = BXDF_REFLECTION;
       if(rough == R(0)) {
         out = N * (R(2) * cos_i) - wo;
@@ -766,7 +843,7 @@ __device__ __noinline__ bool shade
       const R rad = sq_rt(u0);
       R sp, cp; sincos2pi(uni<R>(r.v[1]), &sp, &cp);
       out = local_to(N, rad * cp, rad * sp, sq_rt(R(1) - u0));
-      prop = shader_value(S, m, 0, wl);
+      prop = bake >= 0 ? baked_value(S, bake, 0, wl, b1, b2) : shader_value(S, m, 0, wl);
       type = BXDF_REFLECTION;
       break;
     }
@@ -818,8 +895,9 @@ __device__ __noinline__ bool shade
     }
     default: break;
   }
-  /* Wrong hemisphere for the sampled component (src/ssol_solver.c:468-475) */
-  const R cos_out = dot(N, out);
+  /* Wrong hemisphere for the sampled component, against the geometric
+   * normal (src/ssol_solver.c:468-475) */
+  const R cos_out = dot(Ng, out);
   if((cos_out > R(0) && (type & BXDF_TRANSMISSION))
   || (cos_out < R(0) && (type & BXDF_REFLECTION)))
     prop = R(0);
@@ -901,12 +979,6 @@ template<class R> struct PathState {
   bool overflow;
 };
 
-/* Per-thread FP64 path sums kept in shared memory (column `tid`, stride
- * blockDim): the first receiver entry's 6 values, the 3 global quantities
- * accumulated along the path and the cosine factor */
-enum : int { PS_V0 = 0, PS_ABS = 6, PS_ATM = 7, PS_OTHER = 8, PS_COS = 9,
-             PS_COUNT = 10 };
-
 /* point_init (src/ssol_solver.c:207-352) up to the shadow ray */
 template<class R>
 __device__ __forceinline__ void init_path
@@ -923,6 +995,7 @@ __device__ __forceinline__ void init_path
   const R b1 = sa - b2;
   V3<R> pos = ld3(st.v0) + ld3(st.e1) * b1 + ld3(st.e2) * b2;
   const V3<R> nproxy = ld3(st.n);
+  if(S.tshade) put_uv(ps, stride, (float)b1, (float)b2);
 
   const U32x4 r1 = rng.get(1u, RNG_PRIMARY);
   const V3<R> dir = sample_sun_dir(S, rng, r1);
@@ -1041,7 +1114,7 @@ __device__ int interact
     int type;
     ++bounces;
     if(!shade(S, rng, p.scatter++, si.mtl[p.side - 1], p.medium, p.wl, -dir,
-              p.N, prop, ndir, type, out_medium))
+              p.N, prop, ndir, type, out_medium, p.gid, p.side, ps, stride))
       return END_FAIL;
     const double pr = (double)prop;
     kabs = 1.0 - pr;
@@ -1331,6 +1404,10 @@ realisation_kernel
           dir = p.rd;
           p.N = normalize(h.n);
           pos = p.org + p.rd * h.t;
+          if(S.tshade && h.gid >= 0) {
+            const float2 uv = tri_uv(S, h.gid, pos);
+            put_uv(ps, bd, uv.x, uv.y);
+          }
           if(TRACK && p.tslot >= 0)
             track_vertex(tr, p, pos, p.virt ? p.inc0 : p.prev[0]);
           p.side = dot(p.rd, p.N) < R(0) ? 1 : 2;
@@ -1559,6 +1636,10 @@ batch_kernel
           dir = p.rd;
           p.N = normalize(h.n);
           pos = p.org + p.rd * h.t;
+          if(S.tshade && h.gid >= 0) {
+            const float2 uv = tri_uv(S, h.gid, pos);
+            put_uv(ps, bd, uv.x, uv.y);
+          }
           p.side = dot(p.rd, p.N) < R(0) ? 1 : 2;
           if(p.side == 2) p.N = -p.N;
           p.hit_t = h.t;

@@ -341,6 +341,9 @@ static void bind_scene(DScene<R>& S, const FlatScene<R>& f, const Blob& b,
   S.wl_nodes = (const double*)ptr();
   S.wl_pdf = (const double*)ptr();
   S.wl_cdf = (const double*)ptr();
+  S.tshade = (const DTriShade<R>*)ptr();
+  S.bake_tab = (const R*)ptr();
+  if(f.tshade.empty()) S.tshade = nullptr;
   S.shader_nodes = (int32_t)f.shader_wl.size();
   S.nsamp = (int32_t)f.samp.size();
   S.sun_type = f.sun_type;
@@ -380,6 +383,14 @@ static bool validate(const FlatScene<R>& f)
         if(n.child[k] < 0 || (int64_t)n.child[k] + n.count[k] > nrefs) return false;
       }
     }
+  }
+  if(!f.tshade.empty()) {
+    if(f.tshade.size() != f.tris.size()) return false;
+    const int64_t block = 6 * (int64_t)f.shader_wl.size();
+    for(const DTriShade<R>& t : f.tshade)
+      for(int k = 0; k < 2; ++k)
+        if(t.bake[k] < -1 || (t.bake[k] >= 0 && t.bake[k] + block > (int64_t)f.bake_tab.size()))
+          return false;
   }
   for(uint32_t ref : f.bvh.primrefs) {
     const uint32_t i = primref_index(ref);
@@ -460,6 +471,8 @@ static void add_scene(Blob& b, const FlatScene<R>& f)
   b.add(f.wl_nodes);
   b.add(f.wl_pdf);
   b.add(f.wl_cdf);
+  b.add(f.tshade);
+  b.add(f.bake_tab);
 }
 
 template<class R>
@@ -486,6 +499,8 @@ static res_T upload(ssol_b200_plan* p, const FlatScene<R>& f, DScene<R>& S)
   b.add(f.wl_nodes);
   b.add(f.wl_pdf);
   b.add(f.wl_cdf);
+  b.add(f.tshade);
+  b.add(f.bake_tab);
   const size_t bytes = b.host.size() + 256;
   if(dev_alloc(p->dev, &p->d_scene, bytes) != cudaSuccess) return RES_MEM_ERR;
   p->scene_alloc = bytes;

@@ -465,7 +465,8 @@ class Scene:
         return m
 
     # ---- shapes
-    def mesh(self, vertices, indices):
+    def mesh(self, vertices, indices, normals=None, texcoords=None):
+        """Mesh with optional per-vertex normals and texcoords."""
         h = self._new("ssol_shape_create_mesh", "ssol_shape_ref_put", self.dev)
         verts = [tuple(map(float, v)) for v in vertices]
         ids = [tuple(map(int, t)) for t in indices]
@@ -474,16 +475,26 @@ class Scene:
             t = ids[i]
             out[0], out[1], out[2] = t
 
-        def get_pos(i, out, ctx):
-            v = verts[i]
-            out[0], out[1], out[2] = v
+        def floats(values, n):
+            vals = [tuple(map(float, v)) for v in values]
+
+            def get(i, out, ctx):
+                for k in range(n):
+                    out[k] = vals[i][k]
+            return GET_FLOATS(get)
         cb_ids = GET_IDS(get_ids)
-        cb_pos = GET_FLOATS(get_pos)
-        self._keep += [cb_ids, cb_pos]
-        attr = (VertexData * 1)()
-        attr[0].usage = SSOL_POSITION
-        attr[0].get = cb_pos
-        self.lib.call("ssol_mesh_setup", h, len(ids), cb_ids, len(verts), attr, 1, None)
+        cbs = [(SSOL_POSITION, floats(verts, 3))]
+        if normals is not None:
+            cbs.append((SSOL_NORMAL, floats(normals, 3)))
+        if texcoords is not None:
+            cbs.append((SSOL_TEXCOORD, floats(texcoords, 2)))
+        self._keep += [cb_ids] + [c for _, c in cbs]
+        attr = (VertexData * len(cbs))()
+        for k, (usage, cb) in enumerate(cbs):
+            attr[k].usage = usage
+            attr[k].get = cb
+        self.lib.call("ssol_mesh_setup", h, len(ids), cb_ids, len(verts), attr, len(cbs),
+                      None)
         return h
 
     def rectangle(self, hx, hy):
@@ -529,8 +540,16 @@ class Scene:
 
     # ---- materials
     def _const(self, value):
-        def f(dev, buf, wl, frag, out):
-            out[0] = value
+        """Shader callback: a constant, or a Python function f(wl, frag)
+        of the wavelength and the surface fragment (P, Ng, Ns, uv, ...)"""
+        if callable(value):
+            fn = value
+
+            def f(dev, buf, wl, frag, out):
+                out[0] = float(fn(wl, frag[0]))
+        else:
+            def f(dev, buf, wl, frag, out):
+                out[0] = value
         cb = SHADER(f)
         self._keep.append(cb)
         return cb

@@ -1,0 +1,23 @@
+"""The oracle on spatially varying shaders and vertex normals: the shaders of
+a material that varies over its mesh are called at every hit's surface
+fragment (reference semantics), and the BSDF follows the interpolated
+vertex normal. Closed forms in attr_scenes."""
+import pytest
+
+import attr_scenes as A
+
+
+@pytest.mark.parametrize("kind", ["P", "uv"])
+def test_oracle_varying_reflectivity(oracle, kind):
+    s, h = A.ramp_mirror(oracle, kind)
+    e = s.solve(40000, seed=2)
+    r = e.receiver(h["receiver"])["incoming_flux"]
+    assert abs(r[0] - h["expected"]) <= 3 * r[2]
+    assert r[2] > 0  # the weight varies from path to path
+
+
+def test_oracle_vertex_normals(oracle):
+    s, h = A.tilted_normals(oracle)
+    e = s.solve(20000, seed=3)
+    r = e.receiver(h["receiver"])["incoming_flux"]
+    assert r[0] == pytest.approx(h["expected"], rel=1e-9)
