@@ -529,11 +529,20 @@ static res_T flatten_impl
                                           (const ssol_shape*)shape);
           auto found = varies.find(key);
           if(found == varies.end()) {
-            ssol_surface_fragment fr[6];
-            vertex_fragments(shape, 0, T, Rn, sd, fr);
-            vertex_fragments(shape, ntris - 1, T, Rn, sd, fr + 3);
-            found = varies.emplace(key, material_varies(side_mtl[sd], fr, 6,
-                                                        out.shader_wl[0], dev)).first;
+            /* Probe the vertices of up to 8 triangles spread over the mesh
+             * at both ends of the wavelength grid */
+            const int nprobe = std::min(ntris, 8);
+            std::vector<ssol_surface_fragment> fr((size_t)nprobe * 3);
+            for(int i = 0; i < nprobe; ++i) {
+              const int t = nprobe > 1 ? (int)((long long)i * (ntris - 1) / (nprobe - 1)) : 0;
+              vertex_fragments(shape, t, T, Rn, sd, fr.data() + 3 * i);
+            }
+            const bool v = ntris > 0
+              && (material_varies(side_mtl[sd], fr.data(), 3 * nprobe,
+                                  out.shader_wl.front(), dev)
+                  || material_varies(side_mtl[sd], fr.data(), 3 * nprobe,
+                                     out.shader_wl.back(), dev));
+            found = varies.emplace(key, v).first;
           }
           bake_side[sd] = found->second;
         }

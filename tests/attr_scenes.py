@@ -27,10 +27,12 @@ def ramp_mirror(lib, kind):
         refl = lambda wl, f: 0.5 + 0.04 * f.P[0]  # noqa: E731
         shape = W.grid_mesh(s, 10.0, 10.0, 8, 8)
         expected = 0.5
+        exact = expected
     elif kind == "uv":
         refl = lambda wl, f: f.uv[0]  # noqa: E731
         shape = W.grid_mesh(s, 10.0, 10.0, 8, 8)
         expected = 1.0 / 3.0
+        exact = expected
     else:
         refl = lambda wl, f: f.uv[0] * f.uv[0]  # noqa: E731
         n = 8
@@ -51,6 +53,7 @@ def ramp_mirror(lib, kind):
         # the exact mean over the square is 1/3, the piecewise-linear one
         # 1/3 + (1/8)^2 / 6 per the trapezoid rule in u
         expected = 1.0 / 3.0 + (1.0 / 8) ** 2 / 6
+        exact = 1.0 / 3.0
     m = s.mirror(refl, 0.0)
     mirror = s.instance(s.object([(shape, m, m)]))
     v = s.virtual()
@@ -58,7 +61,8 @@ def ramp_mirror(lib, kind):
                      P.transform_from(P.rotation_pitch_pi(), (0, 0, 5)),
                      receiver=P.SSOL_FRONT, sample=0)
     s.set_sun("directional", (0, 0, -1), DNI)
-    return s, {"mirror": mirror, "receiver": rcv, "expected": DNI * 100 * expected}
+    return s, {"mirror": mirror, "receiver": rcv, "expected": DNI * 100 * expected,
+               "exact": DNI * 100 * exact}
 
 
 def tilted_normals(lib, alpha=0.1, dist=20.0):

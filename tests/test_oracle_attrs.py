@@ -16,6 +16,16 @@ def test_oracle_varying_reflectivity(oracle, kind):
     assert r[2] > 0  # the weight varies from path to path
 
 
+def test_oracle_texcoord_shader_exact(oracle):
+    """The oracle calls u^2 at each hit's texcoords: the exact mean 1/3, not
+    the piecewise-linear mean the device's per-vertex baking gives."""
+    s, h = A.ramp_mirror(oracle, "tex")
+    e = s.solve(500000, seed=4)
+    r = e.receiver(h["receiver"])["incoming_flux"]
+    assert abs(r[0] - h["exact"]) <= 3 * r[2]
+    assert abs(h["expected"] - h["exact"]) > 5 * r[2]  # the two are told apart
+
+
 def test_oracle_vertex_normals(oracle):
     s, h = A.tilted_normals(oracle)
     e = s.solve(20000, seed=3)
