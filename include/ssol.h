@@ -15,8 +15,11 @@
  *  - Shader callbacks are evaluated on the host when `ssol_solve` snapshots
  *    the scene (per material and per sun-spectrum wavelength node); they may
  *    depend on the wavelength but not on the surface position.
- *  - Camera/image/draw (src/ssol.h:546-632, 1225-1244) are not part of this
- *    library: they are CPU preview renderers outside the solve path.
+ *  - `ssol_draw_draft` / `ssol_draw_pt` (src/ssol.h:1225-1244) render the
+ *    whole image on the GPU into a device buffer, copy it back once and then
+ *    hand it to the writer tile by tile (32 x 32, Morton order of tiles, one
+ *    thread), as the reference's draw loop does; include/ssol_b200.h adds
+ *    entry points that leave the image in device memory.
  */
 #ifndef SSOL_H
 #define SSOL_H
@@ -56,7 +59,9 @@ struct mem_allocator;
 struct ssp_rng;
 
 struct ssol_atmosphere;
+struct ssol_camera;
 struct ssol_device;
+struct ssol_image;
 struct ssol_material;
 struct ssol_object;
 struct ssol_instance;
@@ -106,6 +111,22 @@ enum ssol_clipping_op {
   SSOL_CLIPPING_OPS_COUNT__
 };
 
+/* src/ssol.h:98-111 */
+enum ssol_pixel_format {
+  SSOL_PIXEL_DOUBLE3,
+  SSOL_PIXEL_FORMATS_COUNT__
+};
+
+enum ssol_filter_mode {
+  SSOL_FILTER_LINEAR,
+  SSOL_FILTER_NEAREST
+};
+
+enum ssol_address_mode {
+  SSOL_ADDRESS_CLAMP,
+  SSOL_ADDRESS_REPEAT
+};
+
 /* src/ssol.h:113-121 */
 enum ssol_quadric_type {
   SSOL_QUADRIC_PLANE,
@@ -139,6 +160,18 @@ struct ssol_vertex_data {
 #define SSOL_VERTEX_DATA_NULL__ { SSOL_ATTRIBS_COUNT__, NULL }
 static const struct ssol_vertex_data SSOL_VERTEX_DATA_NULL =
   SSOL_VERTEX_DATA_NULL__;
+
+/* Layout of an image's pixels (src/ssol.h:160-171) */
+struct ssol_image_layout {
+  size_t row_pitch; /* bytes between two consecutive rows */
+  size_t offset; /* byte offset of the first pixel */
+  size_t size; /* overall size of the image buffer */
+  size_t width, height; /* pixels in X and Y */
+  enum ssol_pixel_format pixel_format;
+};
+#define SSOL_IMAGE_LAYOUT_NULL__ { 0, 0, 0, 0, 0, SSOL_PIXEL_FORMATS_COUNT__ }
+static const struct ssol_image_layout SSOL_IMAGE_LAYOUT_NULL =
+  SSOL_IMAGE_LAYOUT_NULL__;
 
 /* Quadrics, all in their local frame (src/ssol.h:172-246). */
 struct ssol_quadric_plane { char dummy; }; /* z = 0 */
@@ -403,6 +436,25 @@ struct ssol_mc_primitive {
 static const struct ssol_mc_primitive SSOL_MC_PRIMITIVE_NULL =
   SSOL_MC_PRIMITIVE_NULL__;
 
+/* Pixel sink of the draw functions (src/ssol.h:495-501): `pixels` holds
+ * size[0] x size[1] pixels of format `fmt`, row after row, for the tile whose
+ * first pixel is `origin` */
+typedef res_T
+(*ssol_write_pixels_T)
+  (void* context,
+   const size_t origin[2],
+   const size_t size[2],
+   const enum ssol_pixel_format fmt,
+   const void* pixels);
+
+/* src/ssol.h:503-510; 0 for a format that does not exist (the reference
+ * aborts) */
+static inline size_t
+ssol_sizeof_pixel_format(const enum ssol_pixel_format format)
+{
+  return format == SSOL_PIXEL_DOUBLE3 ? sizeof(double[3]) : 0;
+}
+
 /*
  * Every object is reference counted: `*_create` hands the caller one
  * reference; `*_ref_put` releases it and the object is destroyed when the
@@ -657,6 +709,85 @@ SSOL_API res_T ssol_solve
    const size_t max_failed_count,
    const struct ssol_path_tracker* tracker,
    struct ssol_estimator** estimator);
+
+/* Preview renderers: src/ssol.h:1225-1244 (src/ssol_draw.c,
+ * src/ssol_draw_draft.c, src/ssol_draw_pt.c). Both render with the scene's
+ * sun, need its spectrum and DNI (RES_BAD_ARG otherwise) and ignore virtual
+ * materials.
+ *  - ssol_draw_draft: per pixel, the mean over `spp` sub-pixel positions
+ *    (the same `spp` offsets for every pixel) of max(0, cos(N, -dir)) at
+ *    the first surface the camera ray reaches, N its shading normal;
+ *  - ssol_draw_pt: path tracing with the sun as a directional light (shadow
+ *    ray toward -sun direction), a sky of radiance 0.1 above `up`, the
+ *    materials' BSDFs and Russian roulette once the throughput drops below
+ *    0.1. */
+SSOL_API res_T ssol_draw_draft
+  (struct ssol_scene* scn,
+   struct ssol_camera* cam,
+   const size_t width,
+   const size_t height,
+   const size_t spp,
+   ssol_write_pixels_T writer,
+   void* writer_data);
+
+SSOL_API res_T ssol_draw_pt
+  (struct ssol_scene* scn,
+   struct ssol_camera* cam,
+   const size_t width,
+   const size_t height,
+   const size_t spp,
+   const double up[3],
+   ssol_write_pixels_T writer,
+   void* writer_data);
+
+/* Camera: src/ssol.h:543-575 (src/ssol_camera.c). A pinhole camera; its
+ * basis is kept in single precision as in the reference. Defaults: at the
+ * origin looking toward -z with +y up, horizontal field of view pi/2,
+ * width/height ratio 1. */
+SSOL_API res_T ssol_camera_create
+  (struct ssol_device* dev, struct ssol_camera** cam);
+SSOL_API res_T ssol_camera_ref_get(struct ssol_camera* cam);
+SSOL_API res_T ssol_camera_ref_put(struct ssol_camera* cam);
+SSOL_API res_T ssol_camera_set_proj_ratio
+  (struct ssol_camera* cam, const double proj_ratio); /* width / height */
+SSOL_API res_T ssol_camera_set_fov /* horizontal field of view, radians */
+  (struct ssol_camera* cam, const double fov);
+SSOL_API res_T ssol_camera_look_at
+  (struct ssol_camera* cam,
+   const double position[3],
+   const double target[3],
+   const double up[3]);
+
+/* Image: src/ssol.h:577-632 (src/ssol_image.c). Host memory, rows of
+ * width x pixel size bytes. */
+SSOL_API res_T ssol_image_create
+  (struct ssol_device* dev, struct ssol_image** image);
+SSOL_API res_T ssol_image_ref_get(struct ssol_image* image);
+SSOL_API res_T ssol_image_ref_put(struct ssol_image* image);
+SSOL_API res_T ssol_image_setup
+  (struct ssol_image* image,
+   const size_t width,
+   const size_t height,
+   const enum ssol_pixel_format format);
+SSOL_API res_T ssol_image_get_layout
+  (const struct ssol_image* image, struct ssol_image_layout* layout);
+SSOL_API res_T ssol_image_map
+  (const struct ssol_image* image, char** memory);
+SSOL_API res_T ssol_image_unmap(const struct ssol_image* image);
+SSOL_API res_T ssol_image_sample
+  (const struct ssol_image* image,
+   const enum ssol_filter_mode filter,
+   const enum ssol_address_mode address_u,
+   const enum ssol_address_mode address_v,
+   const double uv[2],
+   void* val);
+/* Writer that copies the tile into an ssol_image (`image`) */
+SSOL_API res_T ssol_image_write
+  (void* image,
+   const size_t origin[2],
+   const size_t size[2],
+   const enum ssol_pixel_format fmt,
+   const void* pixels);
 
 /* Data helpers: src/ssol.h:1249-1273 (src/ssol_data.c). */
 SSOL_API struct ssol_data* ssol_data_set_real

@@ -190,6 +190,27 @@ SSOL_API res_T ssol_b200_batch_finish
    const size_t max_failed_count, void* stream,
    struct ssol_estimator** estimators);
 
+/* Renderers into device memory. No counterpart in the reference: its
+ * ssol_draw_draft / ssol_draw_pt (src/ssol.h:1225-1244) hand tiles to a host
+ * writer, which the ssol.h versions here still do. These leave the image in
+ * a caller's device buffer (a headless device image), width x height
+ * pixels of 3 doubles, row after row (row pitch width x 24 bytes), and
+ * return when it is written. `options` (NULL => defaults) selects the
+ * arithmetic precision and the BVH leaf size; `stats` (may be NULL)
+ * receives the kernel time and work counters (bounces = shaded surface
+ * interactions, paths = camera samples). ssol_b200_draw_pt_device keys its
+ * random streams by `seed`; ssol_draw_pt uses seed 0. */
+SSOL_API res_T ssol_b200_draw_draft_device
+  (struct ssol_scene* scn, struct ssol_camera* cam, const size_t width,
+   const size_t height, const size_t spp,
+   const struct ssol_b200_options* options, double* device_pixels,
+   struct ssol_b200_stats* stats);
+SSOL_API res_T ssol_b200_draw_pt_device
+  (struct ssol_scene* scn, struct ssol_camera* cam, const size_t width,
+   const size_t height, const size_t spp, const double up[3],
+   const uint64_t seed, const struct ssol_b200_options* options,
+   double* device_pixels, struct ssol_b200_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

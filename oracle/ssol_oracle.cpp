@@ -1457,10 +1457,20 @@ OTriAttr tri_attr(const ssol_shape* s, unsigned t, const Affine& xf)
   Affine inv;
   if(!s->nrm.empty() && inverse(xf, inv)) {
     a.has_n = true;
+    /* src/ssol_material.c:632-646 turns the normal by the inverse transpose
+     * only when none of the three linear columns, in FP32, equals the
+     * identity's */
+    bool any_id = false;
+    for(int c = 0; c < 3; ++c) {
+      bool eq = true;
+      for(int r = 0; r < 3; ++r)
+        eq = eq && (float)xf.m[3 * c + r] == (r == c ? 1.f : 0.f);
+      any_id = any_id || eq;
+    }
     for(int k = 0; k < 3; ++k) {
       const unsigned id = s->ids[t * 3 + k];
-      /* inverse transpose of the instance's linear part */
-      a.n[k] = xvec_t(inv, v3(s->nrm[id * 3], s->nrm[id * 3 + 1], s->nrm[id * 3 + 2]));
+      const V n = v3(s->nrm[id * 3], s->nrm[id * 3 + 1], s->nrm[id * 3 + 2]);
+      a.n[k] = any_id ? n : xvec_t(inv, n);
     }
   }
   const V e1 = p[1] - p[0], e2 = p[2] - p[0];
@@ -1493,7 +1503,11 @@ bool varies_over(const ssol_material* m, const ssol_shape* s, const Affine& xf,
   if(m->refl) m->refl(m->dev, m->buf, wl, &ref, &r0);
   if(m->rough) m->rough(m->dev, m->buf, wl, &ref, &g0);
   const unsigned nt = (unsigned)(s->ids.size() / 3);
-  const unsigned probe[2] = {0, nt - 1};
+  /* the vertices of up to 8 triangles spread over the mesh */
+  const unsigned np = std::min(nt, 8u);
+  std::vector<unsigned> probe;
+  for(unsigned i = 0; i < np; ++i)
+    probe.push_back(np > 1 ? (unsigned)((unsigned long long)i * (nt - 1) / (np - 1)) : 0);
   for(unsigned t : probe) {
     const OTriAttr a = tri_attr(s, t, xf);
     V p[3];
@@ -1516,7 +1530,7 @@ bool varies_over(const ssol_material* m, const ssol_shape* s, const Affine& xf,
   return false;
 }
 
-res_T make_scene(ssol_scene* scn, Scene& S)
+res_T make_scene(ssol_scene* scn, Scene& S, bool need_sampled = true)
 {
   if(!scn->sun || !scn->sun->spec || scn->sun->spec->wl.empty() || scn->sun->dni <= 0)
     return RES_BAD_ARG;
@@ -1597,7 +1611,8 @@ res_T make_scene(ssol_scene* scn, Scene& S)
             const auto key = std::make_pair(m, (const ssol_shape*)s);
             auto f = varies.find(key);
             if(f == varies.end())
-              f = varies.emplace(key, varies_over(m, s, inst->xf, sd, S.wl[0])).first;
+              f = varies.emplace(key, varies_over(m, s, inst->xf, sd, S.wl.front())
+                                      || varies_over(m, s, inst->xf, sd, S.wl.back())).first;
             if(f->second) vary[sd] = m;
           }
           if(!s->nrm.empty() || vary[0] || vary[1]) {
@@ -1649,7 +1664,7 @@ res_T make_scene(ssol_scene* scn, Scene& S)
       S.sinst.push_back(o);
     }
   }
-  if(!sampled || S.samp.empty()) return RES_BAD_ARG;
+  if(need_sampled && (!sampled || S.samp.empty())) return RES_BAD_ARG;
   alias_table(area, S.aprob, S.aidx);
   std::vector<int> refs;
   std::vector<std::array<double,6>> boxes;
@@ -2575,4 +2590,491 @@ API res_T ssol_mc_shape_get_mc_primitive(ssol_mc_shape* sh, const unsigned i,
     r[q].E /= area; r[q].V /= area * area; r[q].SE /= area;
   }
   return RES_OK;
+}
+
+/*******************************************************************************
+ * Camera, image and the preview renderers (src/ssol_camera.c,
+ * src/ssol_image.c, src/ssol_draw.c, src/ssol_draw_draft.c,
+ * src/ssol_draw_pt.c), with the same random streams as the B200 library:
+ * draft sub-pixel offsets from Philox (i, 0, 0, 4) with key 0; path tracer
+ * streams keyed by the seed with id = pixel x spp + sample (domains 5:
+ * sub-pixel position, 6: wavelength of an attempt, 7: BSDF sample and 8:
+ * roulette at event (attempt << 20) | bounce). Star-SF's rendering BSDFs
+ * are restated as in the library (Lambertian, specular, dielectric and
+ * thin-slab samplers, Cook-Torrance microfacet with V-cavity G and the
+ * Walter et al. 2007 estimator weight).
+ ******************************************************************************/
+struct ssol_camera {
+  Ref ref; ssol_device* dev;
+  float x[3] = {0, 0, 0}, y[3] = {0, 0, 0}, z[3] = {0, 0, 0}, pos[3] = {0, 0, 0};
+  float fov = 0, rcp_ratio = 1;
+};
+struct ssol_image {
+  Ref ref; ssol_device* dev;
+  std::vector<double> mem; size_t w = 0, h = 0;
+  ssol_pixel_format fmt = SSOL_PIXEL_FORMATS_COUNT__;
+};
+
+namespace {
+
+float f3norm(float o[3], const float v[3])
+{
+  const float l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  if(l == 0.f) return l;
+  for(int c = 0; c < 3; ++c) o[c] = v[c] / l;
+  return l;
+}
+
+void f3cross(float o[3], const float a[3], const float b[3])
+{
+  const float r[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2],
+                      a[0] * b[1] - a[1] * b[0]};
+  std::memcpy(o, r, sizeof(r));
+}
+
+/* camera_ray (src/ssol_camera.h:41-62), FP32 without contraction */
+void cam_ray(const ssol_camera* c, float sx, float sy, float d[3])
+{
+  const float fx = sx * 2.f - 1.f, fy = sy * 2.f - 1.f;
+  for(int k = 0; k < 3; ++k) d[k] = (c->x[k] * fx + c->y[k] * fy) + c->z[k];
+  const float l = std::sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]);
+  for(int k = 0; k < 3; ++k) d[k] = d[k] / l;
+}
+
+enum { DOM_DRAW_OFFSET = 4, DOM_DRAW_PIXEL = 5, DOM_DRAW_WL = 6, DOM_DRAW_BSDF = 7,
+       DOM_DRAW_RR = 8 };
+const int DRAW_MAX_BOUNCES = 1000, DRAW_MAX_FAILURES = 100;
+
+/* Shading normal and fragment of a hit (src/ssol_material.c:551-655 with P
+ * the hit point) */
+V draw_normal(const Scene& S, const OHit& h, int side, V pos, V dir, V Ng,
+              ssol_surface_fragment& frag, bool& use_frag)
+{
+  return shading_inputs(S, h.gid, side, pos, dir, Ng, h.b1, h.b2, frag, use_frag);
+}
+
+struct DBsdf { const ssol_material* m; double refl, rough; };
+
+DBsdf draw_bsdf(const Scene& S, const ssol_material* m, double wl,
+                const ssol_surface_fragment* frag)
+{
+  DBsdf f = {m, 0, 0};
+  if(m->type != SSOL_MATERIAL_MIRROR && m->type != SSOL_MATERIAL_MATTE) return f;
+  if(frag) {
+    if(m->refl) m->refl(m->dev, m->buf, wl, frag, &f.refl);
+    if(m->type == SSOL_MATERIAL_MIRROR && m->rough) m->rough(m->dev, m->buf, wl, frag, &f.rough);
+  } else {
+    f.refl = shader(S, m, 0, wl);
+    if(m->type == SSOL_MATERIAL_MIRROR) f.rough = shader(S, m, 1, wl);
+  }
+  return f;
+}
+
+double mf_d(int distrib, double a, double nh)
+{
+  if(!(nh > 0)) return 0;
+  const double c2 = nh * nh, t2 = (1 - c2) / c2, a2 = a * a;
+  const double inv = 1 / (M_PI * a2 * c2 * c2);
+  if(distrib == SSOL_MICROFACET_BECKMANN) return std::exp(-t2 / a2) * inv;
+  return t2 <= a2 ? inv : 0;
+}
+
+double mf_g(double nh, double no, double ni, double oh)
+{
+  if(!(oh > 0)) return 0;
+  return std::min(1.0, std::min(2 * nh * no / oh, 2 * nh * ni / oh));
+}
+
+double draw_eval(const DBsdf& f, V wo, V N, V wi)
+{
+  const double no = dot(wo, N), ni = dot(wi, N);
+  if(!(no > 0) || !(ni > 0)) return 0;
+  if(f.m->type == SSOL_MATERIAL_MATTE) return f.refl / M_PI;
+  if(f.m->type == SSOL_MATERIAL_MIRROR && f.rough > 0) {
+    const V h = unit(wo + wi);
+    const double nh = dot(N, h), oh = dot(wo, h);
+    return f.refl * mf_d(f.m->distrib, f.rough, nh) * mf_g(nh, no, ni, oh) / (4 * no * ni);
+  }
+  return 0;
+}
+
+/* Returns the weight; type 1 reflection, 2 transmission */
+double draw_sample(const DBsdf& f, const Block& r, double wl, V wo, V N, V& wi, int& type,
+                   bool& to_inside)
+{
+  const ssol_material* m = f.m;
+  type = 0; to_inside = false; wi = N;
+  const double ci = dot(wo, N);
+  if(!(ci > 0)) return 0;
+  V b1, b2;
+  switch(m->type) {
+    case SSOL_MATERIAL_MIRROR: {
+      type = 1;
+      if(f.rough == 0) { wi = N * (2 * ci) - wo; return f.refl; }
+      const double a = f.rough, u0 = unif(r.x[0]);
+      const double t2 = m->distrib == SSOL_MICROFACET_BECKMANN ? -a * a * std::log(1 - u0)
+                                                               : a * a * u0;
+      const double ct = 1 / std::sqrt(1 + t2), st = std::sqrt(t2) * ct;
+      const double ph = 2 * M_PI * unif(r.x[1]);
+      onb(N, b1, b2);
+      const V h = b1 * (std::cos(ph) * st) + b2 * (std::sin(ph) * st) + N * ct;
+      const double oh = dot(wo, h);
+      wi = h * (2 * oh) - wo;
+      const double ni = dot(wi, N);
+      if(!(oh > 0) || !(ni > 0)) return 0;
+      return f.refl * mf_g(ct, ci, ni, oh) * oh / (ci * ct);
+    }
+    case SSOL_MATERIAL_MATTE: {
+      const double u0 = unif(r.x[0]), rad = std::sqrt(u0);
+      const double ph = 2 * M_PI * unif(r.x[1]);
+      onb(N, b1, b2);
+      wi = b1 * (rad * std::cos(ph)) + b2 * (rad * std::sin(ph)) + N * std::sqrt(1 - u0);
+      type = 1;
+      return f.refl;
+    }
+    case SSOL_MATERIAL_DIELECTRIC: {
+      const double ei = data_value(m->out.refractive_index, wl);
+      const double et = data_value(m->in.refractive_index, wl);
+      const double eta = ei / et, s2 = eta * eta * (1 - ci * ci);
+      double F = 1, ct = 0;
+      if(s2 < 1) { ct = std::sqrt(1 - s2); F = fresnel(ci, ct, ei, et); }
+      if(unif(r.x[0]) < F) { wi = N * (2 * ci) - wo; type = 1; }
+      else { wi = unit(N * (eta * ci - ct) - wo * eta); type = 2; to_inside = true; }
+      return 1;
+    }
+    case SSOL_MATERIAL_THIN_DIELECTRIC: {
+      const double ei = data_value(m->out.refractive_index, wl);
+      const double et = data_value(m->slab.refractive_index, wl);
+      const double al = data_value(m->slab.extinction, wl);
+      const double eta = ei / et, s2 = eta * eta * (1 - ci * ci);
+      double Rt = 1, Tt = 0;
+      if(s2 < 1) {
+        const double ct = std::sqrt(1 - s2), F = fresnel(ci, ct, ei, et);
+        const double tau = std::exp(-al * m->thickness / ct);
+        const double den = 1 - F * F * tau * tau;
+        Rt = F + (1 - F) * (1 - F) * F * tau * tau / den;
+        Tt = (1 - F) * (1 - F) * tau / den;
+      }
+      const double p = Rt + Tt;
+      if(p > 0 && unif(r.x[0]) * p < Rt) { wi = N * (2 * ci) - wo; type = 1; }
+      else { wi = -wo; type = 2; }
+      return p;
+    }
+    default: return 0;
+  }
+}
+
+/* Li of src/ssol_draw_pt.c:124-290; false on an inconsistent medium */
+bool draw_li(const Scene& S, const PathRng& rng, uint32_t attempt, V org, V dir,
+             V up, double& L)
+{
+  L = 0;
+  double thr = 1;
+  bool roulette = false;
+  const double wl = wl_sample(S, unif(rng.get(attempt, DOM_DRAW_WL).x[0]));
+  ssol_medium medium = S.air;
+  Self self = {-1, -1, 0, true, false};
+  const V to_sun = -S.sun_dir;
+  for(int b = 0; b < DRAW_MAX_BOUNCES; ++b) {
+    const OHit h = trace(S, org, dir, 0, self, false);
+    if(!h.found) {
+      if(dot(dir, up) > 0) L += thr * 1e-1;
+      break;
+    }
+    const double kext = data_value(medium.extinction, wl);
+    if(kext > 0) {
+      thr *= std::exp(-kext * h.t);
+      if(thr <= 0) break;
+    }
+    const V wo_in = unit(dir);
+    V Ng = unit(h.n);
+    int side = 1;
+    if(!(dot(Ng, wo_in) < 0)) { side = 2; Ng = -Ng; }
+    const V pos = org + dir * h.t;
+    ssol_surface_fragment frag;
+    bool use_frag = false;
+    const V N = draw_normal(S, h, side, pos, wo_in, Ng, frag, use_frag);
+    if(dot(N, wo_in) > 0) break;
+    const ssol_material* m = S.sinst[h.sinst].mtl[side - 1];
+    const DBsdf f = draw_bsdf(S, m, wl, use_frag ? &frag : nullptr);
+    if(m->type == SSOL_MATERIAL_DIELECTRIC && !media_ceq(medium, m->out)) return false;
+    self.gid = h.gid; self.sinst = h.sinst; self.side = side;
+    org = pos;
+    const V wo = -wo_in;
+    const double c = dot(to_sun, N);
+    if(c >= 0 && !(std::fabs(c) <= 1e-6)) {
+      const double fv = draw_eval(f, wo, N, to_sun);
+      if(fv > 0 && !trace(S, org, to_sun, 0, self, true).found) L += thr * fv * c;
+    }
+    const uint32_t ev = (attempt << 20) | (uint32_t)b;
+    V wi;
+    int type;
+    bool inside;
+    double w = draw_sample(f, rng.get(ev, DOM_DRAW_BSDF), wl, wo, N, wi, type, inside);
+    const double cg = dot(Ng, wi);
+    if((cg > 0 && type == 2) || (cg < 0 && type == 1)) w = 0;
+    dir = wi;
+    if(inside) ssol_medium_copy(&medium, &m->in);
+    const double cn = std::fabs(dot(wi, N));
+    if(!roulette) thr *= cn * w;
+    else {
+      if(unif(rng.get(ev, DOM_DRAW_RR).x[0]) >= w) break;
+      thr *= cn;
+    }
+    if(thr <= 0) break;
+    if(!roulette) roulette = thr < 0.1;
+  }
+  return true;
+}
+
+size_t pow2_up(size_t v) { size_t p = 1; while(p < v) p <<= 1; return p; }
+
+uint32_t morton_even(uint32_t code)
+{
+  uint32_t x = code & 0x55555555u;
+  x = (x | (x >> 1)) & 0x33333333u;
+  x = (x | (x >> 2)) & 0x0F0F0F0Fu;
+  x = (x | (x >> 4)) & 0x00FF00FFu;
+  x = (x | (x >> 8)) & 0x0000FFFFu;
+  return x;
+}
+
+/* Whole image, then the writer per 32 x 32 tile in Morton order */
+res_T draw_image(ssol_scene* scn, ssol_camera* cam, size_t W, size_t H, size_t spp,
+                 bool pt, const double* up, ssol_write_pixels_T writer, void* data)
+{
+  Scene S;
+  const res_T r = make_scene(scn, S, false);
+  if(r != RES_OK) return r;
+  std::vector<double> img(W * H * 3);
+  std::vector<float> off(spp * 2);
+  for(size_t i = 0; i < spp; ++i) {
+    const Block b = philox((uint32_t)i, (uint32_t)(i >> 32), 0, DOM_DRAW_OFFSET, 0, 0);
+    off[2 * i] = (float)(b.x[0] >> 8) * (1.0f / 16777216.0f);
+    off[2 * i + 1] = (float)(b.x[1] >> 8) * (1.0f / 16777216.0f);
+  }
+  const float pw = 1.f / (float)W, ph = 1.f / (float)H;
+  const V cpos = v3(cam->pos[0], cam->pos[1], cam->pos[2]);
+  const V vup = up ? v3((float)up[0], (float)up[1], (float)up[2]) : v3(0, 0, 0);
+  #pragma omp parallel for schedule(dynamic, 64)
+  for(long long p = 0; p < (long long)(W * H); ++p) {
+    const size_t px = (size_t)p % W, py = (size_t)p / W;
+    double sum = 0;
+    bool failed = false;
+    for(size_t s = 0; s < spp && !failed; ++s) {
+      float sx, sy;
+      PathRng rng = {(uint64_t)p * spp + s, 0};
+      if(pt) {
+        const Block j = rng.get(0, DOM_DRAW_PIXEL);
+        sx = ((float)px + (float)(j.x[0] >> 8) * (1.0f / 16777216.0f)) * pw;
+        sy = ((float)py + (float)(j.x[1] >> 8) * (1.0f / 16777216.0f)) * ph;
+      } else {
+        sx = ((float)px + off[2 * s]) * pw;
+        sy = ((float)py + off[2 * s + 1]) * ph;
+      }
+      float df[3];
+      cam_ray(cam, sx, sy, df);
+      const V d = v3(df[0], df[1], df[2]);
+      if(pt) {
+        double L = 0;
+        bool ok = false;
+        for(uint32_t a = 0; a < (uint32_t)DRAW_MAX_FAILURES && !ok; ++a)
+          ok = draw_li(S, rng, a, cpos, d, vup, L);
+        if(!ok) failed = true;
+        else sum += L;
+      } else {
+        const Self self = {-1, -1, 0, true, false};
+        const OHit h = trace(S, cpos, d, 0, self, false);
+        if(!h.found) continue;
+        const V wi = unit(d);
+        V N = unit(h.n);
+        int side = 1;
+        if(!(dot(N, wi) < 0)) { N = -N; side = 2; }
+        ssol_surface_fragment frag;
+        bool use_frag;
+        N = draw_normal(S, h, side, cpos + d * h.t, wi, N, frag, use_frag);
+        sum += std::max(dot(N, -wi), 0.0);
+      }
+    }
+    double* o = &img[(size_t)p * 3];
+    if(failed) { o[0] = 1; o[1] = 1; o[2] = 0; }
+    else { const double v = sum / (double)spp; o[0] = v; o[1] = v; o[2] = v; }
+  }
+  const size_t T = 32, ntx = (W + T - 1) / T, nty = (H + T - 1) / T;
+  size_t nt = pow2_up(std::max(ntx, nty));
+  nt *= nt;
+  std::vector<double> tile(T * T * 3);
+  for(size_t code = 0; code < nt; ++code) {
+    size_t org[2] = {morton_even((uint32_t)code), morton_even((uint32_t)(code >> 1))};
+    if(org[0] >= ntx || org[1] >= nty) continue;
+    org[0] *= T; org[1] *= T;
+    const size_t sz[2] = {std::min(T, W - org[0]), std::min(T, H - org[1])};
+    for(size_t y = 0; y < sz[1]; ++y)
+      std::memcpy(&tile[y * sz[0] * 3], &img[((org[1] + y) * W + org[0]) * 3],
+                  sz[0] * 3 * sizeof(double));
+    const res_T wr = writer(data, org, sz, SSOL_PIXEL_DOUBLE3, tile.data());
+    if(wr != RES_OK) return wr;
+  }
+  return RES_OK;
+}
+
+bool scene_ok(const ssol_scene* s)
+{
+  return s->sun && s->sun->spec && s->sun->dni > 0;
+}
+
+double map_addr(double a, ssol_address_mode mode)
+{
+  if(mode == SSOL_ADDRESS_CLAMP) return std::min(std::max(a, 0.0), std::nextafter(1.0, 0.0));
+  double i, f = std::modf(a, &i);
+  if(f < 0) f = 1.0 + f;
+  return f < 1.0 ? f : std::nextafter(1.0, 0.0);
+}
+
+} /* namespace */
+
+API res_T ssol_camera_create(ssol_device* d, ssol_camera** out)
+{
+  if(!d || !out) return RES_BAD_ARG;
+  ssol_camera* c = new ssol_camera();
+  c->dev = d; d->ref.get();
+  c->rcp_ratio = 1.f; c->fov = (float)(M_PI / 2.0);
+  const double p[3] = {0, 0, 0}, t[3] = {0, 0, -1}, u[3] = {0, 1, 0};
+  ssol_camera_look_at(c, p, t, u);
+  *out = c;
+  return RES_OK;
+}
+API res_T ssol_camera_ref_get(ssol_camera* c) { if(!c) return RES_BAD_ARG; c->ref.get(); return RES_OK; }
+API res_T ssol_camera_ref_put(ssol_camera* c)
+{
+  if(!c) return RES_BAD_ARG;
+  if(c->ref.put()) { ssol_device* d = c->dev; delete c; ssol_device_ref_put(d); }
+  return RES_OK;
+}
+API res_T ssol_camera_set_proj_ratio(ssol_camera* c, const double r)
+{
+  float y[3];
+  if(!c || r <= 0 || f3norm(y, c->y) <= 0) return RES_BAD_ARG;
+  c->rcp_ratio = (float)(1.0 / r);
+  for(int k = 0; k < 3; ++k) c->y[k] = y[k] * c->rcp_ratio;
+  return RES_OK;
+}
+API res_T ssol_camera_set_fov(ssol_camera* c, const double fov)
+{
+  float z[3];
+  if(!c || (float)fov <= 0 || f3norm(z, c->z) <= 0) return RES_BAD_ARG;
+  const float depth = (float)(1.0 / std::tan(fov * 0.5));
+  for(int k = 0; k < 3; ++k) c->z[k] = z[k] * depth;
+  c->fov = (float)fov;
+  return RES_OK;
+}
+API res_T ssol_camera_look_at(ssol_camera* c, const double pos[3], const double tgt[3],
+                              const double up[3])
+{
+  if(!c || !pos || !tgt || !up) return RES_BAD_ARG;
+  float p[3], u[3], x[3], y[3], z[3], d[3];
+  for(int k = 0; k < 3; ++k) {
+    p[k] = (float)pos[k]; u[k] = (float)up[k];
+    d[k] = (float)tgt[k] - p[k];
+  }
+  if(f3norm(z, d) <= 0) return RES_BAD_ARG;
+  f3cross(d, z, u);
+  if(f3norm(x, d) <= 0) return RES_BAD_ARG;
+  f3cross(d, z, x);
+  if(f3norm(y, d) <= 0) return RES_BAD_ARG;
+  const float depth = (float)(1.0 / std::tan(c->fov * 0.5));
+  for(int k = 0; k < 3; ++k) {
+    c->x[k] = x[k]; c->y[k] = y[k] * c->rcp_ratio; c->z[k] = z[k] * depth; c->pos[k] = p[k];
+  }
+  return RES_OK;
+}
+
+API res_T ssol_image_create(ssol_device* d, ssol_image** out)
+{
+  if(!d || !out) return RES_BAD_ARG;
+  ssol_image* i = new ssol_image();
+  i->dev = d; d->ref.get();
+  *out = i;
+  return RES_OK;
+}
+API res_T ssol_image_ref_get(ssol_image* i) { if(!i) return RES_BAD_ARG; i->ref.get(); return RES_OK; }
+API res_T ssol_image_ref_put(ssol_image* i)
+{
+  if(!i) return RES_BAD_ARG;
+  if(i->ref.put()) { ssol_device* d = i->dev; delete i; ssol_device_ref_put(d); }
+  return RES_OK;
+}
+API res_T ssol_image_setup(ssol_image* i, const size_t w, const size_t h,
+                           const ssol_pixel_format f)
+{
+  if(!i || !w || !h || (unsigned)f >= SSOL_PIXEL_FORMATS_COUNT__) return RES_BAD_ARG;
+  i->mem.assign(w * h * 3, 0.0);
+  i->w = w; i->h = h; i->fmt = f;
+  return RES_OK;
+}
+API res_T ssol_image_get_layout(const ssol_image* i, ssol_image_layout* l)
+{
+  if(!i || !l) return RES_BAD_ARG;
+  l->row_pitch = i->w * sizeof(double[3]); l->offset = 0; l->size = i->w * i->h;
+  l->width = i->w; l->height = i->h; l->pixel_format = i->fmt;
+  return RES_OK;
+}
+API res_T ssol_image_map(const ssol_image* i, char** m)
+{
+  if(!i || !m) return RES_BAD_ARG;
+  *m = (char*)i->mem.data();
+  return RES_OK;
+}
+API res_T ssol_image_unmap(const ssol_image* i) { return i ? RES_OK : RES_BAD_ARG; }
+API res_T ssol_image_sample(const ssol_image* i, const ssol_filter_mode filter,
+                            const ssol_address_mode au, const ssol_address_mode av,
+                            const double uv[2], void* val)
+{
+  if(!i || !uv || !val || i->fmt != SSOL_PIXEL_DOUBLE3 || i->mem.empty()) return RES_BAD_ARG;
+  double* o = (double*)val;
+  auto px = [&](size_t x, size_t y) { return &i->mem[(y * i->w + x) * 3]; };
+  const double x0 = map_addr(uv[0], au) * (double)i->w, y0 = map_addr(uv[1], av) * (double)i->h;
+  if(filter == SSOL_FILTER_NEAREST) {
+    const double* z = px((size_t)x0, (size_t)y0);
+    for(int k = 0; k < 3; ++k) o[k] = z[k];
+    return RES_OK;
+  }
+  const double x1 = map_addr(uv[0] + 1.0 / (double)i->w, au) * (double)i->w;
+  const double y1 = map_addr(uv[1] + 1.0 / (double)i->h, av) * (double)i->h;
+  const double *a = px((size_t)x0, (size_t)y0), *b = px((size_t)x0, (size_t)y1);
+  const double *c = px((size_t)x1, (size_t)y0), *e = px((size_t)x1, (size_t)y1);
+  double ip;
+  const double s = std::modf(x0, &ip), t = std::modf(y0, &ip);
+  for(int k = 0; k < 3; ++k)
+    o[k] = (1 - s) * ((1 - t) * a[k] + t * b[k]) + s * ((1 - t) * c[k] + t * e[k]);
+  return RES_OK;
+}
+API res_T ssol_image_write(void* image, const size_t org[2], const size_t sz[2],
+                           const ssol_pixel_format fmt, const void* pixels)
+{
+  ssol_image* i = (ssol_image*)image;
+  if(!i || !org || !sz || !pixels || fmt != i->fmt || i->mem.empty()) return RES_BAD_ARG;
+  if(org[0] + sz[0] > i->w || org[1] + sz[1] > i->h) return RES_BAD_ARG;
+  const double* src = (const double*)pixels;
+  for(size_t y = 0; y < sz[1]; ++y)
+    std::memcpy(&i->mem[((org[1] + y) * i->w + org[0]) * 3], src + y * sz[0] * 3,
+                sz[0] * 3 * sizeof(double));
+  return RES_OK;
+}
+
+API res_T ssol_draw_draft(ssol_scene* scn, ssol_camera* cam, const size_t w, const size_t h,
+                          const size_t spp, ssol_write_pixels_T writer, void* data)
+{
+  if(!scn || !spp || !scene_ok(scn)) return RES_BAD_ARG;
+  if(!cam || !w || !h || !writer) return RES_BAD_ARG;
+  return draw_image(scn, cam, w, h, spp, false, nullptr, writer, data);
+}
+
+API res_T ssol_draw_pt(ssol_scene* scn, ssol_camera* cam, const size_t w, const size_t h,
+                       const size_t spp, const double up[3], ssol_write_pixels_T writer,
+                       void* data)
+{
+  if(!scn || !up || !scene_ok(scn)) return RES_BAD_ARG;
+  if(!cam || !w || !h || !spp || !writer) return RES_BAD_ARG;
+  return draw_image(scn, cam, w, h, spp, true, up, writer, data);
 }

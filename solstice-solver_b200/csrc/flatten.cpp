@@ -289,6 +289,26 @@ void vertex_fragments(const ssol_shape* shape, int t, const double T[12],
   }
 }
 
+/* Matrix that takes vertex normals to world space: the inverse transpose of
+ * the instance's linear part, except when one of its three columns, in FP32,
+ * equals the identity's, where src/ssol_material.c:632-646 keeps the normal
+ * as it is */
+void normal_matrix(const double T[12], double Rn[9])
+{
+  bool any_id = false;
+  for(int c = 0; c < 3; ++c) {
+    bool eq = true;
+    for(int r = 0; r < 3; ++r)
+      eq = eq && (float)T[3 * c + r] == (r == c ? 1.f : 0.f);
+    any_id = any_id || eq;
+  }
+  if(any_id) {
+    for(int k = 0; k < 9; ++k) Rn[k] = (k % 4 == 0) ? 1.0 : 0.0;
+  } else {
+    ssolb_d33_invtrans(Rn, T);
+  }
+}
+
 /* Whether a mirror or matte material's shaders give other values at the
  * vertex fragments of a shape than at the reference fragment used for the
  * per-material table (then they are baked per vertex) */
@@ -361,7 +381,8 @@ void build_alias(const std::vector<double>& w, std::vector<float>& prob,
 
 template<class R>
 static res_T flatten_impl
-  (ssol_scene* scn, const BvhBuildParams& bvh_params, FlatScene<R>& out)
+  (ssol_scene* scn, const BvhBuildParams& bvh_params, FlatScene<R>& out,
+   bool for_draw)
 {
   ssol_device* dev = scn->dev;
   out = FlatScene<R>();
@@ -521,7 +542,7 @@ static res_T flatten_impl
          * (src/ssol_material.c:632-646); a side's shaders are baked per vertex
          * when they vary over the shape */
         double Rn[9];
-        ssolb_d33_invtrans(Rn, T);
+        normal_matrix(T, Rn);
         ssol_material* side_mtl[2] = {ss.front, ss.back};
         bool bake_side[2] = {false, false};
         for(int sd = 0; sd < 2; ++sd) {
@@ -760,11 +781,11 @@ static res_T flatten_impl
       out.sinsts.push_back(si);
     }
   }
-  if(!has_sampled || out.samp.empty()) {
+  if(!for_draw && (!has_sampled || out.samp.empty())) {
     dev->log_error("No solstice instance to sample.\n");
     return RES_BAD_ARG;
   }
-  if(!has_receiver) dev->log_warning("No receiver is defined.\n");
+  if(!for_draw && !has_receiver) dev->log_warning("No receiver is defined.\n");
 
   build_alias(samp_area, out.alias_prob, out.alias_idx);
   if(need_tshade) out.tshade = std::move(tsh);
@@ -786,11 +807,13 @@ static res_T flatten_impl
 }
 
 res_T flatten_scene
-  (ssol_scene* scn, const BvhBuildParams& bvh, FlatScene<float>& out)
-{ return flatten_impl<float>(scn, bvh, out); }
+  (ssol_scene* scn, const BvhBuildParams& bvh, FlatScene<float>& out,
+   bool for_draw)
+{ return flatten_impl<float>(scn, bvh, out, for_draw); }
 
 res_T flatten_scene
-  (ssol_scene* scn, const BvhBuildParams& bvh, FlatScene<double>& out)
-{ return flatten_impl<double>(scn, bvh, out); }
+  (ssol_scene* scn, const BvhBuildParams& bvh, FlatScene<double>& out,
+   bool for_draw)
+{ return flatten_impl<double>(scn, bvh, out, for_draw); }
 
 } /* namespace ssolb */

@@ -71,10 +71,14 @@ template<class R> struct FlatScene {
   int32_t air_medium = 0;
 };
 
+/* for_draw: snapshot for the renderers, which sample no instance (no
+ * "nothing to sample" error, no receiver warning) */
 res_T flatten_scene
-  (ssol_scene* scn, const BvhBuildParams& bvh, FlatScene<float>& out);
+  (ssol_scene* scn, const BvhBuildParams& bvh, FlatScene<float>& out,
+   bool for_draw = false);
 res_T flatten_scene
-  (ssol_scene* scn, const BvhBuildParams& bvh, FlatScene<double>& out);
+  (ssol_scene* scn, const BvhBuildParams& bvh, FlatScene<double>& out,
+   bool for_draw = false);
 
 /* Vose's alias method over non-negative weights (deterministic) */
 void build_alias(const std::vector<double>& w, std::vector<float>& prob,

@@ -1926,5 +1926,6 @@ int launch_realisations_f64
 { return launch_impl<double>(S, T, seed, first, count, cfg, stream, track); }
 
 #include "adjoint.cuh"
+#include "draw.cuh"
 
 } /* namespace ssolb */

@@ -100,6 +100,27 @@ int launch_adjoint_f64
   (const DScene<double>& S, const AdjointArgs& A, uint64_t seed, uint64_t first,
    uint64_t count, int pass, void* stream);
 
+/* Arguments of the renderers (draw.cuh). The camera basis is FP32 as in
+ * src/ssol_camera.h; pix_w and pix_h are 1 / width and 1 / height in FP32;
+ * offsets (draft: 2 per sample) and pixels (width x height x 3) are device
+ * arrays; counters (device, 6): rays, BVH nodes, triangle tests, quadric
+ * tests, shaded bounces, camera samples. */
+struct DrawArgs {
+  float cam_x[3], cam_y[3], cam_z[3], cam_pos[3];
+  float pix_w, pix_h;
+  int width, height, spp;
+  const float* offsets;
+  float up[3];
+  uint64_t seed;
+  double* pixels;
+  unsigned long long* counters;
+};
+
+int launch_draft_f32(const DScene<float>& S, const DrawArgs& A, void* stream);
+int launch_draft_f64(const DScene<double>& S, const DrawArgs& A, void* stream);
+int launch_pt_f32(const DScene<float>& S, const DrawArgs& A, void* stream);
+int launch_pt_f64(const DScene<double>& S, const DrawArgs& A, void* stream);
+
 } /* namespace ssolb */
 
 #endif /* SSOL_B200_KERNELS_H */

@@ -66,6 +66,13 @@ enum : uint32_t {
   RNG_SCATTER = 1u, /* event j: j-th BSDF sample of the path */
   RNG_ROULETTE = 2u, /* event r: r-th Russian roulette draw */
   RNG_RETRY = 3u, /* event (j << 6) | k: k-th microfacet re-draw at bounce j */
+  /* Renderers: stream id = pixel x samples per pixel + sample (path
+   * tracer) or sample index (draft sub-pixel offsets, key 0) */
+  RNG_DRAW_OFFSET = 4u, /* event 0: draft sub-pixel offset of sample i */
+  RNG_DRAW_PIXEL = 5u, /* event 0: sub-pixel position of a camera sample */
+  RNG_DRAW_WL = 6u, /* event a: wavelength of attempt a */
+  RNG_DRAW_BSDF = 7u, /* event (a << 20) | b: BSDF sample at bounce b */
+  RNG_DRAW_RR = 8u, /* event (a << 20) | b: roulette draw at bounce b */
   RNG_HOST = 0xffffffffu /* ssp_rng_get on the host */
 };
 

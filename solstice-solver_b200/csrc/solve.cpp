@@ -10,6 +10,7 @@
 #include "flatten.h"
 #include "kernels.h"
 #include "objects.h"
+#include "snapshot.h"
 
 #define SSOL_SHARED_BUILD
 #include "../../include/ssol_b200.h"
@@ -363,7 +364,7 @@ static void bind_scene(DScene<R>& S, const FlatScene<R>& f, const Blob& b,
 
 /* Every index the kernel dereferences, checked on the host before upload */
 template<class R>
-static bool validate(const FlatScene<R>& f)
+static bool validate(const FlatScene<R>& f, bool need_samp = true)
 {
   const int64_t nnodes = (int64_t)f.nodes.size();
   const int64_t nrefs = (int64_t)f.bvh.primrefs.size();
@@ -432,7 +433,7 @@ static bool validate(const FlatScene<R>& f)
   for(const DSpectrum& sp : f.spectra)
     if(sp.count < 1 || (size_t)(sp.first + sp.count) > f.spec_wl.size()) return false;
   const int64_t nsamp = (int64_t)f.samp.size();
-  if(nsamp < 1 || f.alias_prob.size() != f.samp.size()
+  if((need_samp && nsamp < 1) || f.alias_prob.size() != f.samp.size()
   || f.alias_idx.size() != f.samp.size()) return false;
   for(int32_t a : f.alias_idx) if(a < 0 || a >= nsamp) return false;
   for(const DSampTri<R>& t : f.samp) {
@@ -511,6 +512,75 @@ static res_T upload(ssol_b200_plan* p, const FlatScene<R>& f, DScene<R>& S)
   p->scene_bytes = b.host.size();
   bind_scene(S, f, b, (unsigned char*)p->d_scene);
   return RES_OK;
+}
+
+/*******************************************************************************
+ * Device snapshots for the renderers (render.cpp)
+ ******************************************************************************/
+cudaError_t ssolb_dev_alloc(ssol_device* dev, void** p, size_t bytes)
+{ return dev_alloc(dev, p, bytes); }
+
+void ssolb_dev_free(ssol_device* dev, void* p, size_t bytes)
+{ dev_free(dev, p, bytes); }
+
+template<class R>
+static res_T snapshot_upload(ssol_device* dev, const FlatScene<R>& f, DScene<R>& S,
+                             DeviceSnapshot& out)
+{
+  Blob b;
+  add_scene(b, f);
+  out.alloc = b.host.size() + 256;
+  if(dev_alloc(dev, &out.d_scene, out.alloc) != cudaSuccess) {
+    out.d_scene = nullptr;
+    return RES_MEM_ERR;
+  }
+  if(cudaMemcpyAsync(out.d_scene, b.host.data(), b.host.size(), cudaMemcpyHostToDevice,
+                     (cudaStream_t)dev->stream) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  out.bytes = b.host.size();
+  bind_scene(S, f, b, (unsigned char*)out.d_scene);
+  return RES_OK;
+}
+
+res_T ssolb_snapshot_create
+  (ssol_scene* scn, const ssol_b200_options* options, DeviceSnapshot& out)
+{
+  out = DeviceSnapshot();
+  const ssol_b200_options opt = options ? *options : SSOL_B200_OPTIONS_DEFAULT;
+  if(opt.precision != SSOL_B200_FP32 && opt.precision != SSOL_B200_FP64)
+    return RES_BAD_ARG;
+  if(opt.bvh_leaf_size < 0) return RES_BAD_ARG;
+  BvhBuildParams bp;
+  bp.max_leaf = opt.bvh_leaf_size ? opt.bvh_leaf_size : 1;
+  out.precision = opt.precision;
+  std::unique_ptr<FlatScene<float>> f32;
+  std::unique_ptr<FlatScene<double>> f64;
+  res_T res;
+  if(opt.precision == SSOL_B200_FP32) {
+    f32.reset(new FlatScene<float>());
+    res = flatten_scene(scn, bp, *f32, true);
+  } else {
+    f64.reset(new FlatScene<double>());
+    res = flatten_scene(scn, bp, *f64, true);
+  }
+  if(res != RES_OK) return res;
+  if(f32 ? !validate(*f32, false) : !validate(*f64, false)) {
+    scn->dev->log_error("inconsistent device scene snapshot.\n");
+    return RES_UNKNOWN_ERR;
+  }
+  res = device_bind(scn->dev);
+  if(res != RES_OK) return res;
+  res = f32 ? snapshot_upload(scn->dev, *f32, out.s32, out)
+            : snapshot_upload(scn->dev, *f64, out.s64, out);
+  if(res != RES_OK) ssolb_snapshot_release(scn->dev, out);
+  return res;
+}
+
+void ssolb_snapshot_release(ssol_device* dev, DeviceSnapshot& s)
+{
+  dev_free(dev, s.d_scene, s.alloc);
+  s.d_scene = nullptr;
+  s.alloc = 0;
 }
 
 static void plan_release(ssol_b200_plan* p)

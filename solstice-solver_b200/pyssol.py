@@ -164,6 +164,17 @@ class B200Stats(C.Structure):
         "killed", "scene_bytes", "tally_bytes")]
 
 
+class ImageLayout(C.Structure):
+    _fields_ = [("row_pitch", C.c_size_t), ("offset", C.c_size_t), ("size", C.c_size_t),
+                ("width", C.c_size_t), ("height", C.c_size_t), ("pixel_format", C.c_int)]
+
+
+PIXEL_DOUBLE3 = 0
+FILTER_LINEAR, FILTER_NEAREST = 0, 1
+ADDRESS_CLAMP, ADDRESS_REPEAT = 0, 1
+WRITE_PIXELS = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_size_t),
+                           C.POINTER(C.c_size_t), C.c_int, C.c_void_p)
+
 VP = C.c_void_p
 PVP = C.POINTER(C.c_void_p)
 _SIGS = {
@@ -228,6 +239,20 @@ _SIGS = {
     "ssol_estimator_get_rng_state": [VP, PVP],
     "ssol_mc_receiver_get_mc_shape": [C.POINTER(McReceiver), VP, C.POINTER(McShape)],
     "ssol_mc_shape_get_mc_primitive": [C.POINTER(McShape), C.c_uint, C.POINTER(McPrimitive)],
+    "ssol_camera_create": [VP, PVP], "ssol_camera_ref_get": [VP],
+    "ssol_camera_ref_put": [VP],
+    "ssol_camera_set_proj_ratio": [VP, C.c_double], "ssol_camera_set_fov": [VP, C.c_double],
+    "ssol_camera_look_at": [VP, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                            C.POINTER(C.c_double)],
+    "ssol_image_create": [VP, PVP], "ssol_image_ref_get": [VP], "ssol_image_ref_put": [VP],
+    "ssol_image_setup": [VP, C.c_size_t, C.c_size_t, C.c_int],
+    "ssol_image_get_layout": [VP, C.POINTER(ImageLayout)],
+    "ssol_image_map": [VP, C.POINTER(C.c_void_p)], "ssol_image_unmap": [VP],
+    "ssol_image_sample": [VP, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), VP],
+    "ssol_image_write": [VP, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.c_int, VP],
+    "ssol_draw_draft": [VP, VP, C.c_size_t, C.c_size_t, C.c_size_t, WRITE_PIXELS, VP],
+    "ssol_draw_pt": [VP, VP, C.c_size_t, C.c_size_t, C.c_size_t, C.POINTER(C.c_double),
+                     WRITE_PIXELS, VP],
     "ssp_rng_create": [VP, C.c_int, PVP], "ssp_rng_ref_put": [VP],
     "ssp_rng_set": [VP, C.c_uint64], "ssp_rng_discard": [VP, C.c_uint64],
 }
@@ -247,6 +272,11 @@ _OPTIONAL = {
     "ssol_b200_batch_launch_noalloc": [VP, VP, C.POINTER(C.c_uint64), VP],
     "ssol_b200_autotune": [VP, VP, C.c_uint64, C.POINTER(B200Options),
                            C.POINTER(C.c_double)],
+    "ssol_b200_draw_draft_device": [VP, VP, C.c_size_t, C.c_size_t, C.c_size_t,
+                                    C.POINTER(B200Options), VP, C.POINTER(B200Stats)],
+    "ssol_b200_draw_pt_device": [VP, VP, C.c_size_t, C.c_size_t, C.c_size_t,
+                                 C.POINTER(C.c_double), C.c_uint64, C.POINTER(B200Options),
+                                 VP, C.POINTER(B200Stats)],
 }
 
 
@@ -641,6 +671,64 @@ class Scene:
         self.lib.call("ssol_atmosphere_set_extinction", h, C.byref(d))
         self.lib.call("ssol_scene_attach_atmosphere", self.scn, h)
         return h
+
+    # ---- camera and renderers
+    def camera(self, position=(0, 0, 0), target=(0, 0, -1), up=(0, 1, 0), fov=None,
+               ratio=None):
+        """A pinhole camera (ssol_camera_*): fov is the horizontal field of
+        view in radians, ratio width / height; both set before look_at, as
+        the reference's draw test does."""
+        h = self._new("ssol_camera_create", "ssol_camera_ref_put", self.dev)
+        if ratio is not None:
+            self.lib.call("ssol_camera_set_proj_ratio", h, float(ratio))
+        if fov is not None:
+            self.lib.call("ssol_camera_set_fov", h, float(fov))
+        d3 = C.c_double * 3
+        self.lib.call("ssol_camera_look_at", h, d3(*position), d3(*target), d3(*up))
+        return h
+
+    def draw(self, kind, cam, width, height, spp, up=(0, 0, 1), tiles=None, check=True):
+        """ssol_draw_draft (kind "draft") or ssol_draw_pt (kind "pt") through a
+        writer that fills a (height, width, 3) float64 array; `tiles`, when a
+        list, receives (x, y, w, h) per writer call. Returns (res, image)."""
+        import numpy as np
+        img = np.zeros((height, width, 3))
+
+        def write(ctx, org, sz, fmt, pixels):
+            ox, oy, sx, sy = org[0], org[1], sz[0], sz[1]
+            if fmt != PIXEL_DOUBLE3 or ox + sx > width or oy + sy > height:
+                return RES_BAD_ARG
+            buf = np.ctypeslib.as_array(C.cast(pixels, C.POINTER(C.c_double)),
+                                        shape=(sy, sx, 3))
+            img[oy:oy + sy, ox:ox + sx] = buf
+            if tiles is not None:
+                tiles.append((ox, oy, sx, sy))
+            return RES_OK
+
+        cb = WRITE_PIXELS(write)
+        if kind == "draft":
+            res = self.lib.raw("ssol_draw_draft", self.scn, cam, width, height, spp, cb, None)
+        else:
+            res = self.lib.raw("ssol_draw_pt", self.scn, cam, width, height, spp,
+                               (C.c_double * 3)(*up), cb, None)
+        if check and res != RES_OK:
+            raise SsolError("ssol_draw_" + kind, res)
+        return res, img
+
+    def draw_device(self, kind, cam, width, height, spp, device_pixels, up=(0, 0, 1),
+                    seed=0, options=None):
+        """ssol_b200_draw_*_device into `device_pixels` (a device address of
+        width x height x 3 doubles). Returns the B200Stats."""
+        st = B200Stats()
+        opt = C.byref(options) if options is not None else None
+        if kind == "draft":
+            self.lib.call("ssol_b200_draw_draft_device", self.scn, cam, width, height, spp,
+                          opt, C.c_void_p(device_pixels), C.byref(st))
+        else:
+            self.lib.call("ssol_b200_draw_pt_device", self.scn, cam, width, height, spp,
+                          (C.c_double * 3)(*up), seed, opt, C.c_void_p(device_pixels),
+                          C.byref(st))
+        return st
 
     # ---- solve
     def rng(self, seed=0, position=0):

@@ -65,17 +65,26 @@ def ramp_mirror(lib, kind):
                "exact": DNI * 100 * exact}
 
 
-def tilted_normals(lib, alpha=0.1, dist=20.0):
+def tilted_normals(lib, alpha=0.1, dist=20.0, turn_z=False):
     """A flat 2x2 mirror whose vertex normals are all (sin a, 0, cos a): the
     vertical sun is reflected along (sin 2a, 0, cos 2a), onto a 4x4 receiver
     `dist` away on that line (with the geometric normal the light would go
-    straight up and miss it). Incoming flux: DNI x 4 exactly."""
+    straight up and miss it). Incoming flux: DNI x 4 exactly.
+
+    turn_z: the mirror's instance is turned by 90 degrees about z (the same
+    square). Its third column is the identity's, so the vertex normals are
+    kept in shape space (src/ssol_material.c:632-646) and the beam still
+    goes along +x: the same DNI x 4."""
     s = P.Scene(lib)
     n = (math.sin(alpha), 0.0, math.cos(alpha))
     verts = [(-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0)]
     shape = s.mesh(verts, [(0, 2, 1), (2, 0, 3)], normals=[n] * 4)
     m = s.mirror(1.0, 0.0)
-    s.instance(s.object([(shape, m, m)]))
+    if turn_z:
+        s.instance(s.object([(shape, m, m)]),
+                   (0.0, 1.0, 0.0, -1.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0))
+    else:
+        s.instance(s.object([(shape, m, m)]))
     r = (math.sin(2 * alpha), 0.0, math.cos(2 * alpha))
     absorber = s.matte(0.0)
     rcv = s.instance(s.object([(s.rectangle(2, 2), absorber, absorber)]),

@@ -40,12 +40,13 @@ def test_gpu_baked_texcoord_shader(product):
     assert abs(r[0] - h["expected"]) <= 3 * r[2] + 1e-6 * h["expected"]
 
 
+@pytest.mark.parametrize("turn_z", [False, True], ids=["plain", "turned"])
 @pytest.mark.parametrize("precision", [P.FP64, P.FP32], ids=["fp64", "fp32"])
-def test_gpu_vertex_normals(product, oracle, precision):
-    s, h = A.tilted_normals(product)
+def test_gpu_vertex_normals(product, oracle, precision, turn_z):
+    s, h = A.tilted_normals(product, turn_z=turn_z)
     e = s.solve(200000, seed=3, options=P.options(precision=precision))
     r = e.receiver(h["receiver"])["incoming_flux"]
     assert r[0] == pytest.approx(h["expected"], rel=1e-6)
-    so, ho = A.tilted_normals(oracle)
+    so, ho = A.tilted_normals(oracle, turn_z=turn_z)
     ro = so.solve(20000, seed=3).receiver(ho["receiver"])["incoming_flux"]
     assert close(r, ro)

@@ -26,8 +26,9 @@ def test_oracle_texcoord_shader_exact(oracle):
     assert abs(h["expected"] - h["exact"]) > 5 * r[2]  # the two are told apart
 
 
-def test_oracle_vertex_normals(oracle):
-    s, h = A.tilted_normals(oracle)
+@pytest.mark.parametrize("turn_z", [False, True], ids=["plain", "turned"])
+def test_oracle_vertex_normals(oracle, turn_z):
+    s, h = A.tilted_normals(oracle, turn_z=turn_z)
     e = s.solve(20000, seed=3)
     r = e.receiver(h["receiver"])["incoming_flux"]
     assert r[0] == pytest.approx(h["expected"], rel=1e-9)
