@@ -719,6 +719,204 @@ def run_adjoint(args):
     print(json.dumps(line))
 
 
+DRAW = ("{kind}: the 1000-heliostat field (mirrors Beckmann 2 mrad, 12x12 receiver on a "
+        "100 m tower, pillbox sun el 30 az 180) over a 4x4 km matte ground (reflectivity "
+        "0.3), seen from (0, -60, 170) toward (0, 280, 0), 75 deg horizontal field of view, "
+        "{w}x{h} pixels, {spp} samples per pixel, sky radiance 0.1 above +z")
+DRAW_CAMERA = ((0.0, -60.0, 170.0), (0.0, 280.0, 0.0), (0.0, 0.0, 1.0), math.radians(75.0))
+
+
+def draw_scene(lib, args):
+    import pyssol as P
+    import workloads as W
+    s, h = W.heliostat_field(lib, n_helio=args.heliostats)
+    ground = s.matte(0.3)
+    s.instance(s.object([(s.rectangle(2000, 2000), ground, ground)]),
+               P.transform_from(None, (0.0, 0.0, -0.5)), sample=0)
+    pos, tgt, up, fov = DRAW_CAMERA
+    cam = s.camera(pos, tgt, up, fov=fov, ratio=args.width / args.height)
+    desc = DRAW.format(kind="ssol_draw_pt path tracing" if args.config == "pt"
+                       else "ssol_draw_draft", w=args.width, h=args.height, spp=args.spp)
+    return s, cam, desc
+
+
+def oracle_draw_rate(args, seconds):
+    """Oracle camera samples/s on all host cores: the same camera on a
+    reduced image whose samples take about `seconds`."""
+    import pyssol as P
+    lib = P.Lib(ORACLE_LIB)
+    s, cam, _ = draw_scene(lib, args)
+    kind = args.config
+    img = P.C.c_void_p()
+    lib.call("ssol_image_create", s.dev, P.C.byref(img))
+
+    def run(w, hh, spp):
+        lib.call("ssol_image_setup", img, w, hh, P.PIXEL_DOUBLE3)
+        wr = P.WRITE_PIXELS(("ssol_image_write", lib.dll))
+        t = time.perf_counter()
+        if kind == "draft":
+            lib.call("ssol_draw_draft", s.scn, cam, w, hh, spp, wr, img)
+        else:
+            lib.call("ssol_draw_pt", s.scn, cam, w, hh, spp, (P.C.c_double * 3)(0, 0, 1),
+                     wr, img)
+        return time.perf_counter() - t
+
+    probe_w, probe_h = max(16, args.width // 16), max(9, args.height // 16)
+    dt = run(probe_w, probe_h, args.spp)
+    rate = probe_w * probe_h * args.spp / dt
+    scale = min(1.0, math.sqrt(rate * seconds / (args.width * args.height * args.spp)))
+    w, hh = max(16, int(args.width * scale)), max(9, int(args.height * scale))
+    dt = run(w, hh, args.spp)
+    lib.call("ssol_image_ref_put", img)
+    s.close()
+    return w * hh * args.spp / dt, w, hh, dt
+
+
+def run_draw(args):
+    """The preview renderers. value: camera samples/s of the draw kernel (its
+    CUDA-event time, scene resident, L2 flushed between steps); e2e: wall
+    clock of the public ssol_draw_* call with ssol_image_write as the writer
+    (snapshot, upload, kernel, image read-back, tiles to the host image)."""
+    import torch
+    import pyssol as P
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    lib = P.load_product()
+    s, cam, desc = draw_scene(lib, args)
+    opt = P.options(P.FP64 if args.fp64 else P.FP32)
+    W_, H_, spp = args.width, args.height, args.spp
+    buf = torch.empty((H_, W_, 3), dtype=torch.float64, device="cuda")
+    flush = torch.empty(max(1, args.flush_mib) * 1024 * 1024 // 4, dtype=torch.float32,
+                        device="cuda")
+    seed = args.seed
+
+    def step(k):
+        return s.draw_device(args.config, cam, W_, H_, spp, buf.data_ptr(), up=(0, 0, 1),
+                             seed=seed + k, options=opt)
+
+    for w in range(args.warmup):
+        step(w)
+        if args.flush_mib:
+            flush.zero_()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    kms, totals = 0.0, {}
+    for k in range(args.steps):
+        st = step(args.warmup + k)
+        kms += st.kernel_ms
+        for f in ("rays", "node_visits", "triangle_tests", "quadric_tests", "bounces",
+                  "paths"):
+            totals[f] = totals.get(f, 0) + getattr(st, f)
+        scene_bytes = st.scene_bytes
+        if args.flush_mib:
+            flush.zero_()
+            torch.cuda.synchronize()
+    clk = clocks.stop()
+    samples = W_ * H_ * spp
+    value = args.steps * samples / (kms * 1e-3) / 1e6
+
+    e2e = None
+    if not args.no_e2e:
+        img = P.C.c_void_p()
+        lib.call("ssol_image_create", s.dev, P.C.byref(img))
+        lib.call("ssol_image_setup", img, W_, H_, P.PIXEL_DOUBLE3)
+        wr = P.WRITE_PIXELS(("ssol_image_write", lib.dll))
+        up = (P.C.c_double * 3)(0, 0, 1)
+
+        def public():
+            if args.config == "draft":
+                lib.call("ssol_draw_draft", s.scn, cam, W_, H_, spp, wr, img)
+            else:
+                lib.call("ssol_draw_pt", s.scn, cam, W_, H_, spp, up, wr, img)
+        public()
+        t0 = time.perf_counter()
+        e2e_steps = max(1, min(args.steps, 3))
+        for k in range(e2e_steps):
+            public()
+        dt = time.perf_counter() - t0
+        e2e = e2e_steps * samples / dt / 1e6
+        lib.call("ssol_image_ref_put", img)
+
+    peaks = measured_peaks()
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
+    sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = nsm * 128 * 2 * sm_mhz * 1e6 / 1e12
+    achieved = flops_per_run(totals) / (kms * 1e-3) / 1e12 if kms > 0 else 0.0
+    unit = "Msamples/s"
+    line = {
+        "metric": unit, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": kms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.fp64 else "f32",
+        "data": "synthetic (seeded generator, no public scene)",
+        "config": {"workload": desc, "samples_per_step": samples,
+                   "l2": ("flushed: %d MiB write between steps (scene < 2 MB, image %.0f MB)"
+                          % (args.flush_mib, W_ * H_ * 24 / 1e6)
+                          if args.flush_mib else "not flushed (profiling run)")},
+        "e2e": {"value": e2e, "unit": unit, "h2d_bytes_per_step": scene_bytes,
+                "d2h_bytes_per_step": W_ * H_ * 24,
+                "timing": "wall clock around the synchronous ssol_draw_* call"},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak else None,
+                     "traffic": None,
+                     "peak_source": "SMs x 128 FP32 lanes x 2 x measured max SM clock "
+                                    "(MEASURED_PEAKS.json sm_max_mhz)",
+                     "work_model": "20/slab x2 per node + 55/triangle + 90/quadric + "
+                                   "150/bounce + 120/sample (counted on device)",
+                     "counters_per_sample": {k: totals[k] / max(1, totals["paths"]) for k in
+                                             ("rays", "node_visits", "triangle_tests",
+                                              "quadric_tests", "bounces")},
+                     "kernel_ms": kms},
+        "clocks": clk,
+        "image_mean": float(buf.mean()),
+    }
+    if not args.no_cpu:
+        try:
+            rate, cw, ch, cdt = oracle_draw_rate(args, args.cpu_seconds)
+            line["cpu_baseline"] = {
+                "value": rate / 1e6, "unit": unit, "cores": os.cpu_count(), "kind": "port",
+                "sample": "%dx%d pixels x %d samples of the same view in %.1f s (OpenMP, "
+                          "all cores)" % (cw, ch, spp, cdt)}
+        except Exception as exc:
+            line["cpu_baseline"] = {"value": None, "unit": unit, "cores": os.cpu_count(),
+                                    "kind": "port", "sample": "failed: %s" % exc}
+    print(json.dumps(line))
+    s.close()
+
+
+def run_draw_reference(args):
+    """The oracle's renderer on the host cores, each step a bounded sample
+    (a reduced image of the same view)."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    rates = []
+    for k in range(args.warmup + args.steps):
+        rate, cw, ch, cdt = oracle_draw_rate(args, args.ref_step_seconds)
+        if k >= args.warmup:
+            rates.append((rate, cw, ch, cdt))
+    total_s = sum(r[3] for r in rates)
+    total = sum(r[0] * r[3] for r in rates)
+    value = total / total_s / 1e6
+    unit = "Msamples/s"
+    s_desc = DRAW.format(kind="ssol_draw_pt path tracing" if args.config == "pt"
+                         else "ssol_draw_draft", w=args.width, h=args.height, spp=args.spp)
+    line = {
+        "impl": "reference", "metric": unit, "value": value, "unit": unit,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": s_desc, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": os.cpu_count(), "kind": "port",
+                         "sample": "%dx%d pixels x %d samples per step" % (
+                             rates[0][1], rates[0][2], args.spp)},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -726,7 +924,12 @@ def main():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--config", default="field",
-                   choices=["field", "mirror", "beamdown", "suns", "adjoint"])
+                   choices=["field", "mirror", "beamdown", "suns", "adjoint", "draft",
+                            "pt"])
+    p.add_argument("--width", type=int, default=1920)
+    p.add_argument("--height", type=int, default=1080)
+    p.add_argument("--spp", type=int, default=None,
+                   help="samples per pixel of the draw configs (draft 4, pt 16)")
     p.add_argument("--fd-params", type=int, default=32)
     p.add_argument("--fd-paths", type=int, default=100_000_000)
     p.add_argument("--heliostats", type=int, default=1000)
@@ -751,8 +954,14 @@ def main():
     if args.paths is None:
         args.paths = {"beamdown": 200_000_000, "mirror": 1_000_000}.get(args.config,
                                                                          100_000_000)
-    if args.impl == "reference":
+    if args.spp is None:
+        args.spp = 16 if args.config == "pt" else 4
+    if args.impl == "reference" and args.config in ("draft", "pt"):
+        run_draw_reference(args)
+    elif args.impl == "reference":
         run_reference(args)
+    elif args.config in ("draft", "pt"):
+        run_draw(args)
     elif args.config == "suns":
         run_suns(args)
     elif args.config == "adjoint":
