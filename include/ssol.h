@@ -13,8 +13,10 @@
  *    the target, not binary compatibility with RSys-built callers.
  *  - `struct ssp_rng` is the counter-based Philox shim declared in ssp.h.
  *  - Shader callbacks are evaluated on the host when `ssol_solve` snapshots
- *    the scene (per material and per sun-spectrum wavelength node); they may
- *    depend on the wavelength but not on the surface position.
+ *    the scene: per material at the sun-spectrum wavelength nodes, and, for
+ *    mirror and matte shaders that vary over a mesh, at every vertex of that
+ *    mesh; the device interpolates in wavelength and with the barycentric
+ *    weights of the hit. Normal shaders are taken to return Ns.
  *  - `ssol_draw_draft` / `ssol_draw_pt` (src/ssol.h:1225-1244) render the
  *    whole image on the GPU into a device buffer, copy it back once and then
  *    hand it to the writer tile by tile (32 x 32, Morton order of tiles, one
