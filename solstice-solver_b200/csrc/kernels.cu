@@ -956,6 +956,12 @@ __device__ __noinline__ void commit10(double* dst, const double v[6], double f)
   }
 }
 
+__device__ __noinline__ void flush_racc(double* dst, const double* racc)
+{
+#pragma unroll 1
+  for(int k = 0; k < 2 * NRCV_Q; ++k) red_add(dst + k, racc[k]);
+}
+
 template<class R> struct PathState {
   int phase;
   int samp;
@@ -1161,7 +1167,8 @@ template<class R>
 __device__ __noinline__ void commit_path
   (const DScene<R>& S, const DTallies& T, PathState<R>& p, int end,
    double* acc, double* ps, int stride, double* smem_rcv, const int* xr,
-   const int* xp, const double (*xv)[6])
+   const int* xp, const double (*xv)[6], double* racc = nullptr,
+   int* racc_slot = nullptr)
 {
   atomicAdd(&T.nb_samples[p.samp], 1ull);
   if(p.overflow) end = END_FAIL;
@@ -1203,7 +1210,23 @@ __device__ __noinline__ void commit_path
   for(int q = 0; q < 6; ++q) v0[q] = ps[(PS_V0 + q) * stride];
   double* rbase = smem_rcv ? smem_rcv : T.rcv;
   if(p.nent == 1) {
-    commit10(rbase + (size_t)p.r0 * NRCV_Q * 2, v0, f);
+    if(racc) {
+      /* The thread's running sums of one receiver side, flushed when the
+       * side changes: no atomics while its paths keep reaching it */
+      if(*racc_slot != p.r0) {
+        if(*racc_slot >= 0) flush_racc(rbase + (size_t)*racc_slot * NRCV_Q * 2, racc);
+        *racc_slot = p.r0;
+        for(int k = 0; k < 2 * NRCV_Q; ++k) racc[k] = 0.0;
+      }
+      double q[NRCV_Q];
+      expand10(v0, f, q);
+      for(int k = 0; k < NRCV_Q; ++k) {
+        racc[2 * k] += q[k];
+        racc[2 * k + 1] += q[k] * q[k];
+      }
+    } else {
+      commit10(rbase + (size_t)p.r0 * NRCV_Q * 2, v0, f);
+    }
     commit10(T.samp_rcv + ((size_t)p.samp * S.nrcv + p.r0) * NRCV_Q * 2, v0, f);
     if(p.p0 >= 0) commit10(T.prim + (size_t)p.p0 * NRCV_Q * 2, v0, f);
     return;
@@ -1307,6 +1330,8 @@ realisation_kernel
   uint32_t bounces = 0, npaths = 0;
   int xr[MAX_EXTRA], xp[MAX_EXTRA];
   double xv[MAX_EXTRA][6];
+  double racc[2 * NRCV_Q];
+  int racc_slot = -1;
 
   for(;;) {
     /* Regeneration: idle lanes take the next realisations */
@@ -1428,10 +1453,13 @@ realisation_kernel
           : (end == END_FAIL || p.overflow) ? 3 : (p.nent > 0 ? 2 : 0);
         tr.path_nv[p.tslot] = (int32_t)p.tseq;
       }
-      commit_path(S, T, p, end, acc, ps, bd, smem_rcv, xr, xp, xv);
+      commit_path(S, T, p, end, acc, ps, bd, smem_rcv, xr, xp, xv, racc, &racc_slot);
       p.phase = PH_NONE;
     }
   }
+
+  if(racc_slot >= 0)
+    flush_racc((use_smem_rcv ? smem_rcv : T.rcv) + (size_t)racc_slot * NRCV_Q * 2, racc);
 
   /* Warp then block reduction of the global sums, one commit per block */
   const int warp = tid >> 5;
