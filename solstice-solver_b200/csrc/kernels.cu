@@ -1536,6 +1536,18 @@ batch_kernel
   uint32_t bounces = 0, npaths = 0;
   int xr[MAX_EXTRA], xp[MAX_EXTRA];
   double xv[MAX_EXTRA][6];
+  /* Running sums of one (item, receiver side), as in realisation_kernel;
+   * flushed into the item's warp slot (or its tallies) when either changes */
+  double racc[2 * NRCV_Q];
+  int racc_slot = -1, racc_item = -1;
+  auto racc_flush = [&]() {
+    if(racc_slot < 0) return;
+    double* dst = rcvd && racc_item == stag[cur] ? wslots + cur * ss + 2 * NGLOBAL
+      : rcvd && racc_item == stag[cur ^ 1] ? wslots + (cur ^ 1) * ss + 2 * NGLOBAL
+      : tallies[racc_item].rcv;
+    flush_racc(dst + (size_t)racc_slot * NRCV_Q * 2, racc);
+    racc_slot = -1;
+  };
 
   for(;;) {
     const unsigned need = __ballot_sync(0xffffffffu, p.phase == PH_NONE && !done);
@@ -1684,11 +1696,14 @@ batch_kernel
         if(it == stag[cur]) rb = wslots + cur * ss + 2 * NGLOBAL;
         else if(it == stag[cur ^ 1]) rb = wslots + (cur ^ 1) * ss + 2 * NGLOBAL;
       }
-      commit_path(S, tallies[it], p, end, acc, ps, bd, rb, xr, xp, xv);
+      if(racc_item != it) racc_flush();
+      racc_item = it;
+      commit_path(S, tallies[it], p, end, acc, ps, bd, rb, xr, xp, xv, racc, &racc_slot);
       p.phase = PH_NONE;
     }
   }
 
+  racc_flush();
   if(acc_item >= 0) {
     double* sl = acc_item == stag[cur] ? wslots + cur * ss
       : acc_item == stag[cur ^ 1] ? wslots + (cur ^ 1) * ss : nullptr;
