@@ -190,6 +190,24 @@ SSOL_API res_T ssol_b200_batch_finish
    const size_t max_failed_count, void* stream,
    struct ssol_estimator** estimators);
 
+/* Shaders (ssol_shader_getter_T) for materials whose properties are the
+ * same everywhere. No counterpart in the reference, whose callers write such
+ * callbacks themselves. ssol_b200_shader_param0 / _param1 return the first /
+ * second double of the material's parameter buffer (ssol_param_buffer_get,
+ * 0 without a buffer); ssol_b200_shader_Ns returns the fragment's shading
+ * normal. Being plain C, they cost nothing when the scene is snapshot from
+ * several host threads, unlike callbacks into an interpreter that must take
+ * its lock on every call. */
+SSOL_API void ssol_b200_shader_param0
+  (struct ssol_device* dev, struct ssol_param_buffer* buf, const double wavelength,
+   const struct ssol_surface_fragment* frag, double* val);
+SSOL_API void ssol_b200_shader_param1
+  (struct ssol_device* dev, struct ssol_param_buffer* buf, const double wavelength,
+   const struct ssol_surface_fragment* frag, double* val);
+SSOL_API void ssol_b200_shader_Ns
+  (struct ssol_device* dev, struct ssol_param_buffer* buf, const double wavelength,
+   const struct ssol_surface_fragment* frag, double* val);
+
 /* Renderers into device memory. No counterpart in the reference: its
  * ssol_draw_draft / ssol_draw_pt (src/ssol.h:1225-1244) hand tiles to a host
  * writer, which the ssol.h versions here still do. These leave the image in

@@ -70,6 +70,39 @@ int split(std::vector<PrimBox>& p, std::vector<std::array<double, 3>>& c, int b,
   cb.reset();
   for(int i = b; i < e; ++i) cb.grow(c[i].data(), c[i].data());
   const bool force_median = depth >= prm.max_depth - 10;
+  /* Small ranges: exact SAH over the centroid order on each axis (binning's
+   * fixed cost per node dominates there, and the exact sweep is at least as
+   * good a split) */
+  constexpr int EXACT_MAX = 32;
+  if(!force_median && n <= EXACT_MAX) {
+    int ord[3][EXACT_MAX];
+    double best = std::numeric_limits<double>::max();
+    int best_a = -1, best_k = -1;
+    for(int a = 0; a < 3; ++a) {
+      for(int i = 0; i < n; ++i) ord[a][i] = b + i;
+      std::sort(ord[a], ord[a] + n, [&](int x, int y) {
+        return c[x][a] < c[y][a] || (c[x][a] == c[y][a] && x < y);
+      });
+      double right_area[EXACT_MAX];
+      Box acc;
+      acc.reset();
+      for(int k = n - 1; k > 0; --k) {
+        acc.grow(p[ord[a][k]].lo, p[ord[a][k]].hi);
+        right_area[k] = acc.area();
+      }
+      acc.reset();
+      for(int k = 0; k < n - 1; ++k) {
+        acc.grow(p[ord[a][k]].lo, p[ord[a][k]].hi);
+        const double cost = acc.area() * (k + 1) + right_area[k + 1] * (n - k - 1);
+        if(cost < best) { best = cost; best_a = a; best_k = k; }
+      }
+    }
+    PrimBox tp[EXACT_MAX];
+    std::array<double, 3> tc[EXACT_MAX];
+    for(int i = 0; i < n; ++i) { tp[i] = p[ord[best_a][i]]; tc[i] = c[ord[best_a][i]]; }
+    for(int i = 0; i < n; ++i) { p[b + i] = tp[i]; c[b + i] = tc[i]; }
+    return b + best_k + 1;
+  }
   double best_cost = std::numeric_limits<double>::max();
   int best_axis = -1, best_bin = -1;
   constexpr int MAX_BINS = 64;

@@ -11,6 +11,7 @@
  */
 #include "objects.h"
 #include "tessellate.h"
+#include "../../include/ssol_b200.h"
 
 #include <cmath>
 #include <cstdarg>
@@ -738,6 +739,34 @@ extern "C" void* ssol_param_buffer_get(ssol_param_buffer* b)
 {
   if(!b) return nullptr;
   return b->used ? pool_base(b) : nullptr;
+}
+
+/*******************************************************************************
+ * Native shaders for properties that do not vary (include/ssol_b200.h)
+ ******************************************************************************/
+extern "C" void ssol_b200_shader_param0
+  (ssol_device*, ssol_param_buffer* buf, const double, const ssol_surface_fragment*,
+   double* val)
+{
+  const double* p = static_cast<const double*>(ssol_param_buffer_get(buf));
+  *val = p ? p[0] : 0.0;
+}
+
+extern "C" void ssol_b200_shader_param1
+  (ssol_device*, ssol_param_buffer* buf, const double, const ssol_surface_fragment*,
+   double* val)
+{
+  const double* p = static_cast<const double*>(ssol_param_buffer_get(buf));
+  *val = p ? p[1] : 0.0;
+}
+
+extern "C" void ssol_b200_shader_Ns
+  (ssol_device*, ssol_param_buffer*, const double, const ssol_surface_fragment* frag,
+   double* val)
+{
+  val[0] = frag->Ns[0];
+  val[1] = frag->Ns[1];
+  val[2] = frag->Ns[2];
 }
 
 /*******************************************************************************

@@ -77,9 +77,58 @@ namespace {
 struct MemCache {
   std::mutex lock;
   std::vector<std::pair<void*, size_t>> blocks;
+  std::vector<std::pair<void*, size_t>> pinned; /* page-locked host blocks */
 };
 constexpr size_t CACHE_BLOCKS = 8;
 constexpr size_t CACHE_BYTES = size_t(4) << 30;
+constexpr size_t PINNED_BLOCKS = 4;
+constexpr size_t PINNED_BYTES = size_t(2) << 30;
+}
+
+static MemCache* mem_cache(ssol_device* dev)
+{
+  if(!dev->mem_cache) dev->mem_cache = new (std::nothrow) MemCache();
+  return static_cast<MemCache*>(dev->mem_cache);
+}
+
+/* Page-locked host blocks (tally read-back of batches) are kept for reuse
+ * like device blocks: locking hundreds of megabytes takes longer than the
+ * read-back itself */
+static cudaError_t host_alloc(ssol_device* dev, void** p, size_t bytes)
+{
+  MemCache* c = mem_cache(dev);
+  if(c) {
+    std::lock_guard<std::mutex> g(c->lock);
+    size_t best = c->pinned.size();
+    for(size_t i = 0; i < c->pinned.size(); ++i) {
+      const size_t cap = c->pinned[i].second;
+      if(cap >= bytes && cap / 4 <= bytes
+      && (best == c->pinned.size() || cap < c->pinned[best].second))
+        best = i;
+    }
+    if(best < c->pinned.size()) {
+      *p = c->pinned[best].first;
+      c->pinned.erase(c->pinned.begin() + (long)best);
+      return cudaSuccess;
+    }
+  }
+  return cudaMallocHost(p, bytes);
+}
+
+static void host_free(ssol_device* dev, void* p, size_t bytes)
+{
+  if(!p) return;
+  MemCache* c = mem_cache(dev);
+  if(!c) { cudaFreeHost(p); return; }
+  std::lock_guard<std::mutex> g(c->lock);
+  c->pinned.emplace_back(p, bytes);
+  size_t total = 0;
+  for(const auto& b : c->pinned) total += b.second;
+  while(c->pinned.size() > PINNED_BLOCKS || total > PINNED_BYTES) {
+    total -= c->pinned.front().second;
+    cudaFreeHost(c->pinned.front().first);
+    c->pinned.erase(c->pinned.begin());
+  }
 }
 
 static cudaError_t dev_alloc(ssol_device* dev, void** p, size_t bytes)
@@ -129,6 +178,7 @@ void ssolb_device_release_gpu(ssol_device* dev)
   if(dev->mem_cache) {
     MemCache* c = static_cast<MemCache*>(dev->mem_cache);
     for(const auto& b : c->blocks) cudaFree(b.first);
+    for(const auto& b : c->pinned) cudaFreeHost(b.first);
     delete c;
     dev->mem_cache = nullptr;
   }
@@ -1008,15 +1058,16 @@ struct ssol_b200_batch {
   bool timing_valid = false;
   uint64_t h_seed = 0;
   void* h_tally = nullptr; /* pinned tally read-back, allocated on first finish */
+  size_t scene_alloc = 0, tally_alloc = 0; /* bytes of d_scene, d_tally */
 };
 
 static void batch_release(ssol_b200_batch* b)
 {
   if(b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
   if(b->graph) cudaGraphDestroy(b->graph);
-  if(b->d_scene) cudaFree(b->d_scene);
-  if(b->d_tally) cudaFree(b->d_tally);
-  if(b->h_tally) cudaFreeHost(b->h_tally);
+  dev_free(b->dev, b->d_scene, b->scene_alloc);
+  dev_free(b->dev, b->d_tally, b->tally_alloc);
+  host_free(b->dev, b->h_tally, b->tally_total);
   if(b->ev0) cudaEventDestroy(b->ev0);
   if(b->ev1) cudaEventDestroy(b->ev1);
   for(ssol_scene* s : b->scenes) ssol_scene_ref_put(s);
@@ -1042,28 +1093,40 @@ extern "C" res_T ssol_b200_batch_ref_put(ssol_b200_batch* b)
 template<class R>
 static res_T batch_upload(ssol_b200_batch* b, std::vector<FlatScene<R>>& f)
 {
+  /* Each item's arrays are laid out in a blob of its own, on the host
+   * threads; the blobs sit one after the other (256-byte aligned) in one
+   * device block, followed by the DScene array */
   const size_t n = f.size();
-  Blob blob;
-  std::vector<size_t> first_index(n);
+  std::vector<Blob> blobs(n);
+  parallel_for(n, [&](size_t i) { add_scene(blobs[i], f[i]); });
+  std::vector<size_t> base_off(n);
+  size_t total = 0;
   for(size_t i = 0; i < n; ++i) {
-    first_index[i] = blob.offsets.size();
-    add_scene(blob, f[i]);
+    base_off[i] = total;
+    total = (total + blobs[i].host.size() + 255) & ~size_t(255);
   }
-  /* DScene array at the end, filled once the base address is known */
-  std::vector<DScene<R>> S(n);
-  const size_t s_off = blob.add(S);
-  if(cudaMalloc(&b->d_scene, blob.host.size() + 256) != cudaSuccess)
+  const size_t s_off = total;
+  total += n * sizeof(DScene<R>);
+  if(dev_alloc(b->dev, &b->d_scene, total + 256) != cudaSuccess) {
+    b->d_scene = nullptr;
     return RES_MEM_ERR;
+  }
+  b->scene_alloc = total + 256;
   unsigned char* base = (unsigned char*)b->d_scene;
-  for(size_t i = 0; i < n; ++i) bind_scene(S[i], f[i], blob, base, first_index[i]);
-  std::memcpy(blob.host.data() + s_off, S.data(), n * sizeof(DScene<R>));
-  if(cudaMemcpyAsync(b->d_scene, blob.host.data(), blob.host.size(),
-                     cudaMemcpyHostToDevice, (cudaStream_t)b->dev->stream)
-     != cudaSuccess)
+  std::vector<DScene<R>> S(n);
+  const cudaStream_t st = (cudaStream_t)b->dev->stream;
+  for(size_t i = 0; i < n; ++i) {
+    bind_scene(S[i], f[i], blobs[i], base + base_off[i]);
+    if(!blobs[i].host.empty()
+    && cudaMemcpyAsync(base + base_off[i], blobs[i].host.data(), blobs[i].host.size(),
+                       cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return RES_UNKNOWN_ERR;
+  }
+  if(cudaMemcpyAsync(base + s_off, S.data(), n * sizeof(DScene<R>),
+                     cudaMemcpyHostToDevice, st) != cudaSuccess)
     return RES_UNKNOWN_ERR;
-  if(cudaStreamSynchronize((cudaStream_t)b->dev->stream) != cudaSuccess)
-    return RES_UNKNOWN_ERR;
-  b->scene_bytes = blob.host.size();
+  if(cudaStreamSynchronize(st) != cudaSuccess) return RES_UNKNOWN_ERR;
+  b->scene_bytes = total;
   b->d_scenes = base + s_off;
   return RES_OK;
 }
@@ -1149,7 +1212,12 @@ extern "C" res_T ssol_b200_batch_create
   off += 256;
   const size_t o_stats = off;
   off += (sizeof(DStats) + 255) & ~size_t(255);
-  if(cudaMalloc(&b->d_tally, off) != cudaSuccess) { batch_release(b); return RES_MEM_ERR; }
+  if(dev_alloc(dev, &b->d_tally, off) != cudaSuccess) {
+    b->d_tally = nullptr;
+    batch_release(b);
+    return RES_MEM_ERR;
+  }
+  b->tally_alloc = off;
   unsigned char* base = (unsigned char*)b->d_tally;
   std::vector<DTallies> T(nscenes);
   for(size_t i = 0; i < nscenes; ++i)
@@ -1322,7 +1390,7 @@ extern "C" res_T ssol_b200_batch_finish
   if(!b || !rng || !out) return RES_BAD_ARG;
   const cudaStream_t s = stream ? (cudaStream_t)stream : (cudaStream_t)b->dev->stream;
   /* Pinned read-back buffer, kept with the batch */
-  if(!b->h_tally && cudaMallocHost(&b->h_tally, b->tally_total) != cudaSuccess) {
+  if(!b->h_tally && host_alloc(b->dev, &b->h_tally, b->tally_total) != cudaSuccess) {
     b->h_tally = nullptr;
     return RES_MEM_ERR;
   }

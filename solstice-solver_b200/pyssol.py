@@ -296,6 +296,16 @@ class Lib:
                 f = getattr(self.dll, name)
                 f.argtypes = args
                 f.restype = C.c_int
+        self.dll.ssol_param_buffer_create.argtypes = [VP, C.c_size_t, PVP]
+        self.dll.ssol_param_buffer_create.restype = C.c_int
+        self.dll.ssol_param_buffer_ref_put.argtypes = [VP]
+        self.dll.ssol_param_buffer_ref_put.restype = C.c_int
+        self.dll.ssol_param_buffer_allocate.argtypes = [VP, C.c_size_t, C.c_size_t, VP]
+        self.dll.ssol_param_buffer_allocate.restype = VP
+        self.dll.ssol_material_set_param_buffer.argtypes = [VP, VP]
+        self.dll.ssol_material_set_param_buffer.restype = C.c_int
+        # native shaders for constant properties (B200 library only)
+        self.native_shaders = hasattr(self.dll, "ssol_b200_shader_param0")
         self.dll.ssp_rng_get.argtypes = [VP]
         self.dll.ssp_rng_get.restype = C.c_uint64
         self.dll.ssp_rng_canonical.argtypes = [VP]
@@ -591,15 +601,46 @@ class Scene:
         self._keep.append(cb)
         return cb
 
+    def _native(self, material, values):
+        """Native shaders reading `values` from the material's parameter
+        buffer (ssol_b200_shader_param0/1, ssol_b200_shader_Ns), or None when
+        the library has none or a value is a Python function. Python
+        callbacks would take the interpreter's lock on every call when the
+        library snapshots scenes from its worker threads."""
+        if not self.lib.native_shaders or any(callable(v) for v in values):
+            return None
+        buf = self._new("ssol_param_buffer_create", "ssol_param_buffer_ref_put", self.dev,
+                        8 * len(values))
+        mem = self.lib.dll.ssol_param_buffer_allocate(buf, 8 * len(values), 8, None)
+        arr = C.cast(mem, C.POINTER(C.c_double))
+        for i, v in enumerate(values):
+            arr[i] = float(v)
+        self.lib.call("ssol_material_set_param_buffer", material, buf)
+        dll = self.lib.dll
+        return ([SHADER(("ssol_b200_shader_param%d" % i, dll)) for i in range(len(values))],
+                SHADER(("ssol_b200_shader_Ns", dll)))
+
     def mirror(self, reflectivity=1.0, roughness=0.0, distrib=BECKMANN):
         h = self._new("ssol_material_create_mirror", "ssol_material_ref_put", self.dev)
-        s = MirrorShader(self._normal(), self._const(reflectivity), self._const(roughness))
+        nat = self._native(h, (reflectivity, roughness))
+        if nat is not None:
+            (r, g), n = nat
+            s = MirrorShader(n, r, g)
+            self._keep += [n, r, g]
+        else:
+            s = MirrorShader(self._normal(), self._const(reflectivity), self._const(roughness))
         self.lib.call("ssol_mirror_setup", h, C.byref(s), distrib)
         return h
 
     def matte(self, reflectivity=0.0):
         h = self._new("ssol_material_create_matte", "ssol_material_ref_put", self.dev)
-        s = MatteShader(self._normal(), self._const(reflectivity))
+        nat = self._native(h, (reflectivity,))
+        if nat is not None:
+            (r,), n = nat
+            s = MatteShader(n, r)
+            self._keep += [n, r]
+        else:
+            s = MatteShader(self._normal(), self._const(reflectivity))
         self.lib.call("ssol_matte_setup", h, C.byref(s))
         return h
 

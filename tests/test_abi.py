@@ -155,3 +155,30 @@ def test_batch_host_path(product):
         product.raw("ssol_b200_batch_ref_put", h)
     else:
         assert res == P.RES_UNKNOWN_ERR
+
+
+def test_native_constant_shaders(product):
+    """ssol_b200_shader_param0/1 read the material's parameter buffer,
+    ssol_b200_shader_Ns returns the fragment's shading normal"""
+    import ctypes as C
+    import pyssol as P
+    s = P.Scene(product)
+    dll = product.dll
+    buf = C.c_void_p()
+    product.call("ssol_param_buffer_create", s.dev, 16, C.byref(buf))
+    mem = dll.ssol_param_buffer_allocate(buf, 16, 8, None)
+    arr = C.cast(mem, C.POINTER(C.c_double))
+    arr[0], arr[1] = 0.7, 0.003
+    frag = P.SurfaceFragment()
+    frag.Ns[0], frag.Ns[1], frag.Ns[2] = 0.6, 0.0, 0.8
+    out = (C.c_double * 3)()
+    for name, want in (("ssol_b200_shader_param0", 0.7), ("ssol_b200_shader_param1", 0.003)):
+        f = P.SHADER((name, dll))
+        f(s.dev, buf, 500.0, C.byref(frag), out)
+        assert out[0] == want
+        f(s.dev, None, 500.0, C.byref(frag), out)
+        assert out[0] == 0.0
+    P.SHADER(("ssol_b200_shader_Ns", dll))(s.dev, None, 500.0, C.byref(frag), out)
+    assert tuple(out) == (0.6, 0.0, 0.8)
+    product.call("ssol_param_buffer_ref_put", buf)
+    s.close()
