@@ -165,12 +165,20 @@ def cpu_reference_rate(args, seconds):
     t = time.perf_counter()
     s.solve(probe, seed=123)
     rate = probe / (time.perf_counter() - t)
-    n = int(min(max(rate * seconds, probe), 5e8))
-    t = time.perf_counter()
-    est = s.solve(n, seed=124)
-    dt = time.perf_counter() - t
-    del est
-    return n / dt, n, dt
+    # Solves of about a quarter of the sample each, until the sample has run
+    # for `seconds` (the probe's rate is only a first guess)
+    total_n, dt, k = 0, 0.0, 0
+    while dt < seconds and k < 64:
+        n = int(min(max(rate * seconds / 4, probe), 5e8))
+        t = time.perf_counter()
+        est = s.solve(n, seed=124 + k)
+        step = time.perf_counter() - t
+        del est
+        total_n += n
+        dt += step
+        rate = n / step
+        k += 1
+    return total_n / dt, total_n, dt
 
 
 def run_reference(args):
@@ -326,6 +334,27 @@ def run_b200(args):
             dt = float(t[0])
         e2e_value = e2e_steps * e2e_n * world / dt / 1e6
 
+    # Precision: this build against the all-FP64 build on identical random
+    # numbers (same seed and realisation ids), outside the timed region
+    prec = None
+    if not args.fp64 and not args.no_fp64_check and rank == 0:
+        e32 = s.solve(n, seed=args.seed + 11, options=opt)
+        o64 = P.options(P.FP64, block_size=opt.block_size, waves=opt.waves,
+                        leaf=opt.bvh_leaf_size, min_blocks=opt.min_blocks_per_sm)
+        e64 = s.solve(n, seed=args.seed + 11, options=o64)
+        rel = {}
+        for name, a, b in ([("global." + k, e32.globals()[k], e64.globals()[k])
+                            for k in e64.globals()]
+                           + [("receiver." + k, e32.receiver(h["receiver"])[k],
+                               e64.receiver(h["receiver"])[k])
+                              for k in e64.receiver(h["receiver"])]):
+            if b[0] != 0:
+                rel[name] = (a[0] - b[0]) / b[0]
+        prec = {"paths": n, "max_abs_rel_diff": max(abs(v) for v in rel.values()),
+                "rel_diff": rel, "what": "FP32 geometry/BSDF build vs all-FP64 build, "
+                "same seed and realisation ids, every global and receiver estimate"}
+        del e32, e64
+
     peaks = measured_peaks()
     nsm = torch.cuda.get_device_properties(local).multi_processor_count
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
@@ -362,6 +391,7 @@ def run_b200(args):
                                             "quadric_tests", "bounces")},
                      "kernel_ms": kernel_ms},
         "clocks": clk,
+        "precision_vs_fp64": prec,
         "estimate": {"absorbed_by_receivers_W": g["absorbed_by_receivers"][0],
                      "rel_se": g["absorbed_by_receivers"][2] / max(1e-30,
                                                                   g["absorbed_by_receivers"][0])},
@@ -947,6 +977,8 @@ def main():
     p.add_argument("--flush-mib", type=int, default=256,
                    help="L2 flush buffer written between steps (profiling: 0)")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-fp64-check", action="store_true",
+                   help="skip the FP32 vs all-FP64 comparison of the field configs")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--ref-step-seconds", type=float, default=10.0)

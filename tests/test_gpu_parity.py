@@ -91,6 +91,22 @@ def test_fp32_vs_fp64(product):
     assert abs(a - b) <= 1e-3 * abs(b)
 
 
+def test_fp32_vs_fp64_full_field(product):
+    """The 1000-heliostat field with its 64 x 64 per-primitive receiver,
+    5e7 paths: every global and receiver estimate of the FP32 build within
+    1e-5 relative of the all-FP64 build on identical random numbers."""
+    s, h = W.heliostat_field(product)
+    n = 50_000_000
+    e32 = s.solve(n, seed=9, options=P.options(P.FP32))
+    e64 = s.solve(n, seed=9, options=P.options(P.FP64))
+    pairs = [(k, e32.globals()[k], e64.globals()[k]) for k in e64.globals()]
+    r32, r64 = e32.receiver(h["receiver"]), e64.receiver(h["receiver"])
+    pairs += [(k, r32[k], r64[k]) for k in r64]
+    for k, a, b in pairs:
+        assert abs(a[0] - b[0]) <= 1e-5 * abs(b[0]), (k, a[0], b[0])
+    s.close()
+
+
 def test_gpu_solver1_closed_forms(product):
     """src/test_ssol_solver1.c:312-373 on the GPU."""
     s, h = R.solver1_base(product)
