@@ -7,6 +7,8 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
+#include <thread>
 #include <cmath>
 #include <limits>
 
@@ -190,76 +192,164 @@ int split(std::vector<PrimBox>& p, std::vector<std::array<double, 3>>& c, int b,
 
 } /* namespace */
 
+namespace {
+
+/* Node arrays under construction; node ids are local to the builder */
+struct Builder {
+  std::vector<double> lo, hi;
+  std::vector<int32_t> child, count;
+  std::vector<uint32_t> refs;
+  int depth = 0;
+  int new_node()
+  {
+    const int id = (int)(child.size() / 2);
+    lo.resize(lo.size() + 6, 0);
+    hi.resize(hi.size() + 6, 0);
+    child.resize(child.size() + 2, 0);
+    count.resize(count.size() + 2, 0);
+    return id;
+  }
+  void set_slot(int slot, const Box& b, int c, int n)
+  {
+    for(int k = 0; k < 3; ++k) {
+      lo[(size_t)slot * 3 + k] = b.lo[k];
+      hi[(size_t)slot * 3 + k] = b.hi[k];
+    }
+    child[slot] = c;
+    count[slot] = n;
+  }
+};
+
+/* Expands tasks top down. Ranges smaller than `defer_below` (when > 0) are
+ * not expanded but returned in `deferred`, still to be built. */
+void run_tasks(std::vector<PrimBox>& prims, std::vector<std::array<double, 3>>& cent,
+               const BvhBuildParams& prm, Builder& B, std::vector<Task> stack,
+               int defer_below, std::vector<Task>* deferred)
+{
+  while(!stack.empty()) {
+    const Task t = stack.back();
+    stack.pop_back();
+    if(defer_below > 0 && t.end - t.begin < defer_below) {
+      deferred->push_back(t);
+      continue;
+    }
+    B.depth = std::max(B.depth, t.depth + 1);
+    const Box b = bounds(prims, t.begin, t.end);
+    const int s = split(prims, cent, t.begin, t.end, prm, t.depth);
+    if(s < 0) {
+      const int first = (int)B.refs.size();
+      for(int i = t.begin; i < t.end; ++i) B.refs.push_back(prims[i].ref);
+      B.set_slot(t.node * 2 + t.slot, b, first, t.end - t.begin);
+    } else {
+      const int id = B.new_node();
+      B.set_slot(t.node * 2 + t.slot, b, id, 0);
+      stack.push_back({t.begin, s, id, 0, t.depth + 1});
+      stack.push_back({s, t.end, id, 1, t.depth + 1});
+    }
+  }
+}
+
+} /* namespace */
+
 void build_bvh(std::vector<PrimBox> prims, const BvhBuildParams& prm,
                BvhResult& out)
 {
   out = BvhResult();
+  Builder B;
   /* Node 0 is the root; its two slots hold the two top-level children */
-  auto new_node = [&]() {
-    const int id = (int)(out.child.size() / 2);
-    out.lo.resize(out.lo.size() + 6, 0);
-    out.hi.resize(out.hi.size() + 6, 0);
-    out.child.resize(out.child.size() + 2, 0);
-    out.count.resize(out.count.size() + 2, 0);
-    return id;
-  };
-  auto set_slot = [&](int slot, const Box& b, int child, int count) {
-    for(int c = 0; c < 3; ++c) {
-      out.lo[(size_t)slot * 3 + c] = b.lo[c];
-      out.hi[(size_t)slot * 3 + c] = b.hi[c];
-    }
-    out.child[slot] = child;
-    out.count[slot] = count;
-  };
-
-  const int root = new_node();
+  const int root = B.new_node();
   const int n = (int)prims.size();
   if(n == 0) {
     Box empty;
     empty.reset();
-    set_slot(root * 2 + 0, empty, 0, -1);
-    set_slot(root * 2 + 1, empty, 0, -1);
+    B.set_slot(root * 2 + 0, empty, 0, -1);
+    B.set_slot(root * 2 + 1, empty, 0, -1);
+    out.lo = std::move(B.lo);
+    out.hi = std::move(B.hi);
+    out.child = std::move(B.child);
+    out.count = std::move(B.count);
     out.primrefs.push_back(0);
     return;
   }
   std::vector<std::array<double, 3>> cent(prims.size());
   for(size_t i = 0; i < prims.size(); ++i)
     for(int a = 0; a < 3; ++a) cent[i][a] = centroid(prims[i], a);
-  std::vector<Task> stack;
   int m = split(prims, cent, 0, n, prm, 0);
   if(m < 0) {
     /* Whole scene in one leaf; the second slot is an empty box */
     Box empty;
     empty.reset();
-    for(int i = 0; i < n; ++i) out.primrefs.push_back(prims[i].ref);
-    set_slot(root * 2 + 0, bounds(prims, 0, n), 0, n);
-    set_slot(root * 2 + 1, empty, 0, -1);
-    out.depth = 1;
-    return;
-  }
-  stack.push_back({0, m, root, 0, 1});
-  stack.push_back({m, n, root, 1, 1});
-  /* Leaves are emitted in build order into `primrefs` */
-  std::vector<uint32_t> refs;
-  refs.reserve(n);
-  while(!stack.empty()) {
-    const Task t = stack.back();
-    stack.pop_back();
-    out.depth = std::max(out.depth, t.depth + 1);
-    const Box b = bounds(prims, t.begin, t.end);
-    const int s = split(prims, cent, t.begin, t.end, prm, t.depth);
-    if(s < 0) {
-      const int first = (int)refs.size();
-      for(int i = t.begin; i < t.end; ++i) refs.push_back(prims[i].ref);
-      set_slot(t.node * 2 + t.slot, b, first, t.end - t.begin);
+    for(int i = 0; i < n; ++i) B.refs.push_back(prims[i].ref);
+    B.set_slot(root * 2 + 0, bounds(prims, 0, n), 0, n);
+    B.set_slot(root * 2 + 1, empty, 0, -1);
+    B.depth = 1;
+  } else {
+    std::vector<Task> stack = {{0, m, root, 0, 1}, {m, n, root, 1, 1}};
+    const int threads = std::max(1, prm.threads);
+    if(threads == 1 || n < 4096) {
+      run_tasks(prims, cent, prm, B, stack, 0, nullptr);
     } else {
-      const int id = new_node();
-      set_slot(t.node * 2 + t.slot, b, id, 0);
-      stack.push_back({t.begin, s, id, 0, t.depth + 1});
-      stack.push_back({s, t.end, id, 1, t.depth + 1});
+      /* Top levels here, then the subtrees below n / (4 x threads)
+       * primitives on the threads, each into its own builder whose node 0
+       * stands for the parent slot; the splits are the same, so is the tree */
+      std::vector<Task> deferred;
+      run_tasks(prims, cent, prm, B, stack, std::max(512, n / (4 * threads)), &deferred);
+      std::vector<Builder> sub(deferred.size());
+      std::atomic<size_t> next{0};
+      auto work = [&]() {
+        for(size_t i = next.fetch_add(1); i < deferred.size(); i = next.fetch_add(1)) {
+          Builder& L = sub[i];
+          L.new_node();
+          Task t = deferred[i];
+          t.node = 0;
+          t.slot = 0;
+          run_tasks(prims, cent, prm, L, {t}, 0, nullptr);
+        }
+      };
+      std::vector<std::thread> pool;
+      const size_t nt = std::min<size_t>((size_t)threads, deferred.size());
+      for(size_t k = 1; k < nt; ++k) pool.emplace_back(work);
+      work();
+      for(std::thread& th : pool) th.join();
+      /* Merge in the order the tasks were deferred: local node j > 0 becomes
+       * base + j - 1, local leaf refs move by the refs already merged */
+      for(size_t i = 0; i < deferred.size(); ++i) {
+        const Builder& L = sub[i];
+        const int base = (int)(B.child.size() / 2);
+        const int ref_base = (int)B.refs.size();
+        const int nl = (int)(L.child.size() / 2);
+        auto fix = [&](int c, int cnt) { return cnt == 0 ? c - 1 + base : cnt > 0 ? c + ref_base : c; };
+        for(int j = 1; j < nl; ++j) {
+          const int id = B.new_node();
+          for(int k = 0; k < 2; ++k) {
+            const size_t ls = (size_t)j * 2 + k, gs = (size_t)id * 2 + k;
+            for(int c = 0; c < 3; ++c) {
+              B.lo[gs * 3 + c] = L.lo[ls * 3 + c];
+              B.hi[gs * 3 + c] = L.hi[ls * 3 + c];
+            }
+            B.count[gs] = L.count[ls];
+            B.child[gs] = fix(L.child[ls], L.count[ls]);
+          }
+        }
+        const Task& t = deferred[i];
+        const size_t ps = (size_t)t.node * 2 + t.slot;
+        for(int c = 0; c < 3; ++c) {
+          B.lo[ps * 3 + c] = L.lo[c];
+          B.hi[ps * 3 + c] = L.hi[c];
+        }
+        B.count[ps] = L.count[0];
+        B.child[ps] = fix(L.child[0], L.count[0]);
+        B.refs.insert(B.refs.end(), L.refs.begin(), L.refs.end());
+        B.depth = std::max(B.depth, L.depth);
+      }
     }
   }
-  out.primrefs = std::move(refs);
+  out.lo = std::move(B.lo);
+  out.hi = std::move(B.hi);
+  out.child = std::move(B.child);
+  out.count = std::move(B.count);
+  out.primrefs = std::move(B.refs);
+  out.depth = B.depth;
 }
 
 template<class R> static R round_down(double x)

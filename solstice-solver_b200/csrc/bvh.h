@@ -22,6 +22,7 @@ struct BvhBuildParams {
   int max_leaf = 4; /* primitives per leaf */
   int bins = 16; /* SAH bins per axis */
   int max_depth = 30; /* the device traversal stack holds 32 entries */
+  int threads = 1; /* host threads for the subtrees of large scenes */
 };
 
 struct BvhResult {

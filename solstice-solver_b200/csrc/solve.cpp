@@ -50,6 +50,13 @@ static res_T device_bind(ssol_device* dev)
   return RES_OK;
 }
 
+/* Host threads for the work of one scene (its BVH subtrees) */
+static int host_threads()
+{
+  const unsigned hw = std::thread::hardware_concurrency();
+  return (int)std::min(16u, std::max(1u, hw));
+}
+
 /* Runs f(0..n-1) on the host's hardware threads (the calling thread
  * included); used for per-item host work of batches */
 template<class F> static void parallel_for(size_t n, F&& f)
@@ -602,6 +609,7 @@ res_T ssolb_snapshot_create
   if(opt.bvh_leaf_size < 0) return RES_BAD_ARG;
   BvhBuildParams bp;
   bp.max_leaf = opt.bvh_leaf_size ? opt.bvh_leaf_size : 1;
+  bp.threads = host_threads();
   out.precision = opt.precision;
   std::unique_ptr<FlatScene<float>> f32;
   std::unique_ptr<FlatScene<double>> f64;
@@ -678,6 +686,7 @@ extern "C" res_T ssol_b200_plan_create
 
   BvhBuildParams bp;
   bp.max_leaf = opt.bvh_leaf_size;
+  bp.threads = host_threads();
 
   /* Snapshot on the host first: argument errors need no GPU */
   std::unique_ptr<FlatScene<float>> f32;
