@@ -146,6 +146,10 @@ template<typename R> struct alignas(16) DQuadric {
   R w2l[12]; /* world -> local: rows 0..2 of a 3x4 affine map (row major) */
   R l2w[12]; /* local -> world, same layout */
   R param[4]; /* kind specific constants, see quadric_eval in kernels */
+  /* The same surface as an axis-aligned quadric in local coordinates,
+   * F = kx x^2 + ky y^2 + kz (z - z0)^2 + lz z + m = 0, in FP64:
+   * {kx, ky, kz, z0, lz, m, s, 0}; the front normal is s grad F */
+  double gen[8];
   R carve_lo[2], carve_hi[2]; /* AABB of the AND carvings (local xy) */
   R grid_delta; /* cell size of the RT tessellation grid */
   int32_t type;

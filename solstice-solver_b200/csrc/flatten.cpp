@@ -330,6 +330,28 @@ bool material_varies(ssol_material* m, const ssol_surface_fragment* f, int nf,
   return false;
 }
 
+/* The patch's surface as F = kx x^2 + ky y^2 + kz (z - z0)^2 + lz z + m
+ * over its (rounded) kind constants, with the sign that turns grad F into
+ * the front normal of src/ssol_shape.c:236-285 (DQuadric::gen) */
+template<class R>
+static void quadric_general(DQuadric<R>& q)
+{
+  const double p0 = (double)q.param[0], p1 = (double)q.param[1], p3 = (double)q.param[3];
+  double* g = q.gen;
+  for(int k = 0; k < 8; ++k) g[k] = 0;
+  switch(q.type) {
+    case QUAD_PLANE: g[4] = 1; g[6] = 1; break;
+    case QUAD_PARABOL: g[0] = g[1] = 1; g[4] = -4 * p0; g[6] = -1; break;
+    case QUAD_PARABOL2F: g[0] = p0; g[1] = p1; g[4] = -1; g[6] = -1; break;
+    case QUAD_HYPERBOL:
+      g[0] = g[1] = p1 * p1 * p3; g[2] = -1; g[3] = -p1; g[5] = p1 * p1; g[6] = 1;
+      break;
+    case QUAD_PCYLINDER: g[1] = 1; g[4] = -4 * p0; g[6] = -1; break;
+    case QUAD_HEMISPHERE: g[0] = g[1] = g[2] = 1; g[3] = p0; g[5] = -p1; g[6] = -1; break;
+    default: g[4] = 1; g[6] = 1; break;
+  }
+}
+
 /* Quadric patch bounds: local z range over the carving AABB */
 void quadric_z_range(const ssol_shape* s, double& zlo, double& zhi)
 {
@@ -669,6 +691,8 @@ static res_T flatten_impl
         for(int c = 0; c < 4; ++c) q.param[c] = (R)shape->qparam[c];
         if(shape->quadric.type == SSOL_QUADRIC_HEMISPHERE)
           q.param[2] = (R)(shape->hemi_radius * shape->hemi_radius);
+        q.type = shape->quadric.type;
+        quadric_general(q);
         q.carve_lo[0] = (R)shape->carve_lo[0];
         q.carve_lo[1] = (R)shape->carve_lo[1];
         q.carve_hi[0] = (R)shape->carve_hi[0];

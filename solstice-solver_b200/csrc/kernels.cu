@@ -328,53 +328,6 @@ __device__ __forceinline__ V3<R> quadric_grad(int type, const R* q, V3<R> p)
   }
 }
 
-/* Coefficients of a t^2 + b t + c = 0 for the local ray o + t d */
-template<class T>
-__device__ __forceinline__ void quadric_coefs
-  (int type, const T* q, T ox, T oy, T oz, T dx, T dy, T dz,
-   T& a, T& b, T& c)
-{
-  switch(type) {
-    case QUAD_PLANE: a = T(0); b = dz; c = oz; break;
-    case QUAD_PARABOL: {
-      const T f4 = T(4) * q[0];
-      a = dx * dx + dy * dy;
-      b = T(2) * (ox * dx + oy * dy) - f4 * dz;
-      c = ox * ox + oy * oy - f4 * oz;
-      break;
-    }
-    case QUAD_PARABOL2F:
-      a = dx * dx * q[0] + dy * dy * q[1];
-      b = T(2) * (ox * dx * q[0] + oy * dy * q[1]) - dz;
-      c = ox * ox * q[0] + oy * oy * q[1] - oz;
-      break;
-    case QUAD_HYPERBOL: {
-      const T b2 = q[1] * q[1];
-      const T b2a2 = b2 * q[3];
-      const T zz = oz + q[1];
-      a = b2a2 * (dx * dx + dy * dy) - dz * dz;
-      b = T(2) * (b2a2 * (ox * dx + oy * dy) - zz * dz);
-      c = b2a2 * (ox * ox + oy * oy) + b2 - zz * zz;
-      break;
-    }
-    case QUAD_PCYLINDER: {
-      const T f4 = T(4) * q[0];
-      a = dy * dy;
-      b = T(2) * oy * dy - f4 * dz;
-      c = oy * oy - f4 * oz;
-      break;
-    }
-    case QUAD_HEMISPHERE: {
-      const T z0 = -q[0];
-      a = dx * dx + dy * dy + dz * dz;
-      b = T(2) * (ox * dx + oy * dy + oz * dz + z0 * dz);
-      c = ox * ox + oy * oy + oz * oz - q[1] + T(2) * z0 * oz + z0 * z0;
-      break;
-    }
-    default: a = b = c = T(0); break;
-  }
-}
-
 /* Roots in ascending order; stable form of src/ssol_shape.c:864-896 */
 template<class R>
 __device__ __forceinline__ int solve_quadratic(R a, R b, R c, R t[2])
@@ -395,22 +348,23 @@ __device__ __forceinline__ int solve_quadratic(R a, R b, R c, R t[2])
   return 2;
 }
 
-/* One FP64 Newton step on the root of the FP32 solve */
-__device__ __forceinline__ float refine_root
-  (int type, const float* q, float ox, float oy, float oz,
-   float dx, float dy, float dz, float t)
+/* One FP64 Newton step of F(o + t d) on the FP32 root, general form */
+__device__ __forceinline__ float refine_root_general
+  (const double* g, V3<float> o, V3<float> d, float t)
 {
-  double qd[4] = {q[0], q[1], q[2], q[3]};
-  double a, b, c;
-  quadric_coefs<double>(type, qd, ox, oy, oz, dx, dy, dz, a, b, c);
+  const double ox = o.x, oy = o.y, dx = d.x, dy = d.y, dz = d.z;
+  const double zz = (double)o.z - g[3];
+  const double a = g[0] * dx * dx + g[1] * dy * dy + g[2] * dz * dz;
+  const double b = 2.0 * (g[0] * ox * dx + g[1] * oy * dy + g[2] * zz * dz) + g[4] * dz;
+  const double c = g[0] * ox * ox + g[1] * oy * oy + g[2] * zz * zz + g[4] * (double)o.z
+                 + g[5];
   const double td = t;
   const double f = (a * td + b) * td + c;
   const double df = 2.0 * a * td + b;
   return df != 0.0 ? (float)(td - f / df) : t;
 }
-__device__ __forceinline__ double refine_root
-  (int, const double*, double, double, double, double, double, double,
-   double t)
+__device__ __forceinline__ double refine_root_general
+  (const double*, V3<double>, V3<double>, double t)
 { return t; }
 
 template<class R>
@@ -583,22 +537,27 @@ __device__ __forceinline__ void test_quadric
   const DQuadric<R>& Q = S.quads[idx];
   const V3<R> ol = xform_point(Q.w2l, o);
   const V3<R> dl = xform_vec(Q.w2l, d);
-  R a, b, c;
-  quadric_coefs<R>(Q.type, Q.param, ol.x, ol.y, ol.z, dl.x, dl.y, dl.z,
-                   a, b, c);
+  /* One code path for every kind: the general form of DQuadric::gen */
+  const R kx = (R)Q.gen[0], ky = (R)Q.gen[1], kz = (R)Q.gen[2], z0 = (R)Q.gen[3];
+  const R lz = (R)Q.gen[4], m = (R)Q.gen[5];
+  const R zz = ol.z - z0;
+  const R a = kx * dl.x * dl.x + ky * dl.y * dl.y + kz * dl.z * dl.z;
+  const R b = R(2) * (kx * ol.x * dl.x + ky * ol.y * dl.y + kz * zz * dl.z) + lz * dl.z;
+  const R c = kx * ol.x * ol.x + ky * ol.y * ol.y + kz * zz * zz + lz * ol.z + m;
   R roots[2];
   const int n = solve_quadratic(a, b, c, roots);
   for(int k = 0; k < n; ++k) {
-    const R t = refine_root(Q.type, Q.param, ol.x, ol.y, ol.z,
-                            dl.x, dl.y, dl.z, roots[k]);
+    const R t = refine_root_general(Q.gen, ol, dl, roots[k]);
     if(t <= tmin) continue;
     if(!(t < best.t)) break;
     const V3<R> pl = ol + dl * t;
     if(Q.type == QUAD_HYPERBOL && !(pl.z + Q.param[1] > R(0))) continue;
     if(Q.type == QUAD_HEMISPHERE && pl.z > Q.param[0]) continue;
     if(!in_carvings(S, Q, pl.x, pl.y)) continue;
-    const V3<R> nw = normalize(xform_normal(Q.w2l, quadric_grad(Q.type,
-                                                                 Q.param, pl)));
+    const R sg = (R)Q.gen[6];
+    const V3<R> grad = mk(sg * R(2) * kx * pl.x, sg * R(2) * ky * pl.y,
+                          sg * (R(2) * kz * (pl.z - z0) + lz));
+    const V3<R> nw = normalize(xform_normal(Q.w2l, grad));
     const int side = dot(d, nw) < R(0) ? 1 : 2;
     if(Q.sinst == self.sinst && side != self.side) continue;
     if(!side_passes(S, Q.sinst, side, self)) continue;
