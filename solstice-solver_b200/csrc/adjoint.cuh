@@ -145,8 +145,8 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
     if(si.is_punched) {
       const DQuadric<R>& Q = S.quads[si.quadric];
       V3<R> pl = xform_point(Q.w2l, pos);
-      pl.z = quadric_z(Q.type, Q.param, pl.x, pl.y);
-      N = normalize(xform_normal(Q.w2l, quadric_grad(Q.type, Q.param, pl)));
+      pl.z = quadric_general_z(Q, pl.x, pl.y);
+      N = normalize(xform_normal(Q.w2l, quadric_general_normal(Q, pl)));
       pos = xform_point(Q.l2w, pl);
     }
     int side = 1;

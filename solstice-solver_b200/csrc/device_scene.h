@@ -148,7 +148,8 @@ template<typename R> struct alignas(16) DQuadric {
   R param[4]; /* kind specific constants, see quadric_eval in kernels */
   /* The same surface as an axis-aligned quadric in local coordinates,
    * F = kx x^2 + ky y^2 + kz (z - z0)^2 + lz z + m = 0, in FP64:
-   * {kx, ky, kz, z0, lz, m, s, 0}; the front normal is s grad F */
+   * {kx, ky, kz, z0, lz, m, s, h}; the front normal is s grad F, and the
+   * surface's height above (x, y) is the root z0 + h sqrt(...) when kz != 0 */
   double gen[8];
   R carve_lo[2], carve_hi[2]; /* AABB of the AND carvings (local xy) */
   R grid_delta; /* cell size of the RT tessellation grid */

@@ -332,7 +332,8 @@ bool material_varies(ssol_material* m, const ssol_surface_fragment* f, int nf,
 
 /* The patch's surface as F = kx x^2 + ky y^2 + kz (z - z0)^2 + lz z + m
  * over its (rounded) kind constants, with the sign that turns grad F into
- * the front normal of src/ssol_shape.c:236-285 (DQuadric::gen) */
+ * the front normal of src/ssol_shape.c:236-285 and the side of z0 its
+ * height is taken on (DQuadric::gen) */
 template<class R>
 static void quadric_general(DQuadric<R>& q)
 {
@@ -345,9 +346,13 @@ static void quadric_general(DQuadric<R>& q)
     case QUAD_PARABOL2F: g[0] = p0; g[1] = p1; g[4] = -1; g[6] = -1; break;
     case QUAD_HYPERBOL:
       g[0] = g[1] = p1 * p1 * p3; g[2] = -1; g[3] = -p1; g[5] = p1 * p1; g[6] = 1;
+      g[7] = 1; /* upper sheet */
       break;
     case QUAD_PCYLINDER: g[1] = 1; g[4] = -4 * p0; g[6] = -1; break;
-    case QUAD_HEMISPHERE: g[0] = g[1] = g[2] = 1; g[3] = p0; g[5] = -p1; g[6] = -1; break;
+    case QUAD_HEMISPHERE:
+      g[0] = g[1] = g[2] = 1; g[3] = p0; g[5] = -p1; g[6] = -1;
+      g[7] = -1; /* the half below the centre */
+      break;
     default: g[4] = 1; g[6] = 1; break;
   }
 }

@@ -297,35 +297,27 @@ __device__ __forceinline__ V3<R> xform_normal(const R* W, V3<R> n)
             W[2] * n.x + W[6] * n.y + W[10] * n.z);
 }
 
+/* Front normal (local frame, unnormalised) at pl of the general form in
+ * DQuadric::gen */
 template<class R>
-__device__ __forceinline__ R quadric_z(int type, const R* q, R x, R y)
+__device__ __forceinline__ V3<R> quadric_general_normal(const DQuadric<R>& Q, V3<R> pl)
 {
-  switch(type) {
-    case QUAD_PARABOL: return (x * x + y * y) * q[1];
-    case QUAD_PARABOL2F: return x * x * q[0] + y * y * q[1];
-    case QUAD_HYPERBOL:
-      return q[1] * sq_rt(R(1) + (x * x + y * y) * q[3]) - q[1];
-    case QUAD_PCYLINDER: return y * y * q[1];
-    case QUAD_HEMISPHERE: {
-      const R z2 = q[1] - (x * x + y * y);
-      return z2 > R(0) ? q[0] - sq_rt(z2) : q[0];
-    }
-    default: return R(0);
-  }
+  const R sg = (R)Q.gen[6];
+  return mk(sg * R(2) * (R)Q.gen[0] * pl.x, sg * R(2) * (R)Q.gen[1] * pl.y,
+            sg * (R(2) * (R)Q.gen[2] * (pl.z - (R)Q.gen[3]) + (R)Q.gen[4]));
 }
 
+/* Height of the surface above local (x, y): the linear case, or the
+ * root on the side gen[7] of z0 (upper sheet of the hyperboloid, lower
+ * hemisphere); src/ssol_shape.c:236-285 */
 template<class R>
-__device__ __forceinline__ V3<R> quadric_grad(int type, const R* q, V3<R> p)
+__device__ __forceinline__ R quadric_general_z(const DQuadric<R>& Q, R x, R y)
 {
-  switch(type) {
-    case QUAD_PARABOL: return mk(-p.x, -p.y, R(2) * q[0]);
-    case QUAD_PARABOL2F:
-      return mk(-p.x * (R(4) * q[0]), -p.y * (R(4) * q[1]), R(2));
-    case QUAD_HYPERBOL: return mk(p.x, p.y, -(p.z + q[1]) * q[2]);
-    case QUAD_PCYLINDER: return mk(R(0), -p.y, R(2) * q[0]);
-    case QUAD_HEMISPHERE: return mk(-p.x, -p.y, q[0] - p.z);
-    default: return mk(R(0), R(0), R(1));
-  }
+  const R kz = (R)Q.gen[2];
+  const R rest = (R)Q.gen[0] * x * x + (R)Q.gen[1] * y * y + (R)Q.gen[5];
+  if(kz == R(0)) return -rest / (R)Q.gen[4];
+  const R w = -rest / kz;
+  return (R)Q.gen[3] + (R)Q.gen[7] * sq_rt(w > R(0) ? w : R(0));
 }
 
 /* Roots in ascending order; stable form of src/ssol_shape.c:864-896 */
@@ -554,10 +546,7 @@ __device__ __forceinline__ void test_quadric
     if(Q.type == QUAD_HYPERBOL && !(pl.z + Q.param[1] > R(0))) continue;
     if(Q.type == QUAD_HEMISPHERE && pl.z > Q.param[0]) continue;
     if(!in_carvings(S, Q, pl.x, pl.y)) continue;
-    const R sg = (R)Q.gen[6];
-    const V3<R> grad = mk(sg * R(2) * kx * pl.x, sg * R(2) * ky * pl.y,
-                          sg * (R(2) * kz * (pl.z - z0) + lz));
-    const V3<R> nw = normalize(xform_normal(Q.w2l, grad));
+    const V3<R> nw = normalize(xform_normal(Q.w2l, quadric_general_normal(Q, pl)));
     const int side = dot(d, nw) < R(0) ? 1 : 2;
     if(Q.sinst == self.sinst && side != self.side) continue;
     if(!side_passes(S, Q.sinst, side, self)) continue;
@@ -972,8 +961,8 @@ __device__ __forceinline__ void init_path
     /* punched_shape_project_point (src/ssol_shape.c:1408-1447) */
     const DQuadric<R>& Q = S.quads[si.quadric];
     V3<R> pl = xform_point(Q.w2l, pos);
-    pl.z = quadric_z(Q.type, Q.param, pl.x, pl.y);
-    N = normalize(xform_normal(Q.w2l, quadric_grad(Q.type, Q.param, pl)));
+    pl.z = quadric_general_z(Q, pl.x, pl.y);
+    N = normalize(xform_normal(Q.w2l, quadric_general_normal(Q, pl)));
     pos = xform_point(Q.l2w, pl);
   }
   int side = 1;
