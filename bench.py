@@ -39,8 +39,8 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 # DRAM bytes per path of the realisation kernel, from ncu captures of 4e6-path
 # launches of the same scenes (dram__bytes_read.sum + dram__bytes_write.sum);
 # the traffic scales with the paths traced (per-thread frames written back)
-DRAM_BYTES_PER_PATH = {"field": (43.4e6 + 1600.3e6) / 4e6,
-                       "beamdown": (39.5e6 + 268.0e6) / 4e6}
+DRAM_BYTES_PER_PATH = {"field": (31.6e6 + 1104.8e6) / 4e6,
+                       "beamdown": (73.9e6 + 387.0e6) / 4e6}
 
 
 def flops_per_run(st):
