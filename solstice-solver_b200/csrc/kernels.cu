@@ -1468,9 +1468,19 @@ batch_kernel
     reinterpret_cast<int*>(smem + (2 * NGLOBAL + PS_COUNT) * bd) + SMEM_STACK * bd)
     + (size_t)(tid >> 5) * 2 * ss;
   for(int i = (int)lane; i < 2 * ss; i += 32) wslots[i] = 0;
+  /* Copies of the two tagged items' scene records, so that lanes on those
+   * items read their scene from shared memory instead of device memory */
+  DScene<R>* wscene = reinterpret_cast<DScene<R>*>(
+    reinterpret_cast<double*>(reinterpret_cast<int*>(smem + (2 * NGLOBAL + PS_COUNT) * bd)
+                              + SMEM_STACK * bd) + (size_t)(bd >> 5) * 2 * ss)
+    + (size_t)(tid >> 5) * 2;
   __syncwarp();
   int stag[2] = {-1, -1};
   int cur = 0;
+  auto scene_of = [&](int item) -> const DScene<R>& {
+    return item == stag[cur] ? wscene[cur] : item == stag[cur ^ 1] ? wscene[cur ^ 1]
+                                                                   : scenes[item];
+  };
 
   const unsigned long long count = prefix[nitems];
   Rng rng;
@@ -1542,7 +1552,7 @@ batch_kernel
           const uint64_t id = firsts[it] + (g - prefix[it]);
           rng.i_lo = (uint32_t)id;
           rng.i_hi = (uint32_t)(id >> 32);
-          init_path(scenes[it], rng, p, ps, bd);
+          init_path(scene_of(it), rng, p, ps, bd);
           ++npaths;
         }
       }
@@ -1561,6 +1571,12 @@ batch_kernel
             for(int i = (int)lane; i < nd; i += 32) red_add(dst + i, sl[2 * NGLOBAL + i]);
           }
           for(int i = (int)lane; i < ss; i += 32) sl[i] = 0;
+          {
+            const int* src = reinterpret_cast<const int*>(scenes + newest);
+            int* dst = reinterpret_cast<int*>(wscene + prv);
+            constexpr int words = (int)(sizeof(DScene<R>) / sizeof(int));
+            for(int i = (int)lane; i < words; i += 32) dst[i] = src[i];
+          }
           __syncwarp();
           stag[prv] = newest;
           cur = prv;
@@ -1569,7 +1585,7 @@ batch_kernel
     }
     if(!__any_sync(0xffffffffu, p.phase != PH_NONE)) break;
 
-    const DScene<R>& S = scenes[it];
+    const DScene<R>& S = scene_of(it);
     Hit<R> h;
     bool found = false;
     if(p.phase != PH_NONE) {
@@ -1749,7 +1765,8 @@ static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg
   if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
   const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block) * sizeof(double)
                     + (size_t)SMEM_STACK * block * sizeof(int)
-                    + (size_t)(block / 32) * 2 * (2 * NGLOBAL + cfg.rcv_doubles) * sizeof(double);
+                    + (size_t)(block / 32) * 2 * (2 * NGLOBAL + cfg.rcv_doubles) * sizeof(double)
+                    + (size_t)(block / 32) * 2 * sizeof(DScene<R>);
   static bool attr_set = false;
   if(!attr_set) {
     cudaFuncSetAttribute(batch_kernel<R, MINB>,
@@ -1841,7 +1858,8 @@ static int launch_batch_noalloc_variant
   if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
   const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block) * sizeof(double)
                     + (size_t)SMEM_STACK * block * sizeof(int)
-                    + (size_t)(block / 32) * 2 * (2 * NGLOBAL + cfg.rcv_doubles) * sizeof(double);
+                    + (size_t)(block / 32) * 2 * (2 * NGLOBAL + cfg.rcv_doubles) * sizeof(double)
+                    + (size_t)(block / 32) * 2 * sizeof(DScene<R>);
   cudaFuncSetAttribute(batch_kernel<R, MINB>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
   int per_sm = 0;
