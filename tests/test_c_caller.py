@@ -80,7 +80,8 @@ def test_c_caller_on_b200(tmp_path, product, oracle):
     """The C program linked against the B200 library: the same numbers as the
     Python binding on the same library and seed (the same Philox stream;
     only the order of the FP64 atomic adds may differ, hence 1e-9), and
-    within 4 standard errors of the oracle on its own seed."""
+    within 4 standard errors (plus 1e-5 relative for the FP32 geometry) of
+    the oracle on its own seed."""
     exe = _compile(_ensure_product(), str(tmp_path / "solve_mirror_b200"))
     n, seed = 2_000_000, 7
     c_out = _run(exe, n, seed)
@@ -94,6 +95,7 @@ def test_c_caller_on_b200(tmp_path, product, oracle):
     for k in GLOBALS + RECEIVER:
         e_c, se_c = c_out[k]
         e_o, se_o = ref[k]
-        tol = 4 * (se_c ** 2 + se_o ** 2) ** 0.5 + 1e-9 * abs(e_o)
+        # FP32 geometry: 1e-5 relative on top of the statistical bound
+        tol = 4 * (se_c ** 2 + se_o ** 2) ** 0.5 + 1e-5 * abs(e_o)
         assert abs(e_c - e_o) <= tol, (k, e_c, e_o, tol)
     assert c_out["incoming_flux"][0] > 0
