@@ -537,28 +537,7 @@ template<class R>
 static res_T upload(ssol_b200_plan* p, const FlatScene<R>& f, DScene<R>& S)
 {
   Blob b;
-  b.add(f.nodes);
-  b.add(f.bvh.primrefs);
-  b.add(f.tris);
-  b.add(f.quads);
-  b.add(f.carvings);
-  b.add(f.carve_verts);
-  b.add(f.sinsts);
-  b.add(f.mtls);
-  b.add(f.media);
-  b.add(f.spectra);
-  b.add(f.spec_wl);
-  b.add(f.spec_val);
-  b.add(f.shader_tab);
-  b.add(f.shader_wl);
-  b.add(f.samp);
-  b.add(f.alias_prob);
-  b.add(f.alias_idx);
-  b.add(f.wl_nodes);
-  b.add(f.wl_pdf);
-  b.add(f.wl_cdf);
-  b.add(f.tshade);
-  b.add(f.bake_tab);
+  add_scene(b, f);
   const size_t bytes = b.host.size() + 256;
   if(dev_alloc(p->dev, &p->d_scene, bytes) != cudaSuccess) return RES_MEM_ERR;
   p->scene_alloc = bytes;

@@ -90,7 +90,9 @@ def test_c_caller_on_b200(tmp_path, product, oracle):
         e_c, se_c = c_out[k]
         e_p, se_p = py_out[k]
         assert e_c == pytest.approx(e_p, rel=1e-9, abs=1e-12), k
-        assert se_c == pytest.approx(se_p, rel=1e-6, abs=1e-12), k
+        # the SE of a quantity that is the same on every path (cos_factor
+        # here) is rounding noise of sum(w^2)/N - (sum(w)/N)^2
+        assert se_c == pytest.approx(se_p, rel=1e-6, abs=1e-7 * abs(e_p) + 1e-12), k
     ref = _python(oracle, 200_000, 11)
     for k in GLOBALS + RECEIVER:
         e_c, se_c = c_out[k]
