@@ -443,7 +443,12 @@ def run_suns(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     lib = P.load_product()
-    suns = shard_suns(W.sun_grid(), rank, world)
+    grid = W.sun_grid()
+    if args.suns:
+        # evenly spaced subset of the 256 suns (small cases, profiling)
+        step = max(1, len(grid) // args.suns)
+        grid = grid[::step][:args.suns]
+    suns = shard_suns(grid, rank, world)
     built = W.batched_fields(lib, suns, n_helio=args.heliostats)
     scenes = [b[0] for b in built]
     rcv = [b[1]["receiver"] for b in built]
@@ -963,6 +968,8 @@ def main():
     p.add_argument("--fd-params", type=int, default=32)
     p.add_argument("--fd-paths", type=int, default=100_000_000)
     p.add_argument("--heliostats", type=int, default=1000)
+    p.add_argument("--suns", type=int, default=0,
+                   help="suns config: evenly spaced subset of this many suns (0: all 256)")
     p.add_argument("--paths", type=int, default=None,
                    help="realisations per step (field 1e8, beamdown 2e8, mirror 1e6)")
     p.add_argument("--seed", type=int, default=0)
