@@ -41,6 +41,8 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 # the traffic scales with the paths traced (per-thread frames written back)
 DRAM_BYTES_PER_PATH = {"field": (31.6e6 + 1104.8e6) / 4e6,
                        "beamdown": (73.9e6 + 387.0e6) / 4e6}
+# Same for the batched kernel, from a capture of 16 suns (7104261 paths)
+BATCH_DRAM_BYTES_PER_PATH = (70.3e6 + 1878.6e6) / 7104261
 
 
 def flops_per_run(st):
@@ -657,7 +659,10 @@ def run_suns(args):
                 "timing": "wall clock: batch create + launch + finish per step"},
         "gpu_launches": args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                     "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "traffic": BATCH_DRAM_BYTES_PER_PATH * n_total,
+                     "traffic_source": "ncu dram__bytes_read+write of the batched kernel on "
+                                       "16 suns (7.1e6 paths), scaled to this rank's paths per launch",
                      "work_model": "as the field line"},
         "clocks": clk,
     }
