@@ -676,8 +676,10 @@ def run_suns(args):
 
 
 ADJOINT = ("aim gradients (ssol_solve_adjoint) on the 1000-heliostat field: 2000 aim "
-           "angles (2 per heliostat), objectives first-bounce absorbed power and spillage "
+           "angles (2 per heliostat), initial aim offsets uniform in +-2 mrad (seeded), "
+           "objectives first-bounce absorbed power and spillage "
            "sum_c (map - uniform target)^2 on a 64x64 map of the 12x12 receiver")
+AIM_OFFSET = 2e-3  # rad, half-width of the seeded initial aim offsets
 
 
 def run_adjoint(args):
@@ -699,6 +701,18 @@ def run_adjoint(args):
     s, h = W.heliostat_field(lib, n_helio=args.heliostats)
     lower, upper, nx, ny = (-6.0, -6.0), (6.0, 6.0), 64, 64
     n = args.paths
+    # initial aim offsets: every heliostat turned by seeded uniform angles in
+    # +-AIM_OFFSET about its two local axes; gradients and finite differences
+    # are taken about this configuration
+    aims = A.AimField(s, h["heliostats"], h["transforms"], h["receiver"], lower, upper,
+                      nx, ny, 0.0, n)
+    rnd0 = random.Random(args.seed + 5)
+    transforms = []
+    for i in range(len(h["heliostats"])):
+        xf = aims.offset_transform(i, rnd0.uniform(-AIM_OFFSET, AIM_OFFSET),
+                                   rnd0.uniform(-AIM_OFFSET, AIM_OFFSET))
+        lib.call("ssol_instance_set_transform", h["heliostats"][i], P._transform(xf))
+        transforms.append(xf)
     opt = P.options(P.FP64 if args.fp64 else P.FP32)
     base = A.solve_adjoint(s, h["heliostats"], h["receiver"], lower, upper, nx, ny, 0.0,
                            n, seed=args.seed, options=opt, want_map=True)
@@ -720,7 +734,7 @@ def run_adjoint(args):
 
     fd = {}
     if args.fd_params > 0:
-        field = A.AimField(s, h["heliostats"], h["transforms"], h["receiver"], lower, upper,
+        field = A.AimField(s, h["heliostats"], transforms, h["receiver"], lower, upper,
                            nx, ny, target, args.fd_paths, seed=args.seed + 7, options=opt)
         rnd = random.Random(args.seed)
         params = [(rnd.randrange(len(h["heliostats"])), rnd.randrange(2))

@@ -109,13 +109,17 @@ class AimField:
         self.seed = seed
         self.options = options
 
-    def set_offset(self, i, theta_x, theta_y):
+    def offset_transform(self, i, theta_x, theta_y):
+        """The 3x4 column-major transform of heliostat i at offsets (theta_x, theta_y)."""
         t = self.base[i]
         R0 = ((t[0], t[3], t[6]), (t[1], t[4], t[7]), (t[2], t[5], t[8]))
         ex = _unit((t[0], t[1], t[2]))
         ey = _unit((t[3], t[4], t[5]))
         R = _mul(_mul(_rot(ex, theta_x), _rot(ey, theta_y)), R0)
-        xf = P.transform_from(R, (t[9], t[10], t[11]))
+        return P.transform_from(R, (t[9], t[10], t[11]))
+
+    def set_offset(self, i, theta_x, theta_y):
+        xf = self.offset_transform(i, theta_x, theta_y)
         self.scene.lib.call("ssol_instance_set_transform", self.helios[i], P._transform(xf))
 
     def reset(self, i):
