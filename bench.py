@@ -41,6 +41,8 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 # the traffic scales with the paths traced (per-thread frames written back)
 DRAM_BYTES_PER_PATH = {"field": (31.6e6 + 1104.8e6) / 4e6,
                        "beamdown": (73.9e6 + 387.0e6) / 4e6}
+# Both passes of the adjoint kernel on the field, from a capture of 4e6 paths
+ADJOINT_DRAM_BYTES_PER_PATH = (1.69e6 + 0.39e6 + 1.86e6 + 0.40e6) / 4e6
 # Same for the batched kernel, from a capture of 16 suns (7104261 paths)
 BATCH_DRAM_BYTES_PER_PATH = (70.3e6 + 1878.6e6) / 7104261
 
@@ -723,13 +725,26 @@ def run_adjoint(args):
     clocks = Clocks(local)
     clocks.start()
     kms, t0 = 0.0, time.perf_counter()
+    cnt = {}
     for k in range(args.steps):
         r = A.solve_adjoint(s, h["heliostats"], h["receiver"], lower, upper, nx, ny, target,
                             n, seed=args.seed + 100 + k, options=opt)
         kms += r["kernel_ms"]
+        for key, v in r["counters"].items():
+            cnt[key] = cnt.get(key, 0) + v
     wall = time.perf_counter() - t0
     clk = clocks.stop()
     value = args.steps * n / (kms * 1e-3) / 1e6
+    # FP32 work model of the field line; each realisation is sampled in both
+    # passes and each unshadowed one casts a reflected ray (rays - samples)
+    passes = 2
+    samples = passes * args.steps * n
+    reflected = max(0, cnt["rays"] - samples)
+    flops = (20 * 2 * cnt["node_visits"] + 55 * cnt["triangle_tests"]
+             + 90 * cnt["quadric_tests"] + 150 * reflected + 120 * samples)
+    achieved = flops / (kms * 1e-3) / 1e12
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
+    fp32_peak = nsm * 128 * 2 * measured_peaks().get("sm_max_mhz", 1965.0) * 1e6 / 1e12
     e2e = args.steps * n / wall / 1e6
 
     fd = {}
@@ -764,6 +779,18 @@ def run_adjoint(args):
                 "d2h_bytes_per_step": (nx * ny + 4 * len(h["heliostats"])) * 8,
                 "timing": "wall clock around the synchronous ssol_solve_adjoint"},
         "gpu_launches": 2 * args.steps,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "traffic": ADJOINT_DRAM_BYTES_PER_PATH * n / passes,
+                     "traffic_source": "ncu dram__bytes_read+write of both passes on 4e6 "
+                                       "paths, scaled to the step's paths, per launch "
+                                       "(mean of the two passes)",
+                     "peak_source": "SMs x 128 FP32 lanes x 2 x measured max SM clock "
+                                    "(MEASURED_PEAKS.json sm_max_mhz)",
+                     "work_model": "20/slab x2 per node + 55/triangle + 90/quadric + "
+                                   "150/reflected ray + 120/sample per pass (counted on "
+                                   "device)",
+                     "counters_per_path": {k: v / (args.steps * n) for k, v in cnt.items()}},
         "objective": {"absorbed_W": base["absorbed"], "spillage": base["spillage"],
                       "target_W_m2": target},
         "fd_check": {"params": args.fd_params, "paths": args.fd_paths,

@@ -135,6 +135,8 @@ struct ssol_b200_adjoint_result {
   double spillage;
   unsigned long long hits; /* first-bounce paths that reached the receiver */
   double kernel_ms; /* both passes */
+  /* device work of both passes */
+  unsigned long long rays, node_visits, triangle_tests, quadric_tests;
 };
 
 /* d_absorbed and d_spillage receive 2 x nheliostats values (theta_x, theta_y

@@ -28,7 +28,9 @@ class AdjointMap(C.Structure):
 class AdjointResult(C.Structure):
     _fields_ = [("absorbed", C.c_double), ("absorbed_se", C.c_double),
                 ("spillage", C.c_double), ("hits", C.c_ulonglong),
-                ("kernel_ms", C.c_double)]
+                ("kernel_ms", C.c_double), ("rays", C.c_ulonglong),
+                ("node_visits", C.c_ulonglong), ("triangle_tests", C.c_ulonglong),
+                ("quadric_tests", C.c_ulonglong)]
 
 
 _SIG = [P.VP, P.VP, C.c_size_t, P.PVP, C.c_size_t, C.POINTER(AdjointMap),
@@ -66,6 +68,8 @@ def solve_adjoint(scene, heliostats, receiver, lower, upper, nx, ny, target, n,
         raise P.SsolError("ssol_solve_adjoint", err)
     out = {"absorbed": res.absorbed, "absorbed_se": res.absorbed_se,
            "spillage": res.spillage, "hits": res.hits, "kernel_ms": res.kernel_ms,
+           "counters": {k: getattr(res, k) for k in ("rays", "node_visits",
+                                                      "triangle_tests", "quadric_tests")},
            "d_absorbed": list(ga[:2 * nh]), "d_spillage": list(gs[:2 * nh])}
     if want_map:
         out["map"] = list(fmap)

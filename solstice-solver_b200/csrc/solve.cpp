@@ -953,6 +953,7 @@ extern "C" res_T ssol_solve_adjoint
   A.map_scale = 1.0 / ((double)n * cw * ch);
 
   std::vector<double> h_map(ncell), h_sums(3);
+  unsigned long long h_cnt[4] = {0, 0, 0, 0};
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   bool ok = cudaMemsetAsync(dbuf, 0, bytes, s) == cudaSuccess
     && cudaMemcpyAsync(d_slot, slot.data(), insts.size() * sizeof(int),
@@ -973,6 +974,7 @@ extern "C" res_T ssol_solve_adjoint
                        cudaMemcpyDeviceToHost, s) == cudaSuccess
     && cudaMemcpyAsync(h_sums.data(), d_sums, 3 * sizeof(double),
                        cudaMemcpyDeviceToHost, s) == cudaSuccess
+    && cudaMemcpyAsync(h_cnt, d_cnt, sizeof(h_cnt), cudaMemcpyDeviceToHost, s) == cudaSuccess
     && (!nh || (cudaMemcpyAsync(d_absorbed, d_gabs, 2 * nh * sizeof(double),
                                 cudaMemcpyDeviceToHost, s) == cudaSuccess
              && cudaMemcpyAsync(d_spillage, d_gspill, 2 * nh * sizeof(double),
@@ -992,6 +994,10 @@ extern "C" res_T ssol_solve_adjoint
   result->absorbed_se = std::sqrt(var / (double)n);
   result->hits = (unsigned long long)h_sums[2];
   result->kernel_ms = ms;
+  result->rays = h_cnt[0];
+  result->node_visits = h_cnt[1];
+  result->triangle_tests = h_cnt[2];
+  result->quadric_tests = h_cnt[3];
   double spill = 0;
   for(size_t c = 0; c < ncell; ++c) {
     const double m = h_map[c] * A.map_scale;

@@ -82,6 +82,11 @@ def test_adjoint_primal_matches_oracle(product, oracle, builder):
     assert max(abs(x - y) for x, y in zip(r["map"], m)) <= 1e-3 * peak
     spill = sum(x * x for x in m)
     assert abs(r["spillage"] - spill) <= 1e-3 * spill
+    # device work of both passes: every sample that reaches the reflection
+    # cast a shadow ray first, and each ray visits at least the root
+    c = r["counters"]
+    assert c["rays"] >= 2 * r["hits"] and c["node_visits"] >= c["rays"]
+    assert c["triangle_tests"] > 0
 
 
 def test_adjoint_matches_finite_differences(product):
