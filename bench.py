@@ -42,7 +42,7 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 DRAM_BYTES_PER_PATH = {"field": (31.6e6 + 1104.8e6) / 4e6,
                        "beamdown": (73.9e6 + 387.0e6) / 4e6}
 # Both passes of the adjoint kernel on the field, from a capture of 4e6 paths
-ADJOINT_DRAM_BYTES_PER_PATH = (1.69e6 + 0.39e6 + 1.86e6 + 0.40e6) / 4e6
+ADJOINT_DRAM_BYTES_PER_PATH = (2.34e6 + 21.63e6 + 6.28e6 + 54.82e6) / 4e6
 # Same for the batched kernel, from a capture of 16 suns (7104261 paths)
 BATCH_DRAM_BYTES_PER_PATH = (70.3e6 + 1878.6e6) / 7104261
 
