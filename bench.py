@@ -39,8 +39,18 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 # DRAM bytes per path of the realisation kernel, from ncu captures of 4e6-path
 # launches of the same scenes (dram__bytes_read.sum + dram__bytes_write.sum);
 # the traffic scales with the paths traced (per-thread frames written back)
-DRAM_BYTES_PER_PATH = {"field": (31.6e6 + 1104.8e6) / 4e6,
-                       "beamdown": (73.9e6 + 387.0e6) / 4e6}
+DRAM_BYTES_PER_PATH = {"field": (110.2e6 + 859.3e6) / 4e6,
+                       "beamdown": (73.9e6 + 387.0e6) / 4e6}  # beam-down: id order
+
+# Kernels of one plain launch of n realisations: below 2^16 the realisation
+# kernel alone; from 2^16 on, per chunk of 2^24 realisations, the coherent
+# order's presort (count, scan, scatter) and the realisation kernel (every
+# bench scene samples fewer than 12288 primitives)
+SORT_MIN, SORT_CHUNK = 1 << 16, 1 << 24
+
+
+def launches_per_plain_launch(n):
+    return 1 if n < SORT_MIN else 4 * ((n + SORT_CHUNK - 1) // SORT_CHUNK)
 # Both passes of the adjoint kernel on the field, from a capture of 4e6 paths
 ADJOINT_DRAM_BYTES_PER_PATH = (2.34e6 + 21.63e6 + 6.28e6 + 54.82e6) / 4e6
 # Same for the batched kernel, from a capture of 16 suns (7104261 paths)
@@ -379,13 +389,16 @@ def run_b200(args):
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
                 "timing": "wall clock around synchronous ssol_solve"},
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * launches_per_plain_launch(n),
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak else None,
                      "traffic": (DRAM_BYTES_PER_PATH[args.config] * n
                                  if args.config in DRAM_BYTES_PER_PATH else None),
-                     "traffic_source": "ncu dram__bytes_read+write of a 4e6-path launch, "
-                                       "scaled to paths_per_step (bytes per launch)",
+                     "traffic_source": "ncu dram__bytes_read+write of a 4e6-path launch of "
+                                       "the realisation kernel, scaled to paths_per_step "
+                                       "(bytes per step: its chunks' launches together)",
+                     "timing": "CUDA events around each step: the realisation kernel and "
+                               "the coherent order's presort (2.5 % of the step)",
                      "peak_source": "SMs x 128 FP32 lanes x 2 x measured max SM clock "
                                     "(MEASURED_PEAKS.json sm_max_mhz)",
                      "work_model": "20/slab x2 per node + 55/triangle + 90/quadric + "

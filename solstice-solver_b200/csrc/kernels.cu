@@ -32,6 +32,9 @@
 #include <float.h>
 #include <math.h>
 
+#include <mutex>
+#include <numeric>
+
 namespace ssolb {
 
 /*******************************************************************************
@@ -933,16 +936,26 @@ template<class R> struct PathState {
   bool overflow;
 };
 
-/* point_init (src/ssol_solver.c:207-352) up to the shadow ray */
+/* Sampled proxy primitive of a primary draw: Vose alias table, bucket =
+ * floor(u * n) computed exactly on the 24-bit integer draw */
 template<class R>
-__device__ __forceinline__ void init_path
-  (const DScene<R>& S, const Rng& rng, PathState<R>& p, double* ps, int stride)
+__device__ __forceinline__ int sample_prim(const DScene<R>& S, const U32x4& r0)
 {
-  const U32x4 r0 = rng.get(0u, RNG_PRIMARY);
-  /* bucket = floor(u * n) computed exactly on the 24-bit integer draw */
   int k = (int)(((unsigned long long)(r0.v[0] >> 8)
                  * (unsigned long long)S.nsamp) >> 24);
   if(!(uni<float>(r0.v[1]) < S.alias_prob[k])) k = S.alias_idx[k];
+  return k;
+}
+
+/* point_init (src/ssol_solver.c:207-352) up to the shadow ray; `draw` is the
+ * realisation's primary draw when the caller already has it */
+template<class R>
+__device__ __forceinline__ void init_path
+  (const DScene<R>& S, const Rng& rng, PathState<R>& p, double* ps, int stride,
+   const U32x4* draw = nullptr)
+{
+  const U32x4 r0 = draw ? *draw : rng.get(0u, RNG_PRIMARY);
+  const int k = sample_prim(S, r0);
   const DSampTri<R> st = S.samp[k];
   const R sa = sq_rt(uni<R>(r0.v[2]));
   const R b2 = sa * uni<R>(r0.v[3]);
@@ -1221,6 +1234,11 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 
 constexpr int SMEM_RCV_MAX = 16;
 constexpr int MAX_BLOCK = 256;
+/* Coherent order (see presort_count) */
+constexpr int SORT_MAX_BINS = 12288; /* shared-memory histogram of primitives */
+constexpr uint64_t SORT_CHUNK = 1ull << 24; /* realisations per sorted chunk */
+constexpr uint64_t SORT_MIN = 1ull << 16; /* smaller launches keep id order */
+constexpr uint32_t SORT_SEG = 256; /* sorted realisations per warp segment */
 
 /* Append one vertex of a tracked path (src/ssol_solver.c:909-922, 1014-1019,
  * 1080-1083: the sun end, the sampled point, every hit and the end at
@@ -1247,7 +1265,8 @@ __global__ void __launch_bounds__(MAX_BLOCK, MINB)
 realisation_kernel
   (const DScene<R> S, const DTallies T, uint64_t seed, uint64_t first,
    uint64_t count, unsigned long long max_segments,
-   unsigned long long* next_path, const DTrack tr)
+   unsigned long long* next_path, const DTrack tr, const uint4* sorted_draw,
+   const uint32_t* sorted_off, uint32_t seg_mul)
 {
   /* Shared memory: per-thread FP64 global sums [12][blockDim], per-thread
    * path sums [10][blockDim], the receiver-side sums, the first traversal
@@ -1281,10 +1300,59 @@ realisation_kernel
   double racc[2 * NRCV_Q];
   int racc_slot = -1;
 
+  /* Coherent order: the warp's current segment [seg_cur, seg_end) of the
+   * sorted realisations */
+  uint32_t seg_cur = 0, seg_end = 0;
+  const uint32_t nseg = (uint32_t)((count + SORT_SEG - 1) / SORT_SEG);
+
   for(;;) {
     /* Regeneration: idle lanes take the next realisations */
     const unsigned need = __ballot_sync(0xffffffffu, p.phase == PH_NONE && !done);
-    if(need) {
+    if(need && sorted_off) {
+      /* Segments of SORT_SEG sorted realisations (one or two primitives) go
+       * to warps whole, in a strided order, so that a warp's lanes start on
+       * the same heliostat while the warps of the GPU spread over the field */
+      const int leader = __ffs(need) - 1;
+      const unsigned rank = __popc(need & ((1u << lane) - 1u));
+      const unsigned c = __popc(need);
+      const unsigned avail = seg_end - seg_cur;
+      uint32_t idx = 0;
+      bool got = rank < avail, exhausted = false;
+      if(got) idx = seg_cur + rank;
+      if(c > avail) {
+        unsigned long long sg = 0;
+        if((int)lane == leader) sg = atomicAdd(next_path, 1ull);
+        sg = __shfl_sync(0xffffffffu, sg, leader);
+        if(sg < nseg) {
+          const uint32_t s0 = (uint32_t)((sg * seg_mul) % nseg) * SORT_SEG;
+          const uint32_t s1 = (uint32_t)min((uint64_t)s0 + SORT_SEG, count);
+          if(!got && rank - avail < s1 - s0) {
+            idx = s0 + (rank - avail);
+            got = true;
+          }
+          seg_cur = s0 + min(c - avail, s1 - s0);
+          seg_end = s1;
+        } else {
+          seg_cur = seg_end;
+          exhausted = true;
+        }
+      } else {
+        seg_cur += c;
+      }
+      if(p.phase == PH_NONE && !done) {
+        if(got) {
+          const uint64_t id = first + sorted_off[idx];
+          const uint4 d = sorted_draw[idx];
+          const U32x4 r0 = {{d.x, d.y, d.z, d.w}};
+          rng.i_lo = (uint32_t)id;
+          rng.i_hi = (uint32_t)(id >> 32);
+          init_path(S, rng, p, ps, bd, &r0);
+          ++npaths;
+        } else if(exhausted) {
+          done = true;
+        }
+      }
+    } else if(need) {
       const int leader = __ffs(need) - 1;
       unsigned long long base = 0;
       if((int)lane == leader)
@@ -1696,8 +1764,112 @@ batch_kernel
 }
 
 /*******************************************************************************
+ * Coherent order. The realisations of a launch, chunk by chunk, are sorted by
+ * the primitive their primary draw samples (a counting sort), so that the
+ * lanes of a warp start on the same or neighbouring heliostats and trace
+ * nearly parallel shadow and reflected rays. Every realisation is traced once
+ * with its own stream; only the order, and so the order of the FP64 sums,
+ * changes. The primary draw travels with the sorted offset so that init_path
+ * does not draw it again.
+ ******************************************************************************/
+
+/* Primary draw and sampled primitive of realisation first + j; histogram of
+ * the primitives, per block in shared memory */
+template<class R>
+__global__ void __launch_bounds__(256) presort_count
+  (const DScene<R> S, uint64_t seed, uint64_t first, uint32_t n, uint32_t* keys,
+   uint4* draws, uint32_t* hist)
+{
+  __shared__ uint32_t h[SORT_MAX_BINS];
+  for(int i = threadIdx.x; i < S.nsamp; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  Rng rng;
+  rng.k0 = (uint32_t)seed;
+  rng.k1 = (uint32_t)(seed >> 32);
+  for(uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n;
+      j += gridDim.x * blockDim.x) {
+    const uint64_t id = first + j;
+    rng.i_lo = (uint32_t)id;
+    rng.i_hi = (uint32_t)(id >> 32);
+    const U32x4 r0 = rng.get(0u, RNG_PRIMARY);
+    const int k = sample_prim(S, r0);
+    keys[j] = (uint32_t)k;
+    draws[j] = make_uint4(r0.v[0], r0.v[1], r0.v[2], r0.v[3]);
+    atomicAdd(&h[k], 1u);
+  }
+  __syncthreads();
+  for(int i = threadIdx.x; i < S.nsamp; i += blockDim.x)
+    if(h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+/* Exclusive prefix sum of the nb histogram bins, one block of 1024 threads */
+__global__ void __launch_bounds__(1024) presort_scan
+  (const uint32_t* hist, uint32_t* off, int nb)
+{
+  __shared__ uint32_t part[1024];
+  const int t = threadIdx.x;
+  const int per = (nb + 1023) / 1024;
+  const int b0 = min(t * per, nb), b1 = min(b0 + per, nb);
+  uint32_t sum = 0;
+  for(int i = b0; i < b1; ++i) sum += hist[i];
+  part[t] = sum;
+  __syncthreads();
+  for(int d = 1; d < 1024; d <<= 1) {
+    const uint32_t v = t >= d ? part[t - d] : 0u;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  uint32_t run = t ? part[t - 1] : 0u;
+  for(int i = b0; i < b1; ++i) {
+    off[i] = run;
+    run += hist[i];
+  }
+}
+
+/* Each realisation to the next free place of its primitive's range */
+__global__ void __launch_bounds__(256) presort_scatter
+  (const uint32_t* keys, const uint4* draws, uint32_t n, uint32_t* off,
+   uint4* out_draws, uint32_t* out_off)
+{
+  for(uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n;
+      j += gridDim.x * blockDim.x) {
+    const uint32_t pos = atomicAdd(&off[keys[j]], 1u);
+    out_draws[pos] = draws[j];
+    out_off[pos] = j;
+  }
+}
+
+/* Per-device pool of the sort's scratch: stream-ordered allocations, so
+ * that launches on different streams never share a buffer, kept by the pool
+ * between launches */
+static cudaMemPool_t sort_pool(int dev)
+{
+  static cudaMemPool_t pools[64] = {};
+  static std::mutex lock;
+  if(dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> g(lock);
+  if(!pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    if(cudaMemPoolCreate(&pools[dev], &props) != cudaSuccess) {
+      pools[dev] = nullptr;
+      return nullptr;
+    }
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  return pools[dev];
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+/*******************************************************************************
  * Host launchers
  ******************************************************************************/
+
 template<class R, int MINB, bool TRACK>
 static int launch_variant
   (const DScene<R>& S, const DTallies& T, uint64_t seed, uint64_t first,
@@ -1729,12 +1901,56 @@ static int launch_variant
   const uint64_t needed = (count + block - 1) / block;
   if(blocks > needed) blocks = needed;
   if(blocks < 1) blocks = 1;
-  /* Work counter of this launch: counters[3] */
-  cudaMemsetAsync(T.counters + 3, 0, sizeof(unsigned long long),
-                  (cudaStream_t)stream);
-  realisation_kernel<R, MINB, TRACK><<<(unsigned)blocks, block, smem,
-                                       (cudaStream_t)stream>>>
-    (S, T, seed, first, count, cfg.max_segments, T.counters + 3, tr);
+  const cudaStream_t st = (cudaStream_t)stream;
+  const bool sort = !TRACK && cfg.coherent && count >= SORT_MIN && S.nsamp > 1
+                 && S.nsamp <= SORT_MAX_BINS;
+  if(!sort) {
+    /* Work counter of this launch: counters[3] */
+    cudaMemsetAsync(T.counters + 3, 0, sizeof(unsigned long long), st);
+    realisation_kernel<R, MINB, TRACK><<<(unsigned)blocks, block, smem, st>>>
+      (S, T, seed, first, count, cfg.max_segments, T.counters + 3, tr, nullptr,
+       nullptr, 1u);
+    return (int)cudaGetLastError();
+  }
+  const uint64_t chunk = count < SORT_CHUNK ? count : SORT_CHUNK;
+  const size_t o_keys = 0;
+  const size_t o_draws = o_keys + align256(chunk * sizeof(uint32_t));
+  const size_t o_sdraws = o_draws + align256(chunk * sizeof(uint4));
+  const size_t o_soff = o_sdraws + align256(chunk * sizeof(uint4));
+  const size_t o_hist = o_soff + align256(chunk * sizeof(uint32_t));
+  const size_t o_off = o_hist + align256((size_t)S.nsamp * sizeof(uint32_t));
+  const size_t bytes = o_off + align256((size_t)S.nsamp * sizeof(uint32_t));
+  cudaMemPool_t pool = sort_pool(dev);
+  unsigned char* buf = nullptr;
+  if(!pool || cudaMallocFromPoolAsync((void**)&buf, bytes, pool, st) != cudaSuccess)
+    return (int)cudaErrorMemoryAllocation;
+  uint32_t* keys = (uint32_t*)(buf + o_keys);
+  uint4* draws = (uint4*)(buf + o_draws);
+  uint4* sdraws = (uint4*)(buf + o_sdraws);
+  uint32_t* soff = (uint32_t*)(buf + o_soff);
+  uint32_t* hist = (uint32_t*)(buf + o_hist);
+  uint32_t* off = (uint32_t*)(buf + o_off);
+  const unsigned sort_blocks = (unsigned)nsm * 8u;
+  for(uint64_t c0 = 0; c0 < count; c0 += chunk) {
+    const uint32_t n = (uint32_t)(count - c0 < chunk ? count - c0 : chunk);
+    cudaMemsetAsync(hist, 0, (size_t)S.nsamp * sizeof(uint32_t), st);
+    presort_count<R><<<sort_blocks, 256, 0, st>>>(S, seed, first + c0, n, keys, draws, hist);
+    presort_scan<<<1, 1024, 0, st>>>(hist, off, S.nsamp);
+    presort_scatter<<<sort_blocks, 256, 0, st>>>(keys, draws, n, off, sdraws, soff);
+    uint64_t nb = (n + block - 1) / block;
+    if(nb > blocks) nb = blocks;
+    /* Segment s of the launch is segment (s x mul) mod nseg of the sorted
+     * order, mul coprime with nseg and near nseg / golden ratio */
+    const uint32_t nseg = (uint32_t)((n + SORT_SEG - 1) / SORT_SEG);
+    uint32_t mul = (uint32_t)(0.6180339887 * nseg) | 1u;
+    while(nseg > 1 && std::gcd(mul, nseg) != 1u) mul += 2;
+    if(nseg <= 1) mul = 1;
+    cudaMemsetAsync(T.counters + 3, 0, sizeof(unsigned long long), st);
+    realisation_kernel<R, MINB, TRACK><<<(unsigned)nb, block, smem, st>>>
+      (S, T, seed, first + c0, n, cfg.max_segments, T.counters + 3, tr, sdraws, soff,
+       mul);
+  }
+  cudaFreeAsync(buf, st);
   return (int)cudaGetLastError();
 }
 
