@@ -1827,16 +1827,43 @@ __global__ void __launch_bounds__(1024) presort_scan
   }
 }
 
-/* Each realisation to the next free place of its primitive's range */
+/* Each realisation to the next free place of its primitive's range. A block
+ * ranks a tile of SCATTER_PER x 256 realisations in shared memory, reserves
+ * one range per primitive of the tile with a single global atomic, then
+ * writes: one global atomic per (tile, primitive) instead of one per
+ * realisation */
+constexpr int SCATTER_PER = 16;
+
 __global__ void __launch_bounds__(256) presort_scatter
   (const uint32_t* keys, const uint4* draws, uint32_t n, uint32_t* off,
-   uint4* out_draws, uint32_t* out_off)
+   uint4* out_draws, uint32_t* out_off, int nb)
 {
-  for(uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n;
-      j += gridDim.x * blockDim.x) {
-    const uint32_t pos = atomicAdd(&off[keys[j]], 1u);
-    out_draws[pos] = draws[j];
-    out_off[pos] = j;
+  __shared__ uint32_t cnt[SORT_MAX_BINS];
+  const uint32_t tile = 256u * SCATTER_PER;
+  for(uint32_t t0 = blockIdx.x * tile; t0 < n; t0 += gridDim.x * tile) {
+    for(int i = threadIdx.x; i < nb; i += 256) cnt[i] = 0;
+    __syncthreads();
+    uint32_t k[SCATTER_PER], rank[SCATTER_PER];
+#pragma unroll
+    for(int e = 0; e < SCATTER_PER; ++e) {
+      const uint32_t j = t0 + e * 256u + threadIdx.x;
+      k[e] = j < n ? keys[j] : 0u;
+      rank[e] = j < n ? atomicAdd(&cnt[k[e]], 1u) : 0u;
+    }
+    __syncthreads();
+    for(int i = threadIdx.x; i < nb; i += 256)
+      if(cnt[i]) cnt[i] = atomicAdd(&off[i], cnt[i]);
+    __syncthreads();
+#pragma unroll
+    for(int e = 0; e < SCATTER_PER; ++e) {
+      const uint32_t j = t0 + e * 256u + threadIdx.x;
+      if(j < n) {
+        const uint32_t pos = cnt[k[e]] + rank[e];
+        out_draws[pos] = draws[j];
+        out_off[pos] = j;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -1936,7 +1963,8 @@ static int launch_variant
     cudaMemsetAsync(hist, 0, (size_t)S.nsamp * sizeof(uint32_t), st);
     presort_count<R><<<sort_blocks, 256, 0, st>>>(S, seed, first + c0, n, keys, draws, hist);
     presort_scan<<<1, 1024, 0, st>>>(hist, off, S.nsamp);
-    presort_scatter<<<sort_blocks, 256, 0, st>>>(keys, draws, n, off, sdraws, soff);
+    presort_scatter<<<sort_blocks, 256, 0, st>>>(keys, draws, n, off, sdraws, soff,
+                                                 S.nsamp);
     uint64_t nb = (n + block - 1) / block;
     if(nb > blocks) nb = blocks;
     /* Segment s of the launch is segment (s x mul) mod nseg of the sorted
