@@ -42,11 +42,11 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 DRAM_BYTES_PER_PATH = {"field": (110.2e6 + 859.3e6) / 4e6,
                        "beamdown": (73.9e6 + 387.0e6) / 4e6}  # beam-down: id order
 
-# Kernels of one plain launch of n realisations: below 2^16 the realisation
-# kernel alone; from 2^16 on, per chunk of 2^24 realisations, the coherent
+# Kernels of one plain launch of n realisations: below 2^24 the realisation
+# kernel alone; from 2^24 on, per chunk of 2^24 realisations, the coherent
 # order's presort (count, scan, scatter) and the realisation kernel (every
 # bench scene samples fewer than 12288 primitives)
-SORT_MIN, SORT_CHUNK = 1 << 16, 1 << 24
+SORT_MIN, SORT_CHUNK = 1 << 24, 1 << 24
 
 
 def launches_per_plain_launch(n):

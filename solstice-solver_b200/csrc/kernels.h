@@ -19,7 +19,7 @@ struct LaunchConfig {
   int rcv_doubles = 0; /* batched launches: largest item receiver-sum array
                         * (nrcv x 10 x 2); 0 => receiver sums go straight
                         * to device memory */
-  bool coherent = true; /* plain launches of at least 2^16 realisations run
+  bool coherent = true; /* plain launches of at least 2^24 realisations run
                          * in the order of their sampled primitives */
 };
 
