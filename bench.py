@@ -36,10 +36,11 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
             "map, pillbox sun 4.65 mrad el 30 az 180 DNI 900, extinction 1e-4/m")
 
 
-# DRAM bytes per path of the realisation kernel, from ncu captures of 4e6-path
-# launches of the same scenes (dram__bytes_read.sum + dram__bytes_write.sum);
+# DRAM bytes per path of the realisation kernel, from ncu captures of launches
+# of the same scenes (field: one sorted chunk of 2^24 paths; beam-down: 4e6
+# paths) (dram__bytes_read.sum + dram__bytes_write.sum);
 # the traffic scales with the paths traced (per-thread frames written back)
-DRAM_BYTES_PER_PATH = {"field": (110.2e6 + 859.3e6) / 4e6,
+DRAM_BYTES_PER_PATH = {"field": (416.7e6 + 3763.9e6) / 16777216,
                        "beamdown": (73.9e6 + 387.0e6) / 4e6}  # beam-down: id order
 
 # Kernels of one plain launch of n realisations: below 2^24 the realisation
@@ -394,8 +395,8 @@ def run_b200(args):
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak else None,
                      "traffic": (DRAM_BYTES_PER_PATH[args.config] * n
                                  if args.config in DRAM_BYTES_PER_PATH else None),
-                     "traffic_source": "ncu dram__bytes_read+write of a 4e6-path launch of "
-                                       "the realisation kernel, scaled to paths_per_step "
+                     "traffic_source": "ncu dram__bytes_read+write of a launch of the "
+                                       "realisation kernel, scaled to paths_per_step "
                                        "(bytes per step: its chunks' launches together)",
                      "timing": "CUDA events around each step: the realisation kernel and "
                                "the coherent order's presort (2.5 % of the step)",
