@@ -1312,6 +1312,9 @@ realisation_kernel
   for(;;) {
     /* Regeneration: idle lanes take the next realisations */
     const unsigned need = __ballot_sync(0xffffffffu, p.phase == PH_NONE && !done);
+    bool start = false;
+    uint64_t off = 0;
+    U32x4 r0;
     if(need && sorted_off) {
       /* Segments of SORT_SEG sorted realisations (one or two primitives) go
        * to warps whole, in a strided order, so that a warp's lanes start on
@@ -1345,13 +1348,10 @@ realisation_kernel
       }
       if(p.phase == PH_NONE && !done) {
         if(got) {
-          const uint64_t id = first + sorted_off[idx];
+          start = true;
+          off = sorted_off[idx];
           const uint4 d = sorted_draw[idx];
-          const U32x4 r0 = {{d.x, d.y, d.z, d.w}};
-          rng.i_lo = (uint32_t)id;
-          rng.i_hi = (uint32_t)(id >> 32);
-          init_path(S, rng, p, ps, bd, &r0);
-          ++npaths;
+          r0 = {{d.x, d.y, d.z, d.w}};
         } else if(exhausted) {
           done = true;
         }
@@ -1367,20 +1367,27 @@ realisation_kernel
         if(idx >= count) {
           done = true;
         } else {
-          const uint64_t id = first + idx;
-          rng.i_lo = (uint32_t)id;
-          rng.i_hi = (uint32_t)(id >> 32);
-          init_path(S, rng, p, ps, bd);
-          ++npaths;
-          if(TRACK) {
-            p.tslot = idx < tr.npaths ? (int)idx : -1;
-            p.tseq = 0;
-            if(p.tslot >= 0) {
-              if(tr.sun_len > 0)
-                track_vertex(tr, p, p.org + p.rd * (R)tr.sun_len, S.dni);
-              track_vertex(tr, p, p.org, p.prev[0]);
-            }
-          }
+          start = true;
+          off = idx;
+        }
+      }
+    }
+    /* One init_path for both orders, so that a realisation computes the same
+     * bits whichever order it runs in */
+    if(start) {
+      const uint64_t id = first + off;
+      rng.i_lo = (uint32_t)id;
+      rng.i_hi = (uint32_t)(id >> 32);
+      if(!sorted_off) r0 = rng.get(0u, RNG_PRIMARY);
+      init_path(S, rng, p, ps, bd, &r0);
+      ++npaths;
+      if(TRACK) {
+        p.tslot = off < tr.npaths ? (int)off : -1;
+        p.tseq = 0;
+        if(p.tslot >= 0) {
+          if(tr.sun_len > 0)
+            track_vertex(tr, p, p.org + p.rd * (R)tr.sun_len, S.dni);
+          track_vertex(tr, p, p.org, p.prev[0]);
         }
       }
     }
