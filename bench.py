@@ -121,6 +121,17 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return None
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -231,8 +242,15 @@ def run_reference(args):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc, "paths_per_step": n, "l2": "n/a (CPU)"},
+        "config": {"workload": desc, "paths_per_step": n, "l2": "n/a (CPU)",
+                   "paths_per_step_note": (
+                       "a bounded sample of the %d-realisation step: about %.0f s of "
+                       "CPU work per step, so that the whole run ends within minutes; "
+                       "paths are independent and the per-solve set-up is below 1 %% "
+                       "of a step, so paths/s does not depend on the sample size"
+                       % (args.paths, args.ref_step_seconds))},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
+                         "cpu_model": cpu_model(),
                          "sample": "%d realisations per step of the same scene" % n},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -419,15 +437,43 @@ def run_b200(args):
             rate, cn, cdt = cpu_reference_rate(args, args.cpu_seconds)
             line["cpu_baseline"] = {
                 "value": rate / 1e6, "unit": METRIC, "cores": os.cpu_count(), "kind": "port",
+                "cpu_model": cpu_model(),
                 "sample": "%d realisations of the same scene in %.1f s (OpenMP, all cores)"
                           % (cn, cdt)}
         except Exception as exc:
             line["cpu_baseline"] = {"value": None, "unit": METRIC, "cores": os.cpu_count(),
-                                    "kind": "port", "sample": "failed: %s" % exc}
-    if rank == 0:
-        print(json.dumps(line))
+                                    "kind": "port", "cpu_model": cpu_model(),
+                                    "sample": "failed: %s" % exc}
     del e
     s.close()
+    if args.config == "field" and args.heliostats == 1000 and not args.no_suns:
+        # The other half of the metric: time to 0.1 % SE on absorbed power
+        # for the 256 suns, batched against plain per-sun launches
+        r = suns_comparison(args, lib, opt, stream, sp, flush, dist, local, rank, world,
+                            min(args.steps, 3), min(args.warmup, 3))
+        line["time_to_0.1pct_se"] = {
+            "workload": SUNS, "suns": r["suns"], "paths": r["paths"],
+            "steps": min(args.steps, 3), "warmup": min(args.warmup, 3),
+            "batched_s": r["time_to_0.1pct_se_s"]["batched"],
+            "plain_fp32_plan_loop_s": r["time_to_0.1pct_se_s"]["plain_plan_loop"],
+            "plain_fp32_ssol_solve_loop_s": r["time_to_0.1pct_se_s"]["ssol_solve_loop"],
+            "speedup_vs_plan_loop": r["speedup_batched_vs_plain_plan_loop"],
+            "speedup_vs_ssol_solve_loop": r["speedup_batched_vs_ssol_solve_loop"],
+            "from_scratch_s": r["time_to_0.1pct_se_from_scratch_s"],
+            "speedup_from_scratch_vs_plan_loop": r["speedup_from_scratch_vs_plain_plan_loop"],
+            "speedup_from_scratch_vs_ssol_solve_loop":
+                r["speedup_from_scratch_vs_ssol_solve_loop"],
+            "suns_reaching_0.1pct_se": r["reached"],
+            "batched_mpaths_s": r["paths"] / r["per_step_batched_ms"] / 1e3,
+            "clocks": r["clocks"],
+            "arms": "batched: every sun in one persistent launch replayed from a CUDA "
+                    "graph (CUDA events); plain_fp32_plan_loop: one plain FP32 plan "
+                    "launch per sun, scenes resident (CUDA events); "
+                    "plain_fp32_ssol_solve_loop: one ssol_solve per sun (wall clock); "
+                    "from_scratch: pilot of 1e5 per sun, read-back, then the rest, "
+                    "set-up included (wall clock)"}
+    if rank == 0:
+        print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -438,8 +484,9 @@ SUNS = ("256 suns (16 elevations 5-85 deg x 16 azimuths, DNI U[300,1000]) over t
         "relative SE on absorbed power (from a pilot of log-U[1e5,1e7] budgets)")
 
 
-def run_suns(args):
-    """Batched multi-sun form against plain per-sun launches.
+def suns_comparison(args, lib, opt, stream, sp, flush, dist, local, rank, world,
+                    steps, warmup):
+    """Batched multi-sun form against plain per-sun launches, as a dict.
 
     Pilot: one batched launch with the seeded log-uniform budgets gives each
     sun's relative SE on absorbed power, hence the realisations n_i it needs
@@ -448,19 +495,12 @@ def run_suns(args):
     (b) a loop of plain plan launches, one per sun, scenes resident in HBM,
     (c) end to end through the public API, per step: batch create (scene
     build and upload), launch, finish (tally read-back and estimators);
-    and (d) the reference user's loop of one ssol_solve per sun."""
+    and (d) the reference user's loop of one ssol_solve per sun. From
+    scratch (e): each approach runs a pilot of 1e5 realisations per sun,
+    reads its estimates back and traces what each sun still needs."""
     import torch
     import pyssol as P
     import workloads as W
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    lib = P.load_product()
     grid = W.sun_grid()
     if args.suns:
         # evenly spaced subset of the 256 suns (small cases, profiling)
@@ -469,17 +509,6 @@ def run_suns(args):
     suns = shard_suns(grid, rank, world)
     built = W.batched_fields(lib, suns, n_helio=args.heliostats)
     scenes = [b[0] for b in built]
-    rcv = [b[1]["receiver"] for b in built]
-    opt = P.options(P.FP64 if args.fp64 else P.FP32, block_size=args.block,
-                    waves=args.waves, leaf=args.leaf, min_blocks=args.minb)
-    if args.autotune:
-        opt, _ = P.autotune(scenes[len(scenes) // 2], args.autotune_paths, opt,
-                            seed=args.seed + 77)
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    sp = P.C.c_void_p(stream.cuda_stream)
-    flush = torch.empty(max(1, args.flush_mib) * 1024 * 1024 // 4, dtype=torch.float32,
-                        device="cuda")
     rng = scenes[0].rng(seed=args.seed)
 
     # pilot
@@ -496,8 +525,8 @@ def run_suns(args):
     pilot.close()
     n_total = sum(need)
 
-    def timed(step, steps):
-        for w in range(args.warmup):
+    def timed(step):
+        for w in range(warmup):
             step()
             flush.zero_()
         torch.cuda.synchronize()
@@ -522,7 +551,7 @@ def run_suns(args):
     batch = P.Batch(lib, scenes, opt)
     clocks = Clocks(local)
     clocks.start()
-    ms_batched = timed(lambda: batch.launch(rng, need, sp), args.steps)
+    ms_batched = timed(lambda: batch.launch(rng, need, sp))
     clk = clocks.stop()
     ests = batch.finish(rng, 0, sp)
     # counters and scene bytes are batch-wide (every item's estimator carries
@@ -544,7 +573,7 @@ def run_suns(args):
     def plain_step():
         for pl, n in zip(plans, need):
             lib.call("ssol_b200_plan_launch", pl, rng, 0, n, sp)
-    ms_plain = timed(plain_step, args.steps)
+    ms_plain = timed(plain_step)
     for pl in plans:
         lib.raw("ssol_b200_plan_ref_put", pl)
 
@@ -553,13 +582,14 @@ def run_suns(args):
     d2h = tally_bytes
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for k in range(max(1, min(args.steps, 2))):
+    e2e_steps = max(1, min(steps, 2))
+    for k in range(e2e_steps):
         b = P.Batch(lib, scenes, opt)
         b.launch(rng, need, sp)
         es = b.finish(rng, 0, sp)
         del es
         b.close()
-    e2e_s = (time.perf_counter() - t0) / max(1, min(args.steps, 2))
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
     t0 = time.perf_counter()
     for sc, n in zip(scenes, need):
         e = sc.solve(n, rng=rng, options=opt)
@@ -628,33 +658,18 @@ def run_suns(args):
             del e2
         del e
     scratch_solve = time.perf_counter() - t0
+    for sc in scenes:
+        sc.close()
 
-    per_step_b = ms_batched / args.steps
-    per_step_p = ms_plain / args.steps
-    value = n_all / (per_step_b * 1e-3) / 1e6
+    per_step_b = ms_batched / steps
+    per_step_p = ms_plain / steps
     agg = {k: bstats[k] for k in ("rays", "node_visits", "triangle_tests",
                                   "quadric_tests", "bounces", "paths")}
-    peaks = measured_peaks()
-    nsm = torch.cuda.get_device_properties(local).multi_processor_count
-    sm_mhz = peaks.get("sm_max_mhz", 1965.0)
-    fp32_peak = nsm * 128 * 2 * sm_mhz * 1e6 / 1e12
-    # the counters cover the warm-up and timed launches of the batch
-    launches = args.warmup + args.steps
-    achieved = flops_per_run(agg) / launches / (per_step_b * 1e-3) / 1e12
-    line = {
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step_b,
-        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-        "dtype": "f64" if args.fp64 else "f32",
-        "data": "synthetic (seeded sun grid, DNI and budgets)",
-        "config": {"workload": SUNS, "suns": len(suns) * world,
-                   "paths_per_step": int(n_all),
-                   "l2": "flushed: 256 MiB write between steps",
-                   "parallelism": "sun slots per GPU" if world > 1 else "1 GPU",
-                   "launch": {"block": opt.block_size,
-                              "blocks_per_sm_budget": opt.min_blocks_per_sm,
-                              "waves": opt.waves, "bvh_leaf": opt.bvh_leaf_size,
-                              "autotuned": bool(args.autotune)}},
+    return {
+        "suns": len(suns) * world, "paths": int(n_all), "n_total_rank": n_total,
+        "per_step_batched_ms": per_step_b, "per_step_plain_ms": per_step_p,
+        "agg": agg, "launches": warmup + steps, "clocks": clk, "h2d": h2d, "d2h": d2h,
+        "e2e_s": e2e_s, "reached": reached,
         "time_to_0.1pct_se_s": {"batched": per_step_b * 1e-3,
                                 "plain_plan_loop": per_step_p * 1e-3,
                                 "ssol_solve_loop": solve_loop_s,
@@ -669,23 +684,78 @@ def run_suns(args):
         "speedup_from_scratch_vs_ssol_solve_loop": scratch_solve / scratch_batched,
         "speedup_batched_vs_plain_plan_loop": per_step_p / per_step_b,
         "speedup_batched_vs_ssol_solve_loop": solve_loop_s / (per_step_b * 1e-3),
-        "suns_reaching_0.1pct_se": reached,
-        "e2e": {"value": n_all / e2e_s / 1e6, "unit": METRIC, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h,
+    }
+
+
+def run_suns(args):
+    """The batched multi-sun line (see suns_comparison)."""
+    import torch
+    import pyssol as P
+    import workloads as W
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    lib = P.load_product()
+    opt = P.options(P.FP64 if args.fp64 else P.FP32, block_size=args.block,
+                    waves=args.waves, leaf=args.leaf, min_blocks=args.minb)
+    if args.autotune:
+        s, h = W.heliostat_field(lib, n_helio=args.heliostats, elevation=45.0)
+        opt, _ = P.autotune(s, args.autotune_paths, opt, seed=args.seed + 77)
+        s.close()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp = P.C.c_void_p(stream.cuda_stream)
+    flush = torch.empty(max(1, args.flush_mib) * 1024 * 1024 // 4, dtype=torch.float32,
+                        device="cuda")
+    r = suns_comparison(args, lib, opt, stream, sp, flush, dist, local, rank, world,
+                        args.steps, args.warmup)
+    per_step_b = r["per_step_batched_ms"]
+    value = r["paths"] / (per_step_b * 1e-3) / 1e6
+    peaks = measured_peaks()
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
+    sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = nsm * 128 * 2 * sm_mhz * 1e6 / 1e12
+    # the counters cover the warm-up and timed launches of the batch
+    achieved = flops_per_run(r["agg"]) / r["launches"] / (per_step_b * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step_b,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64" if args.fp64 else "f32",
+        "data": "synthetic (seeded sun grid, DNI and budgets)",
+        "config": {"workload": SUNS, "suns": r["suns"],
+                   "paths_per_step": r["paths"],
+                   "l2": "flushed: 256 MiB write between steps",
+                   "parallelism": "sun slots per GPU" if world > 1 else "1 GPU",
+                   "launch": {"block": opt.block_size,
+                              "blocks_per_sm_budget": opt.min_blocks_per_sm,
+                              "waves": opt.waves, "bvh_leaf": opt.bvh_leaf_size,
+                              "autotuned": bool(args.autotune)}},
+        "e2e": {"value": r["paths"] / r["e2e_s"] / 1e6, "unit": METRIC,
+                "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
                 "timing": "wall clock: batch create + launch + finish per step"},
         "gpu_launches": args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                     "traffic": BATCH_DRAM_BYTES_PER_PATH * n_total,
+                     "traffic": BATCH_DRAM_BYTES_PER_PATH * r["n_total_rank"],
                      "traffic_source": "ncu dram__bytes_read+write of the batched kernel on "
                                        "16 suns (7.1e6 paths), scaled to this rank's paths per launch",
                      "work_model": "as the field line"},
-        "clocks": clk,
+        "clocks": r["clocks"],
+        "suns_reaching_0.1pct_se": r["reached"],
     }
+    for k in ("time_to_0.1pct_se_s", "time_to_0.1pct_se_from_scratch_s",
+              "speedup_from_scratch_vs_plain_plan_loop",
+              "speedup_from_scratch_vs_ssol_solve_loop",
+              "speedup_batched_vs_plain_plan_loop", "speedup_batched_vs_ssol_solve_loop"):
+        line[k] = r[k]
     if rank == 0:
         print(json.dumps(line))
-    for sc in scenes:
-        sc.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -1047,6 +1117,8 @@ def main():
     p.add_argument("--no-fp64-check", action="store_true",
                    help="skip the FP32 vs all-FP64 comparison of the field configs")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-suns", action="store_true",
+                   help="field config: skip the 256-sun time-to-SE comparison")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--ref-step-seconds", type=float, default=10.0)
     args = p.parse_args()

@@ -170,18 +170,23 @@ SSOL_API res_T ssol_b200_batch_launch
 /* No counterpart in the reference. The same launch as
  * ssol_b200_batch_launch for callers that must not have device memory
  * allocated on their behalf while they launch: code that owns every device
- * allocation through its own pool, or that launches inside a region (a
- * caller's stream capture, a real-time loop) where allocating would break
- * its rules. The batch (scenes in, tallies out) is created beforehand; this
- * call allocates nothing: no cudaMalloc/cudaFree and no CUDA graph. The
- * kernel's scratch (budget prefix sums, per-item first realisation ids, the
- * work counter and launch counters) lives in a static device array sized for
- * at most 4096 items, which every GPU that loads the library keeps until the
- * process exits; batches with more items get RES_BAD_ARG. The first call on
- * a device looks up that array's device address (make it before any stream
- * capture). All calls share the array, so calls that overlap on the GPU
- * race; each call sets it up anew. Work counters of these launches are not
- * reported in ssol_b200_stats. Returns when the launch has completed. */
+ * allocation through its own pool, or a real-time loop whose rules forbid
+ * allocating (an allocation can block, or fail, at any time). The batch
+ * (scenes in, tallies out) is created beforehand; this call allocates
+ * nothing: no cudaMalloc/cudaFree and no CUDA graph. The kernel's scratch
+ * (budget prefix sums, per-item first realisation ids, the work counter and
+ * launch counters) lives in a static device array sized for at most 4096
+ * items, which every GPU that loads the library keeps until the process
+ * exits; batches with more items get RES_BAD_ARG. The first call on a device
+ * looks up that array's device address, with that device current, and keeps
+ * it for later calls (make that first call before any stream capture; after
+ * a cudaDeviceReset the kept address is stale and the process must not call
+ * this entry point again on that device). All calls share the array, so
+ * calls that overlap on the GPU race; each call sets it up anew. The call
+ * copies the budgets from host memory and waits for `stream` before it
+ * returns, so it is made outside any capture of `stream` (RES_BAD_ARG
+ * otherwise). Work counters of these launches are not reported in
+ * ssol_b200_stats. */
 SSOL_API res_T ssol_b200_batch_launch_noalloc
   (struct ssol_b200_batch* batch, const struct ssp_rng* rng,
    const uint64_t* budgets, void* stream);

@@ -32,6 +32,7 @@
 #include <float.h>
 #include <math.h>
 
+#include <atomic>
 #include <mutex>
 #include <numeric>
 
@@ -1908,6 +1909,22 @@ static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
  * Host launchers
  ******************************************************************************/
 
+/* The dynamic shared-memory limit of a kernel is an attribute of one
+ * device's context: raise it once per (kernel, device). `Tag` tells the
+ * kernels apart (one set of flags per template instance). */
+template<class Tag, class K>
+static void raise_smem_limit(K kernel, int dev)
+{
+  static std::atomic<unsigned long long> done_mask{0};
+  const unsigned long long bit = dev >= 0 && dev < 64 ? 1ull << dev : 0ull;
+  if(bit && (done_mask.load(std::memory_order_acquire) & bit)) return;
+  if(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          160 * 1024) == cudaSuccess && bit)
+    done_mask.fetch_or(bit, std::memory_order_acq_rel);
+}
+template<class R, int MINB, bool TRACK> struct RealisationTag {};
+template<class R, int MINB> struct BatchTag {};
+
 template<class R, int MINB, bool TRACK>
 static int launch_variant
   (const DScene<R>& S, const DTallies& T, uint64_t seed, uint64_t first,
@@ -1923,12 +1940,7 @@ static int launch_variant
   const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block + rcv_doubles)
                       * sizeof(double)
                     + (size_t)SMEM_STACK * block * sizeof(int);
-  static bool attr_set = false;
-  if(!attr_set) {
-    cudaFuncSetAttribute(realisation_kernel<R, MINB, TRACK>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    attr_set = true;
-  }
+  raise_smem_limit<RealisationTag<R, MINB, TRACK>>(realisation_kernel<R, MINB, TRACK>, dev);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor
     (&per_sm, realisation_kernel<R, MINB, TRACK>, block, smem);
@@ -2022,12 +2034,7 @@ static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg
                     + (size_t)SMEM_STACK * block * sizeof(int)
                     + (size_t)(block / 32) * 2 * (2 * NGLOBAL + cfg.rcv_doubles) * sizeof(double)
                     + (size_t)(block / 32) * 2 * sizeof(DScene<R>);
-  static bool attr_set = false;
-  if(!attr_set) {
-    cudaFuncSetAttribute(batch_kernel<R, MINB>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    attr_set = true;
-  }
+  raise_smem_limit<BatchTag<R, MINB>>(batch_kernel<R, MINB>, dev);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor
     (&per_sm, batch_kernel<R, MINB>, block, smem);
@@ -2079,18 +2086,22 @@ static __device__ __align__(256) unsigned long long
  * not an address a kernel may be given */
 static int noalloc_scratch_address(unsigned long long** out)
 {
-  static unsigned long long* cache[64] = {};
+  /* Atomic entries: two host threads may make their first call on a device
+   * at the same time (both then store the same address) */
+  static std::atomic<unsigned long long*> cache[64] = {};
   int dev = 0;
   cudaError_t err = cudaGetDevice(&dev);
   if(err != cudaSuccess) return (int)err;
   if(dev < 0 || dev >= 64) return (int)cudaErrorInvalidDevice;
-  if(!cache[dev]) {
+  unsigned long long* addr = cache[dev].load(std::memory_order_acquire);
+  if(!addr) {
     void* ptr = nullptr;
     err = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if(err != cudaSuccess) return (int)err;
-    cache[dev] = (unsigned long long*)ptr;
+    addr = (unsigned long long*)ptr;
+    cache[dev].store(addr, std::memory_order_release);
   }
-  *out = cache[dev];
+  *out = addr;
   return 0;
 }
 
@@ -2115,8 +2126,7 @@ static int launch_batch_noalloc_variant
                     + (size_t)SMEM_STACK * block * sizeof(int)
                     + (size_t)(block / 32) * 2 * (2 * NGLOBAL + cfg.rcv_doubles) * sizeof(double)
                     + (size_t)(block / 32) * 2 * sizeof(DScene<R>);
-  cudaFuncSetAttribute(batch_kernel<R, MINB>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+  raise_smem_limit<BatchTag<R, MINB>>(batch_kernel<R, MINB>, dev);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor
     (&per_sm, batch_kernel<R, MINB>, block, smem);

@@ -1358,6 +1358,18 @@ extern "C" res_T ssol_b200_batch_launch_noalloc
   b->h_prefix[n] = total;
   if(!total) return RES_OK;
   const cudaStream_t s = stream ? (cudaStream_t)stream : (cudaStream_t)b->dev->stream;
+  /* The call copies the budgets from host memory and waits for `stream`
+   * before it returns; on a stream that is recording a capture, the wait
+   * would end the capture with an error and the copies would read host
+   * arrays that later calls overwrite */
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if(cudaStreamIsCapturing(s, &cap) != cudaSuccess
+  || cap != cudaStreamCaptureStatusNone) {
+    b->dev->log_error("ssol_b200_batch_launch_noalloc: the stream is being "
+                      "captured; this call waits for its launch and must be "
+                      "made outside a capture.\n");
+    return RES_BAD_ARG;
+  }
   const LaunchConfig cfg = batch_config(b);
   const int err = b->opt.precision == SSOL_B200_FP32
     ? launch_batch_noalloc_f32((const DScene<float>*)b->d_scenes, b->d_tallies,
