@@ -78,9 +78,20 @@ SSOL_API res_T ssol_b200_plan_create
 SSOL_API res_T ssol_b200_plan_ref_get(struct ssol_b200_plan* plan);
 SSOL_API res_T ssol_b200_plan_ref_put(struct ssol_b200_plan* plan);
 /* Zero the device tallies, asynchronously on `stream` (NULL => the plan's
- * own stream) */
+ * own stream), and clear an abort request (call it once the plan's earlier
+ * launches have completed) */
 SSOL_API res_T ssol_b200_plan_reset
   (struct ssol_b200_plan* plan, void* stream);
+/* Host-side stop of a long solve, from any thread: the plan's running and
+ * queued launches take no new realisations (paths in flight finish; the
+ * request is read by the kernels' work fetch through host memory mapped into
+ * the device's address space, so it takes effect within a few milliseconds).
+ * It stays until ssol_b200_plan_reset. ssol_b200_plan_finish then builds the
+ * estimator of the realisations that ran (realisation count below the one
+ * asked for) and returns RES_BAD_OP, as the reference's solve returns the
+ * error that stopped its loop with a valid estimator
+ * (src/ssol_solver.c:1229, 1339). */
+SSOL_API res_T ssol_b200_plan_abort(struct ssol_b200_plan* plan);
 /* Enqueue realisations [first, first + count) of the streams keyed by `rng`;
  * tallies accumulate. Asynchronous. */
 SSOL_API res_T ssol_b200_plan_launch

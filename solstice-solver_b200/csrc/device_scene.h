@@ -254,8 +254,21 @@ struct DTallies {
   double* samp_rcv; /* nsampled x nrcv x NRCV_Q x 2 */
   double* prim; /* nprim_slots x NRCV_Q x 2 */
   unsigned long long* nb_samples; /* nsampled */
-  unsigned long long* counters; /* [0] failed, [1] killed, [2] overflow */
+  unsigned long long* counters; /* [0] failed, [1] killed, [2] overflow,
+                                   [3] work counter, [4] stop word */
   DStats* stats;
+};
+
+/* Early stop of a plain launch (src/ssol_solver.c:1229, 1240-1248): once
+ * `max_failed` paths have failed, the kernel sets the device word `stop`
+ * and its warps take no new realisations; `abort` (host memory mapped into
+ * the device's address space, or null) is a word the host may set at any
+ * time for the same effect. Paths in flight always finish. `stop` null
+ * disables the failure limit. */
+struct DControl {
+  unsigned long long max_failed;
+  unsigned long long* stop;
+  const volatile unsigned int* abort;
 };
 
 /* Path tracking (ssol_path_tracker): the realisations of launch index

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <limits>
 #include <map>
+#include <set>
 
 void ssolb_d33_invtrans(double out[9], const double m[9]); /* objects.cpp */
 
@@ -184,7 +185,7 @@ int intern_medium(FlatScene<R>& out, Interner& in, const ssol_medium& m)
 /* Evaluate shader callbacks once per sun wavelength node on a canonical
  * fragment; shaders may vary with the wavelength, not with the position */
 template<class R>
-void tabulate_shaders(FlatScene<R>& out, ssol_material* m, ssol_device* dev)
+bool tabulate_shaders(FlatScene<R>& out, ssol_material* m, ssol_device* dev)
 {
   ssol_surface_fragment frag = SSOL_SURFACE_FRAGMENT_NULL;
   frag.dir[2] = -1;
@@ -200,12 +201,23 @@ void tabulate_shaders(FlatScene<R>& out, ssol_material* m, ssol_device* dev)
     out.shader_tab.push_back((R)rough);
   }
   if(m->normal) {
-    double n[3] = {0, 0, 0};
-    m->normal(dev, m->buf, out.shader_wl[0], &frag, n);
-    if(n[0] != 0 || n[1] != 0 || n[2] != 1)
-      dev->log_warning("normal shaders other than the shading normal are "
-                       "not supported on the device; using Ns.\n");
+    /* Normal shaders are evaluated per hit by the reference
+     * (src/ssol_material.c:551-655); the device uses Ns, so any other
+     * normal is refused rather than silently replaced */
+    ssol_surface_fragment tilted = frag;
+    tilted.Ns[0] = 0.6; tilted.Ns[2] = 0.8;
+    const ssol_surface_fragment* probes[2] = {&frag, &tilted};
+    for(const ssol_surface_fragment* f : probes) {
+      double n[3] = {0, 0, 0};
+      m->normal(dev, m->buf, out.shader_wl[0], f, n);
+      if(n[0] != f->Ns[0] || n[1] != f->Ns[1] || n[2] != f->Ns[2]) {
+        dev->log_error("normal shaders other than the shading normal Ns are "
+                       "not supported on the device.\n");
+        return false;
+      }
+    }
   }
+  return true;
 }
 
 /* Fragments of the three vertices of mesh triangle t seen from `side`
@@ -328,6 +340,81 @@ bool material_varies(ssol_material* m, const ssol_surface_fragment* f, int nf,
     if(r != r0 || g != g0) return true;
   }
   return false;
+}
+
+/* Whether a mirror or matte material's shaders read the fragment's
+ * incoming direction: at each probe fragment, the values with dir = -Ng and
+ * with dir tilted toward dPdu differ. The reference evaluates the shaders
+ * per hit with the ray's direction (src/ssol_material.c:551-655); the device
+ * tables and per-vertex bakes cannot hold that. */
+bool material_reads_dir(ssol_material* m, const ssol_surface_fragment* f, int nf,
+                        double wl, ssol_device* dev)
+{
+  if(m->type != SSOL_MATERIAL_MIRROR && m->type != SSOL_MATERIAL_MATTE) return false;
+  for(int i = 0; i < nf; ++i) {
+    ssol_surface_fragment g = f[i];
+    double t[3], l = 0;
+    for(int c = 0; c < 3; ++c) { t[c] = g.dir[c] + 0.5 * g.dPdu[c]; l += t[c] * t[c]; }
+    l = std::sqrt(l);
+    if(!(l > 0)) continue;
+    for(int c = 0; c < 3; ++c) g.dir[c] = t[c] / l;
+    double r0 = 0, g0 = 0, r1 = 0, g1 = 0;
+    if(m->reflectivity) {
+      m->reflectivity(dev, m->buf, wl, &f[i], &r0);
+      m->reflectivity(dev, m->buf, wl, &g, &r1);
+    }
+    if(m->roughness) {
+      m->roughness(dev, m->buf, wl, &f[i], &g0);
+      m->roughness(dev, m->buf, wl, &g, &g1);
+    }
+    if(r0 != r1 || g0 != g1) return true;
+  }
+  return false;
+}
+
+/* Fragments at a 3 x 3 grid of points of a punched surface (the carving's
+ * box, points outside the carvings skipped; its centre always kept), seen
+ * from `side`: P on the quadric through the local -> world map M, Ng = Ns the
+ * side's unit normal, dir = -Ng, dPdu and dPdv the local x and y axes */
+static int punched_fragments(const ssol_shape* shape, const double M[12], int side,
+                             ssol_surface_fragment f[9])
+{
+  int n = 0;
+  for(int j = 0; j < 3; ++j)
+    for(int i = 0; i < 3; ++i) {
+      const double x = shape->carve_lo[0] + 0.5 * i * (shape->carve_hi[0] - shape->carve_lo[0]);
+      const double y = shape->carve_lo[1] + 0.5 * j * (shape->carve_hi[1] - shape->carve_lo[1]);
+      if(!(i == 1 && j == 1) && !ssolb_in_carvings(shape->carvings, x, y)) continue;
+      const double h = 1e-4 * std::max(1.0, shape->carve_hi[0] - shape->carve_lo[0]);
+      const double z = ssolb_quadric_z(shape->quadric.type, shape->qparam, x, y);
+      const double zx = (ssolb_quadric_z(shape->quadric.type, shape->qparam, x + h, y)
+                       - ssolb_quadric_z(shape->quadric.type, shape->qparam, x - h, y)) / (2 * h);
+      const double zy = (ssolb_quadric_z(shape->quadric.type, shape->qparam, x, y + h)
+                       - ssolb_quadric_z(shape->quadric.type, shape->qparam, x, y - h)) / (2 * h);
+      const double pl[3] = {x, y, z}, tu[3] = {1, 0, zx}, tv[3] = {0, 1, zy};
+      ssol_surface_fragment& fr = f[n++];
+      fr = SSOL_SURFACE_FRAGMENT_NULL;
+      double pw[3], du[3], dv[3], ng[3];
+      apply(M, pl, pw);
+      for(int c = 0; c < 3; ++c) {
+        du[c] = M[c] * tu[0] + M[3 + c] * tu[1] + M[6 + c] * tu[2];
+        dv[c] = M[c] * tv[0] + M[3 + c] * tv[1] + M[6 + c] * tv[2];
+      }
+      ng[0] = du[1] * dv[2] - du[2] * dv[1];
+      ng[1] = du[2] * dv[0] - du[0] * dv[2];
+      ng[2] = du[0] * dv[1] - du[1] * dv[0];
+      double l = std::sqrt(ng[0] * ng[0] + ng[1] * ng[1] + ng[2] * ng[2]);
+      if(!(l > 0)) l = 1;
+      const double sg = side == 0 ? 1.0 : -1.0;
+      for(int c = 0; c < 3; ++c) {
+        fr.P[c] = pw[c];
+        fr.Ng[c] = fr.Ns[c] = sg * ng[c] / l;
+        fr.dir[c] = -fr.Ng[c];
+        fr.dPdu[c] = du[c];
+        fr.dPdv[c] = dv[c];
+      }
+    }
+  return n;
 }
 
 /* The patch's surface as F = kx x^2 + ky y^2 + kz (z - z0)^2 + lz z + m
@@ -482,6 +569,7 @@ static res_T flatten_impl
 
   /* Materials */
   std::map<const ssol_material*, int> mtl_index;
+  bool bad_shader = false;
   auto material_id = [&](ssol_material* m) {
     auto it = mtl_index.find(m);
     if(it != mtl_index.end()) return it->second;
@@ -494,7 +582,7 @@ static res_T flatten_impl
     d.slab_medium = intern_medium(out, in, m->slab_medium);
     d.thickness = m->thickness;
     d.table = (int32_t)out.shader_tab.size();
-    tabulate_shaders(out, m, dev);
+    if(!tabulate_shaders(out, m, dev)) bad_shader = true;
     const int id = (int)out.mtls.size();
     out.mtls.push_back(d);
     mtl_index.emplace(m, id);
@@ -509,6 +597,7 @@ static res_T flatten_impl
   std::vector<DTriShade<R>> tsh;
   bool need_tshade = false;
   std::map<std::pair<const ssol_material*, const ssol_shape*>, bool> varies;
+  std::set<std::pair<const ssol_material*, const ssol_shape*>> punched_checked;
   std::vector<double> samp_area;
   for(size_t ii = 0; ii < scn->instances.size(); ++ii) {
     ssol_instance* inst = scn->instances[ii];
@@ -590,6 +679,15 @@ static res_T flatten_impl
                                   out.shader_wl.front(), dev)
                   || material_varies(side_mtl[sd], fr.data(), 3 * nprobe,
                                      out.shader_wl.back(), dev));
+            if(ntris > 0
+            && (material_reads_dir(side_mtl[sd], fr.data(), 3 * nprobe,
+                                   out.shader_wl.front(), dev)
+                || material_reads_dir(side_mtl[sd], fr.data(), 3 * nprobe,
+                                      out.shader_wl.back(), dev))) {
+              dev->log_error("shaders that read the incoming direction are not "
+                             "supported on the device.\n");
+              return RES_BAD_ARG;
+            }
             found = varies.emplace(key, v).first;
           }
           bake_side[sd] = found->second;
@@ -689,6 +787,30 @@ static res_T flatten_impl
         if(!invert(W, M)) {
           dev->log_error("singular instance transform.\n");
           return RES_BAD_ARG;
+        }
+        /* The device evaluates a punched surface's shaders from the
+         * per-material table: shaders that vary over it, or read the
+         * incoming direction, are refused */
+        ssol_material* pside[2] = {ss.front, ss.back};
+        for(int sd = 0; sd < 2; ++sd) {
+          const auto key = std::make_pair((const ssol_material*)pside[sd],
+                                          (const ssol_shape*)shape);
+          if(punched_checked.count(key)) continue;
+          punched_checked.insert(key);
+          ssol_surface_fragment fr[9];
+          const int nf = punched_fragments(shape, M, sd, fr);
+          for(const double wl : {out.shader_wl.front(), out.shader_wl.back()}) {
+            if(material_varies(pside[sd], fr, nf, wl, dev)) {
+              dev->log_error("shaders that vary over a punched surface are not "
+                             "supported on the device.\n");
+              return RES_BAD_ARG;
+            }
+            if(material_reads_dir(pside[sd], fr, nf, wl, dev)) {
+              dev->log_error("shaders that read the incoming direction are not "
+                             "supported on the device.\n");
+              return RES_BAD_ARG;
+            }
+          }
         }
         DQuadric<R> q;
         to_rows(q.w2l, W);
@@ -810,6 +932,7 @@ static res_T flatten_impl
       out.sinsts.push_back(si);
     }
   }
+  if(bad_shader) return RES_BAD_ARG;
   if(!for_draw && (!has_sampled || out.samp.empty())) {
     dev->log_error("No solstice instance to sample.\n");
     return RES_BAD_ARG;

@@ -1130,12 +1130,15 @@ __device__ __noinline__ void commit_path
   (const DScene<R>& S, const DTallies& T, PathState<R>& p, int end,
    double* acc, double* ps, int stride, double* smem_rcv, const int* xr,
    const int* xp, const double (*xv)[6], double* racc = nullptr,
-   int* racc_slot = nullptr)
+   int* racc_slot = nullptr, const DControl* ctl = nullptr)
 {
   atomicAdd(&T.nb_samples[p.samp], 1ull);
   if(p.overflow) end = END_FAIL;
   if(end == END_FAIL) {
-    atomicAdd(&T.counters[0], 1ull);
+    /* The failure that reaches the limit stops the launch's work fetch
+     * (src/ssol_solver.c:1240-1245) */
+    const unsigned long long nf = atomicAdd(&T.counters[0], 1ull) + 1ull;
+    if(ctl && ctl->stop && nf >= ctl->max_failed) atomicExch(ctl->stop, 1ull);
     if(p.overflow) atomicAdd(&T.counters[2], 1ull);
     return;
   }
@@ -1271,7 +1274,7 @@ realisation_kernel
   (const DScene<R> S, const DTallies T, uint64_t seed, uint64_t first,
    uint64_t count, unsigned long long max_segments,
    unsigned long long* next_path, const DTrack tr, const uint4* sorted_draw,
-   const uint32_t* sorted_off, uint32_t seg_mul)
+   const uint32_t* sorted_off, uint32_t seg_mul, const DControl ctl)
 {
   /* Shared memory: per-thread FP64 global sums [12][blockDim], per-thread
    * path sums [10][blockDim], the receiver-side sums, the first traversal
@@ -1309,6 +1312,8 @@ realisation_kernel
    * sorted realisations */
   uint32_t seg_cur = 0, seg_end = 0;
   const uint32_t nseg = (uint32_t)((count + SORT_SEG - 1) / SORT_SEG);
+  const bool polled = ctl.stop || ctl.abort;
+  uint32_t fetches = 0;
 
   for(;;) {
     /* Regeneration: idle lanes take the next realisations */
@@ -1316,7 +1321,23 @@ realisation_kernel
     bool start = false;
     uint64_t off = 0;
     U32x4 r0;
-    if(need && sorted_off) {
+    /* Early stop: the failure limit's device word at every fetch, the
+     * host's abort word (a read across the bus) every 16th; a halted warp
+     * takes no new realisation and ends once its paths in flight end */
+    bool halt = false;
+    if(need && polled) {
+      const int leader = __ffs(need) - 1;
+      int h = 0;
+      if((int)lane == leader) {
+        if(ctl.stop && *(volatile const unsigned long long*)ctl.stop) h = 1;
+        if(ctl.abort && (fetches & 15u) == 0u && *ctl.abort) h = 1;
+      }
+      ++fetches;
+      halt = __shfl_sync(0xffffffffu, h, leader) != 0;
+    }
+    if(halt) {
+      if(p.phase == PH_NONE) done = true;
+    } else if(need && sorted_off) {
       /* Segments of SORT_SEG sorted realisations (one or two primitives) go
        * to warps whole, in a strided order, so that a warp's lanes start on
        * the same heliostat while the warps of the GPU spread over the field */
@@ -1481,7 +1502,7 @@ realisation_kernel
           : (end == END_FAIL || p.overflow) ? 3 : (p.nent > 0 ? 2 : 0);
         tr.path_nv[p.tslot] = (int32_t)p.tseq;
       }
-      commit_path(S, T, p, end, acc, ps, bd, smem_rcv, xr, xp, xv, racc, &racc_slot);
+      commit_path(S, T, p, end, acc, ps, bd, smem_rcv, xr, xp, xv, racc, &racc_slot, &ctl);
       p.phase = PH_NONE;
     }
   }
@@ -1954,12 +1975,16 @@ static int launch_variant
   const cudaStream_t st = (cudaStream_t)stream;
   const bool sort = !TRACK && cfg.coherent && count >= SORT_MIN && S.nsamp > 1
                  && S.nsamp <= SORT_MAX_BINS;
+  DControl ctl;
+  ctl.max_failed = cfg.max_failed;
+  ctl.stop = cfg.max_failed != ~0ull ? T.counters + 4 : nullptr;
+  ctl.abort = cfg.abort_word;
   if(!sort) {
     /* Work counter of this launch: counters[3] */
     cudaMemsetAsync(T.counters + 3, 0, sizeof(unsigned long long), st);
     realisation_kernel<R, MINB, TRACK><<<(unsigned)blocks, block, smem, st>>>
       (S, T, seed, first, count, cfg.max_segments, T.counters + 3, tr, nullptr,
-       nullptr, 1u);
+       nullptr, 1u, ctl);
     return (int)cudaGetLastError();
   }
   const uint64_t chunk = count < SORT_CHUNK ? count : SORT_CHUNK;
@@ -1999,7 +2024,7 @@ static int launch_variant
     cudaMemsetAsync(T.counters + 3, 0, sizeof(unsigned long long), st);
     realisation_kernel<R, MINB, TRACK><<<(unsigned)nb, block, smem, st>>>
       (S, T, seed, first + c0, n, cfg.max_segments, T.counters + 3, tr, sdraws, soff,
-       mul);
+       mul, ctl);
   }
   cudaFreeAsync(buf, st);
   return (int)cudaGetLastError();

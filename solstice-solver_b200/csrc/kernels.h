@@ -21,6 +21,11 @@ struct LaunchConfig {
                         * to device memory */
   bool coherent = true; /* plain launches of at least 2^24 realisations run
                          * in the order of their sampled primitives */
+  /* Plain launches: stop handing out realisations once this many paths
+   * have failed (~0: never), or once the host sets *abort_word (mapped host
+   * memory, may be null) */
+  unsigned long long max_failed = ~0ull;
+  const unsigned int* abort_word = nullptr;
 };
 
 /* Enqueue the realisations [first, first + count) of the stream keyed by

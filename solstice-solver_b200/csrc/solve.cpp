@@ -238,6 +238,10 @@ struct ssol_b200_plan {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double kernel_ms = 0;
   bool timing_valid = false;
+  /* Abort word: host memory mapped into the device's address space, set by
+   * ssol_b200_plan_abort and polled by the launches' work fetch */
+  unsigned int* abort_host = nullptr;
+  const unsigned int* abort_dev = nullptr;
 };
 
 static TallyLayout tally_layout(int nrcv, int nsampled, int nprim_slots)
@@ -255,7 +259,7 @@ static TallyLayout tally_layout(int nrcv, int nsampled, int nprim_slots)
   tl.samp_rcv = take((size_t)nsampled * nrcv * NRCV_Q * 2 * sizeof(double));
   tl.prim = take((size_t)nprim_slots * NRCV_Q * 2 * sizeof(double));
   tl.nb_samples = take((size_t)nsampled * sizeof(unsigned long long));
-  tl.counters = take(4 * sizeof(unsigned long long));
+  tl.counters = take(8 * sizeof(unsigned long long));
   tl.stats = take(sizeof(DStats));
   tl.total = off;
   return tl;
@@ -306,6 +310,9 @@ static res_T make_estimator
   const size_t failed = (size_t)cnt[0];
   e->failed_count = failed;
   e->realisation_count = (size_t)nreal - std::min<size_t>(failed, nreal);
+  /* `nreal` counts the realisations that ran: an early stop leaves the
+   * rest unstarted, as the reference's loop skips them once its error flag
+   * is set (src/ssol_solver.c:1229) */
   for(int q = 0; q < NGLOBAL; ++q) {
     e->global[q][0] = g[2 * q];
     e->global[q][1] = g[2 * q + 1];
@@ -626,6 +633,7 @@ static void plan_release(ssol_b200_plan* p)
   dev_free(p->dev, p->d_tally, p->tl.total);
   if(p->ev0) cudaEventDestroy(p->ev0);
   if(p->ev1) cudaEventDestroy(p->ev1);
+  if(p->abort_host) cudaFreeHost(p->abort_host);
   if(p->scn) ssol_scene_ref_put(p->scn);
   ssol_device* dev = p->dev;
   delete p;
@@ -712,6 +720,16 @@ extern "C" res_T ssol_b200_plan_create
     return RES_MEM_ERR;
   }
   p->t = bind_tallies(p->tl, (unsigned char*)p->d_tally);
+  void* dptr = nullptr;
+  if(cudaHostAlloc((void**)&p->abort_host, 64, cudaHostAllocMapped) != cudaSuccess
+  || cudaHostGetDevicePointer(&dptr, p->abort_host, 0) != cudaSuccess) {
+    if(p->abort_host) cudaFreeHost(p->abort_host);
+    p->abort_host = nullptr;
+    plan_release(p);
+    return RES_MEM_ERR;
+  }
+  p->abort_dev = (const unsigned int*)dptr;
+  *p->abort_host = 0;
   cudaEventCreate(&p->ev0);
   cudaEventCreate(&p->ev1);
   *out = p;
@@ -723,9 +741,17 @@ static cudaStream_t plan_stream(ssol_b200_plan* p, void* stream)
   return stream ? (cudaStream_t)stream : (cudaStream_t)p->dev->stream;
 }
 
+extern "C" res_T ssol_b200_plan_abort(ssol_b200_plan* p)
+{
+  if(!p || !p->abort_host) return RES_BAD_ARG;
+  __atomic_store_n(p->abort_host, 1u, __ATOMIC_SEQ_CST);
+  return RES_OK;
+}
+
 extern "C" res_T ssol_b200_plan_reset(ssol_b200_plan* p, void* stream)
 {
   if(!p) return RES_BAD_ARG;
+  if(p->abort_host) __atomic_store_n(p->abort_host, 0u, __ATOMIC_SEQ_CST);
   if(cudaMemsetAsync(p->d_tally, 0, p->tl.total, plan_stream(p, stream))
      != cudaSuccess)
     return RES_UNKNOWN_ERR;
@@ -736,7 +762,8 @@ extern "C" res_T ssol_b200_plan_reset(ssol_b200_plan* p, void* stream)
 
 static res_T plan_launch
   (ssol_b200_plan* p, const ssp_rng* rng, const uint64_t first,
-   const uint64_t count, void* stream, const DTrack* track)
+   const uint64_t count, void* stream, const DTrack* track,
+   const unsigned long long max_failed = ~0ull)
 {
   if(!p || !rng) return RES_BAD_ARG;
   if(!count) return RES_OK;
@@ -747,6 +774,8 @@ static res_T plan_launch
   cfg.waves = p->opt.waves;
   cfg.max_segments = p->opt.max_segments;
   cfg.min_blocks = p->opt.min_blocks_per_sm;
+  cfg.max_failed = max_failed;
+  cfg.abort_word = p->abort_dev;
   const uint64_t start = rng->position + first;
   cudaEventRecord(p->ev0, s);
   const int err = p->opt.precision == SSOL_B200_FP32
@@ -797,9 +826,17 @@ extern "C" res_T ssol_b200_plan_finish
     if(cudaEventElapsedTime(&ms, p->ev0, p->ev1) == cudaSuccess)
       p->kernel_ms = ms;
   }
-  return make_estimator(p->dev, p->scn, p->meta, p->tl, h.data(), nreal, rng,
-                        nreal, (const DStats*)(h.data() + p->tl.stats),
-                        p->kernel_ms, p->scene_bytes, max_failed, out);
+  /* Realisations that ran: fewer than asked for after an early stop */
+  const DStats* st = (const DStats*)(h.data() + p->tl.stats);
+  const uint64_t ran = std::min<uint64_t>(nreal, st->paths);
+  res_T res = make_estimator(p->dev, p->scn, p->meta, p->tl, h.data(), ran, rng,
+                             nreal, st, p->kernel_ms, p->scene_bytes, max_failed, out);
+  if(res == RES_OK && p->abort_host && __atomic_load_n(p->abort_host, __ATOMIC_SEQ_CST)) {
+    p->dev->log_error("the solve was aborted: %llu of %llu realisations ran.\n",
+                      (unsigned long long)ran, (unsigned long long)nreal);
+    res = RES_BAD_OP;
+  }
+  return res;
 }
 
 extern "C" res_T ssol_b200_autotune
@@ -1448,7 +1485,7 @@ extern "C" res_T ssol_solve_ex
   res_T res = ssol_b200_plan_create(scn, options, &plan);
   if(res != RES_OK) return res;
   if(!tracker) {
-    res = ssol_b200_plan_launch(plan, rng, 0, n, nullptr);
+    res = plan_launch(plan, rng, 0, n, nullptr, nullptr, (unsigned long long)max_failed);
     if(res == RES_OK)
       res = ssol_b200_plan_finish(plan, rng, n, max_failed, nullptr, out);
     ssol_b200_plan_ref_put(plan);
@@ -1483,7 +1520,7 @@ extern "C" res_T ssol_solve_ex
   || cudaMemsetAsync(tr.path_type, 0xff, (size_t)tr.npaths * sizeof(int32_t), s)
        != cudaSuccess)
     res = RES_UNKNOWN_ERR;
-  if(res == RES_OK) res = plan_launch(plan, rng, 0, n, s, &tr);
+  if(res == RES_OK) res = plan_launch(plan, rng, 0, n, s, &tr, (unsigned long long)max_failed);
   if(res == RES_OK) res = ssol_b200_plan_finish(plan, rng, n, max_failed, s, out);
   if(*out) {
     unsigned long long nv = 0;

@@ -262,6 +262,7 @@ _OPTIONAL = {
     "ssol_b200_plan_create": [VP, C.POINTER(B200Options), PVP],
     "ssol_b200_plan_ref_put": [VP],
     "ssol_b200_plan_reset": [VP, VP],
+    "ssol_b200_plan_abort": [VP],
     "ssol_b200_plan_launch": [VP, VP, C.c_uint64, C.c_uint64, VP],
     "ssol_b200_plan_finish": [VP, VP, C.c_uint64, C.c_size_t, VP, PVP],
     "ssol_b200_batch_create": [PVP, C.c_size_t, C.POINTER(B200Options), PVP],

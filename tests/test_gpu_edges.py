@@ -7,7 +7,9 @@ exact identities:
 - a scene without receivers (warning only; nothing is absorbed by receivers);
 - the failure rule (src/ssol_solver.c:1240-1245, 1340): every path meets a
   dielectric whose outside medium is not the air; RES_BAD_OP with a valid
-  estimator whatever max_failed_count, as on the oracle;
+  estimator whatever max_failed_count, as on the oracle; once the limit is
+  reached no new realisation is scheduled (src/ssol_solver.c:1229);
+- a host-side abort of a running plan (ssol_b200_plan_abort);
 - a 256 x 256 per-primitive receiver map (131072 triangles): the primitive
   estimates integrate to the receiver's, to rounding."""
 import math
@@ -120,3 +122,57 @@ def test_large_primitive_map(product):
     integral = sum(p["incoming_flux"][0] for p in prims) * cell
     assert total > 0
     assert integral == pytest.approx(total, rel=1e-9)
+
+
+def test_failure_limit_stops_the_work_fetch(product, oracle):
+    """src/ssol_solver.c:1229, 1240-1248: once max_failed_count paths have
+    failed, no new realisation is scheduled; the call returns RES_BAD_OP with
+    an estimator counting only what ran. Every path of this scene fails."""
+    n = 4_000_000
+    for lib in (product, oracle):
+        s = _failing_scene(lib)
+        e = s.solve(n, seed=3, max_failed=10, check=False)
+        assert e is not None and e.res == P.RES_BAD_OP
+        failed, ran = e.count("failed_count"), e.count("realisation_count")
+        assert failed >= 10
+        assert failed + ran < n // 4, (failed, ran)
+    # no limit reached: every realisation runs
+    s = _failing_scene(product)
+    e = s.solve(50000, seed=3, max_failed=1 << 40, check=False)
+    assert e.res == P.RES_OK
+    assert e.count("failed_count") == 50000 and e.count("realisation_count") == 0
+
+
+def test_host_abort_of_a_running_plan(product):
+    """ssol_b200_plan_abort while a long launch runs: its warps stop taking
+    realisations within milliseconds, ssol_b200_plan_finish returns
+    RES_BAD_OP with the estimator of what ran, and a reset clears it."""
+    import time
+    s, h = W.single_mirror(product)
+    plan = P.C.c_void_p()
+    product.call("ssol_b200_plan_create", s.scn, None, P.C.byref(plan))
+    rng = s.rng(seed=4)
+    n = 8_000_000_000
+    t0 = time.perf_counter()
+    product.call("ssol_b200_plan_launch", plan, rng, 0, n, None)
+    time.sleep(0.05)
+    product.call("ssol_b200_plan_abort", plan)
+    est = P.C.c_void_p()
+    res = product.raw("ssol_b200_plan_finish", plan, rng, n, 0, None, P.C.byref(est))
+    dt = time.perf_counter() - t0
+    e = P.Estimator(s, est, res)
+    assert res == P.RES_BAD_OP
+    ran = e.count("realisation_count")
+    assert 0 < ran < n // 2, ran
+    assert dt < 3.0, dt
+    g = e.globals()
+    assert g["cos_factor"][0] > 0
+    del e
+    product.call("ssol_b200_plan_reset", plan, None)
+    product.call("ssol_b200_plan_launch", plan, rng, 0, 100000, None)
+    est = P.C.c_void_p()
+    res = product.raw("ssol_b200_plan_finish", plan, rng, 100000, 0, None, P.C.byref(est))
+    e = P.Estimator(s, est, res)
+    assert res == P.RES_OK and e.count("realisation_count") == 100000
+    del e
+    product.raw("ssol_b200_plan_ref_put", plan)
