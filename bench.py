@@ -15,7 +15,9 @@ e2e:   the same metric through the public C API, `ssol_solve` per step:
        on all host cores, each step a bounded sample of the same workload.
 Multi-GPU (torchrun): each rank traces a disjoint range of realisations of
 the same scene (weak scaling, no collective on the data path); the time is
-the max over ranks.
+the max over ranks. After the timed region the ranks' tally vectors are
+all-reduced in place over NCCL (the one collective), so that the line's
+estimate is that of all ranks' realisations.
 """
 import argparse
 import json
@@ -334,8 +336,19 @@ def run_b200(args):
         t = torch.tensor([ms, kernel_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, kernel_ms = float(t[0]), float(t[1])
+    # The one collective of the multi-GPU path: each rank's tally vectors
+    # (disjoint realisation ranges of one scene) all-reduced in place over
+    # NCCL, outside the timed region, so that every rank's plan then holds
+    # the tallies of all realisations and builds their merged estimator
+    merged_n = args.steps * n
+    if dist:
+        sums, counts = (torch.as_tensor(x, device="cuda") for x in P.plan_tallies(lib, plan))
+        dist.all_reduce(sums)
+        dist.all_reduce(counts)
+        torch.cuda.synchronize()
+        merged_n = args.steps * n * world
     est = P.C.c_void_p()
-    res = lib.raw("ssol_b200_plan_finish", plan, rng, args.steps * n, 0, sp, P.C.byref(est))
+    res = lib.raw("ssol_b200_plan_finish", plan, rng, merged_n, 0, sp, P.C.byref(est))
     e = P.Estimator(s, est, res)
     st = e.stats()
     g = e.globals()
@@ -430,7 +443,10 @@ def run_b200(args):
         "precision_vs_fp64": prec,
         "estimate": {"absorbed_by_receivers_W": g["absorbed_by_receivers"][0],
                      "rel_se": g["absorbed_by_receivers"][2] / max(1e-30,
-                                                                  g["absorbed_by_receivers"][0])},
+                                                                  g["absorbed_by_receivers"][0]),
+                     "realisations": merged_n,
+                     "what": ("merged over the ranks: plan tallies all-reduced over NCCL"
+                              if dist else "this GPU's plan")},
     }
     if rank == 0 and not args.no_cpu:
         try:

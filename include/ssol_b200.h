@@ -83,14 +83,15 @@ SSOL_API res_T ssol_b200_plan_ref_put(struct ssol_b200_plan* plan);
 SSOL_API res_T ssol_b200_plan_reset
   (struct ssol_b200_plan* plan, void* stream);
 /* Host-side stop of a long solve, from any thread: the plan's running and
- * queued launches take no new realisations (paths in flight finish; the
- * request is read by the kernels' work fetch through host memory mapped into
- * the device's address space, so it takes effect within a few milliseconds).
- * It stays until ssol_b200_plan_reset. ssol_b200_plan_finish then builds the
- * estimator of the realisations that ran (realisation count below the one
- * asked for) and returns RES_BAD_OP, as the reference's solve returns the
- * error that stopped its loop with a valid estimator
- * (src/ssol_solver.c:1229, 1339). */
+ * queued launches take no new realisations (paths in flight finish). The
+ * call copies a flag into the plan's device tallies on a stream of its own
+ * (a copy-engine transfer, which runs beside the plan's kernels) and
+ * returns once it has landed; the kernels' work fetch polls it, so it takes
+ * effect within microseconds. It stays until ssol_b200_plan_reset.
+ * ssol_b200_plan_finish then builds the estimator of the realisations that
+ * ran (realisation count below the one asked for) and returns RES_BAD_OP, as
+ * the reference's solve returns the error that stopped its loop with a valid
+ * estimator (src/ssol_solver.c:1229, 1339). */
 SSOL_API res_T ssol_b200_plan_abort(struct ssol_b200_plan* plan);
 /* Enqueue realisations [first, first + count) of the streams keyed by `rng`;
  * tallies accumulate. Asynchronous. */
@@ -105,6 +106,31 @@ SSOL_API res_T ssol_b200_plan_finish
    void* stream, struct ssol_estimator** estimator);
 SSOL_API res_T ssol_b200_plan_get_stats
   (const struct ssol_b200_plan* plan, struct ssol_b200_stats* stats);
+
+/* Tallies across GPUs. The reference merges its per-thread sums inside
+ * ssol_solve (src/ssol_solver.c:1254-1333); several GPUs tracing disjoint
+ * realisations of one scene merge theirs the same way, by adding them.
+ * ssol_b200_plan_get_tallies gives device pointers to the plan's FP64 sums
+ * (`nsums` doubles: sum w and sum w^2 of every estimate) and its 64-bit
+ * counts (`ncounts`: samples per sampled instance, failures, launch
+ * counters). Adding the vectors of the plans of one scene element-wise, for
+ * instance by an in-place all-reduce over their GPUs, leaves in each the
+ * tallies of all their realisations; ssol_b200_plan_finish with the total
+ * realisation count then builds the merged estimator. */
+SSOL_API res_T ssol_b200_plan_get_tallies
+  (struct ssol_b200_plan* plan, double** sums, size_t* nsums, uint64_t** counts,
+   size_t* ncounts);
+/* The same vectors on the host, where no GPU is needed: their sizes for a
+ * scene, and the estimator of `realisations_count` realisations of `scn`
+ * built from (merged) host copies, with ssol_b200_plan_finish's rules
+ * (failure limit, RNG end state). RES_BAD_ARG if the sizes do not match the
+ * scene. */
+SSOL_API res_T ssol_b200_tallies_size
+  (struct ssol_scene* scn, size_t* nsums, size_t* ncounts);
+SSOL_API res_T ssol_b200_estimator_create_from_tallies
+  (struct ssol_scene* scn, const struct ssp_rng* rng, const uint64_t realisations_count,
+   const size_t max_failed_count, const double* sums, const size_t nsums,
+   const uint64_t* counts, const size_t ncounts, struct ssol_estimator** estimator);
 
 /* Autotuner: times `trial_paths` realisations of `scn` for every launch
  * shape in {block 128, 256} x {register budget 1, 2, 3 blocks per SM} x
@@ -167,6 +193,31 @@ struct ssol_b200_batch;
 
 SSOL_API res_T ssol_b200_batch_create
   (struct ssol_scene* const* scenes, const size_t nscenes,
+   const struct ssol_b200_options* options, struct ssol_b200_batch** batch);
+/* A tracking field over several sun positions, as one batch built on the
+ * device: item i is `scn` with its sun's direction and DNI set to suns[i]
+ * (its sunshape and spectrum kept) and every listed heliostat turned to
+ * track that sun. A heliostat instance keeps its translation p and gets the
+ * rotation whose columns are x, y, n: n the unit bisector of the direction
+ * to the sun (-direction, normalised as ssol_sun_set_direction does) and the
+ * unit direction from p to its aim point (aim_points, 3 per heliostat); x
+ * the unit vector of up x n, up = +z (+x when n is vertical); y = n x x.
+ * Its object's mirror normal is thus its local +z. The scene is snapshot
+ * once on the host; per item the device rewrites the heliostats' triangles
+ * and sampled triangles, in the arithmetic and rounding of a host snapshot
+ * of the re-aimed scene, and refits the BVH built for `scn` (the tree keeps
+ * its topology; every child box is recomputed). Heliostats must be mesh
+ * instances of `scn`, and the scene must have no vertex normals and no
+ * shaders baked per vertex (RES_BAD_ARG otherwise). The other batch calls
+ * apply; finish returns one estimator per sun. */
+struct ssol_b200_sun_position {
+  double direction[3]; /* from the sun toward the scene */
+  double dni; /* W/m^2, > 0 */
+};
+SSOL_API res_T ssol_b200_batch_create_tracking
+  (struct ssol_scene* scn, struct ssol_instance* const* heliostats,
+   const size_t nheliostats, const double* aim_points,
+   const struct ssol_b200_sun_position* suns, const size_t nsuns,
    const struct ssol_b200_options* options, struct ssol_b200_batch** batch);
 SSOL_API res_T ssol_b200_batch_ref_get(struct ssol_b200_batch* batch);
 SSOL_API res_T ssol_b200_batch_ref_put(struct ssol_b200_batch* batch);

@@ -50,26 +50,37 @@ def _run(cmd, log):
 
 
 def build(verbose=False):
-    """Build the library if needed; return its path."""
+    """Build the library if needed; return its path. The translation units
+    compile in parallel (the device code is split so that its template
+    instances spread over several nvcc runs)."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(BUILD, exist_ok=True)
     headers = _headers()
     objs = []
     log = []
+    jobs = []
     for name in sorted(os.listdir(CSRC)):
         src = os.path.join(CSRC, name)
-        if name.endswith(".cu"):
-            obj = os.path.join(BUILD, name + ".o")
-            if _stale(obj, [src] + headers):
-                out = _run([NVCC] + NVCC_FLAGS + ["-c", src, "-o", obj], log)
-                with open(os.path.join(BUILD, name + ".ptxas.txt"), "w") as f:
-                    f.write(out)
-        elif name.endswith(".cpp"):
-            obj = os.path.join(BUILD, name + ".o")
-            if _stale(obj, [src] + headers):
-                _run(["g++"] + CXX_FLAGS + ["-c", src, "-o", obj], log)
-        else:
+        if not name.endswith((".cu", ".cpp")):
             continue
+        obj = os.path.join(BUILD, name + ".o")
         objs.append(obj)
+        if _stale(obj, [src] + headers):
+            jobs.append((name, src, obj))
+
+    def compile_one(job):
+        name, src, obj = job
+        if name.endswith(".cu"):
+            out = _run([NVCC] + NVCC_FLAGS + ["-c", src, "-o", obj], None)
+            with open(os.path.join(BUILD, name + ".ptxas.txt"), "w") as f:
+                f.write(out)
+            return out
+        return _run(["g++"] + CXX_FLAGS + ["-c", src, "-o", obj], None)
+
+    if jobs:
+        workers = max(1, min(len(jobs), os.cpu_count() or 1))
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            log.extend(ex.map(compile_one, jobs))
     if _stale(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs +
              ["-Xcompiler", "-fPIC", "-lpthread", "-ldl", "-lrt"], log)

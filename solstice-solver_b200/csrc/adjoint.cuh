@@ -1,7 +1,7 @@
 /*
  * adjoint.cuh - ssol_solve_adjoint: gradients of a receiver flux objective
  * with respect to the aim angles of heliostats (no counterpart in the
- * reference). Included by kernels.cu inside namespace ssolb, where the
+ * reference). Included by kernels_aux.cu inside namespace ssolb, where the
  * sampling, tracing and shading helpers live.
  *
  * Objective. Only first-bounce paths count: a realisation sampled on a

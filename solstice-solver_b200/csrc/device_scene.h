@@ -188,7 +188,16 @@ template<typename R> struct alignas(16) DSampTri {
   int32_t pad;
 };
 
-/* Counters for the roofline model (see kernels.cu) */
+/* Scene features a kernel variant handles (set per launch from the
+ * snapshot): a variant without a feature drops its code from the hot loop */
+enum : int32_t {
+  FEAT_QUADRIC = 1, /* punched quadric patches */
+  FEAT_DIELECTRIC = 2, /* dielectric or thin-dielectric materials */
+  FEAT_ATTRIBUTES = 4, /* per-triangle shading attributes (DScene::tshade) */
+  FEAT_ALL = 7
+};
+
+/* Counters for the roofline model (see kernels_device.cuh) */
 struct DStats {
   unsigned long long rays;
   unsigned long long node_visits;
@@ -255,20 +264,21 @@ struct DTallies {
   double* prim; /* nprim_slots x NRCV_Q x 2 */
   unsigned long long* nb_samples; /* nsampled */
   unsigned long long* counters; /* [0] failed, [1] killed, [2] overflow,
-                                   [3] work counter, [4] stop word */
+                                   [3] work counter, [4] stop word,
+                                   [5] abort word */
   DStats* stats;
 };
 
 /* Early stop of a plain launch (src/ssol_solver.c:1229, 1240-1248): once
  * `max_failed` paths have failed, the kernel sets the device word `stop`
- * and its warps take no new realisations; `abort` (host memory mapped into
- * the device's address space, or null) is a word the host may set at any
- * time for the same effect. Paths in flight always finish. `stop` null
- * disables the failure limit. */
+ * and its warps take no new realisations; `abort` (device memory, or null)
+ * is a word the host may set at any time, by a copy on a stream of its own,
+ * for the same effect. Paths in flight always finish. `stop` null disables
+ * the failure limit. */
 struct DControl {
   unsigned long long max_failed;
   unsigned long long* stop;
-  const volatile unsigned int* abort;
+  const unsigned long long* abort;
 };
 
 /* Path tracking (ssol_path_tracker): the realisations of launch index

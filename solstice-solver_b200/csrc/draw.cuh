@@ -2,7 +2,7 @@
  * draw.cuh - the preview renderers behind ssol_draw_draft and ssol_draw_pt
  * (src/ssol_draw.c, src/ssol_draw_draft.c, src/ssol_draw_pt.c) as CUDA
  * kernels that write a device image: width x height pixels of 3 doubles,
- * row after row. Included by kernels.cu, whose ray casting (trace_ray with
+ * row after row. Included by kernels_aux.cu, whose ray casting (trace_ray with
  * the hit filter's "discard virtual materials" mode), Philox streams,
  * wavelength sampler, media and shader tables they share.
  *

@@ -465,6 +465,8 @@ void quadric_z_range(const ssol_shape* s, double& zlo, double& zhi)
 
 } /* namespace */
 
+void sun_frame(const double dir[3], double out[9]) { basis(dir, out); }
+
 void build_alias(const std::vector<double>& w, std::vector<float>& prob,
                  std::vector<int32_t>& alias)
 {
@@ -695,6 +697,8 @@ static res_T flatten_impl
         const bool has_n = !shape->nrm.empty();
         const bool attrs = has_n || bake_side[0] || bake_side[1];
         if(attrs) need_tshade = true;
+        out.meta.meshes.push_back({inst, shape, first_gid, ntris,
+                                   inst->sample ? (int)out.samp.size() : -1});
         for(int t = 0; t < ntris; ++t) {
           double v[3][3];
           float vf[3][3];
@@ -941,6 +945,13 @@ static res_T flatten_impl
 
   build_alias(samp_area, out.alias_prob, out.alias_idx);
   if(need_tshade) out.tshade = std::move(tsh);
+  /* Features the kernel variant must handle */
+  out.meta.features = 0;
+  if(!out.quads.empty()) out.meta.features |= FEAT_QUADRIC;
+  for(const DMaterial& d : out.mtls)
+    if(d.type == MTL_DIELECTRIC || d.type == MTL_THIN_DIELECTRIC)
+      out.meta.features |= FEAT_DIELECTRIC;
+  if(!out.tshade.empty()) out.meta.features |= FEAT_ATTRIBUTES;
 
   /* Bounding box of the ray-traced geometry (src/ssol_solver.c:563-570 uses
    * the scene view's box for the tracked segments to and from infinity) */

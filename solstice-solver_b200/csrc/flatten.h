@@ -38,6 +38,16 @@ struct FlatMeta {
   double sampled_area_proxy = 0;
   size_t scene_bytes = 0; /* bytes uploaded to the device */
   double aabb_lo[3] = {0, 0, 0}, aabb_hi[3] = {0, 0, 0}; /* ray-traced geometry */
+  int features = 0; /* FEAT_* bits of the snapshot (kernel variant) */
+  /* Where each (instance, mesh shaded shape) landed: its triangles
+   * [tri_first, tri_first + ntris) and, for sampled instances, its sampled
+   * triangles from samp_first (-1 otherwise), in the same order */
+  struct MeshRange {
+    const ssol_instance* inst;
+    const ssol_shape* shape;
+    int tri_first, ntris, samp_first;
+  };
+  std::vector<MeshRange> meshes;
 };
 
 template<class R> struct FlatScene {
@@ -79,6 +89,10 @@ res_T flatten_scene
 res_T flatten_scene
   (ssol_scene* scn, const BvhBuildParams& bvh, FlatScene<double>& out,
    bool for_draw = false);
+
+/* The sun's frame as a snapshot stores it (columns X, Y, dir), from its
+ * unit direction */
+void sun_frame(const double dir[3], double out[9]);
 
 /* Vose's alias method over non-negative weights (deterministic) */
 void build_alias(const std::vector<double>& w, std::vector<float>& prob,

@@ -1,12 +1,14 @@
 /*
  * kernels.h - host-callable launchers of the realisation kernel
- * (kernels.cu). Plain C++ types only, so that host code compiled by the
+ * (kernels_*.cu). Plain C++ types only, so that host code compiled by the
  * system C++ compiler can call them.
  */
 #ifndef SSOL_B200_KERNELS_H
 #define SSOL_B200_KERNELS_H
 
 #include "device_scene.h"
+
+#include <stddef.h>
 
 namespace ssolb {
 
@@ -22,10 +24,13 @@ struct LaunchConfig {
   bool coherent = true; /* plain launches of at least 2^24 realisations run
                          * in the order of their sampled primitives */
   /* Plain launches: stop handing out realisations once this many paths
-   * have failed (~0: never), or once the host sets *abort_word (mapped host
-   * memory, may be null) */
+   * have failed (~0: never), or once the host sets the tallies' abort word
+   * (when `abortable`) */
   unsigned long long max_failed = ~0ull;
-  const unsigned int* abort_word = nullptr;
+  bool abortable = false;
+  /* FEAT_* bits the scene needs; the launch picks the smallest variant
+   * that covers them */
+  int features = FEAT_ALL;
 };
 
 /* Enqueue the realisations [first, first + count) of the stream keyed by
@@ -76,6 +81,33 @@ int launch_batch_noalloc_f64
    const unsigned long long* h_firsts, const LaunchConfig& cfg, void* stream);
 int launch_batch_f64(const BatchLaunch<double>& b, const LaunchConfig& cfg,
                      void* stream);
+
+/* Tracking batches (one snapshot, one item per sun position): per item,
+ * each tracked heliostat turns toward the item's sun, its triangles and
+ * sampled triangles are rewritten, and the BVH is refitted. Device arrays:
+ * helio (per heliostat: position, aim point), to_sun (per item: unit vector
+ * toward the sun), per tracked triangle its heliostat, its index in tris, its
+ * index in samp (-1 if not sampled) and its 9 local vertex coordinates; the
+ * items' tris, samp and nodes arrays (item i at base + i x stride elements,
+ * already holding copies of the snapshot's); the BVH's node indices grouped
+ * by depth, deepest first (level_first: nlevels + 1 offsets). */
+struct TrackArgs {
+  int nitems, ntracked, nlevels;
+  const double* helio;
+  const double* to_sun;
+  const int32_t* tri_helio;
+  const int32_t* tri_index;
+  const int32_t* tri_samp;
+  const double* local;
+  void* tris; size_t tri_stride;
+  void* samp; size_t samp_stride;
+  void* nodes; size_t node_stride;
+  const uint32_t* primrefs;
+  const int32_t* level_nodes;
+  const int32_t* level_first;
+};
+int launch_track_f32(const TrackArgs& A, void* stream);
+int launch_track_f64(const TrackArgs& A, void* stream);
 
 /* Arguments of the adjoint passes (adjoint.cuh). Device pointers: inst_slot
  * (parameter slot per instance, -1 if none), axes (per slot: centre, e_x,

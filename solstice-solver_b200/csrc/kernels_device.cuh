@@ -1,5 +1,9 @@
 /*
- * kernels.cu - the sm_100a realisation loop of `ssol_solve`.
+ * kernels_device.cuh - device code of the sm_100a realisation loop of
+ * `ssol_solve`, and the templates of its host launchers. Included by the
+ * kernels_*.cu translation units, each of which instantiates some of the
+ * launchers, so that they compile in parallel.
+ *
  *
  * One thread traces whole optical paths, persistent over a grid-stride range
  * of realisations. Per path it restates, on the flat device scene of
@@ -24,6 +28,9 @@
  * plain build, double for the all-FP64 build); quadric roots found in FP32 get
  * one FP64 Newton step.
  */
+#ifndef SSOL_B200_KERNELS_DEVICE_CUH
+#define SSOL_B200_KERNELS_DEVICE_CUH
+
 #include "device_scene.h"
 #include "kernels.h"
 #include "philox.h"
@@ -197,7 +204,7 @@ __device__ __forceinline__ V3<R> sun_local_to_world(const DScene<R>& S, V3<R> p)
 /* Buie zenith angle by rejection (src/ssol_ranst_sun_dir.c:177-195); the
  * draws of attempt k come from event 2 + k of the primary domain */
 template<class R>
-__device__ __noinline__ double buie_theta(const DScene<R>& S, const Rng& rng)
+__device__ __noinline__ double buie_theta(const DScene<R>& S, const Rng rng)
 {
   const double thetaSD = S.buie[0], dCSSD = S.buie[1], gamma = S.buie[2];
   const double ek1000g = S.buie[3], alpha = S.buie[4];
@@ -589,7 +596,7 @@ constexpr int SMEM_STACK = 8;
 /* Closest accepted hit, or the first accepted hit when `any` (shadow rays).
  * Deferred node i < SMEM_STACK of this thread is stack[i * stride] in shared
  * memory, deeper ones go to `spill`. */
-template<class R>
+template<class R, int FEAT = FEAT_ALL>
 __device__ bool trace_ray
   (const DScene<R>& S, V3<R> o, V3<R> d, R tmin, const SelfInfo& self,
    bool any, Hit<R>& best, Counters& cnt, int* stack, int stride)
@@ -628,7 +635,7 @@ __device__ bool trace_ray
         for(int p = 0; p < N.count[k]; ++p) {
           const uint32_t ref = N.count[k] == 1 ? (uint32_t)N.child[k]
                                                : S.primrefs[N.child[k] + p];
-          if(primref_kind(ref) == PRIM_TRIANGLE) {
+          if(!(FEAT & FEAT_QUADRIC) || primref_kind(ref) == PRIM_TRIANGLE) {
             ++cnt.tris;
             test_triangle(S, (int)primref_index(ref), o, d, sh, tmin, eps,
                           self, best, found);
@@ -716,26 +723,48 @@ __device__ __forceinline__ V3<R> local_to(V3<R> n, R x, R y, R z)
   return b1 * x + b2 * y + n * z;
 }
 
-/* Returns false on an inconsistent medium (RES_BAD_OP) */
-template<class R>
-__device__ __noinline__ bool shade
-  (const DScene<R>& S, const Rng& rng, uint32_t scatter, int mtl_idx,
-   int medium, double wl, V3<R> wo, V3<R> Ng, R& prop, V3<R>& out,
-   int& type, int& next_medium, int gid, int side, const double* ps, int stride)
+/* One BSDF sample: the propagated fraction, the outgoing direction, the
+ * sampled component (BXDF_*, 0 if none) and the medium beyond; `ok` false
+ * on an inconsistent medium (RES_BAD_OP). Returned by value, and the random
+ * stream passed by value, so that nothing of the caller's state has to
+ * live in memory across the call. */
+template<class R> struct Scatter {
+  V3<R> out;
+  R prop;
+  int type;
+  int next_medium;
+  bool ok;
+};
+
+template<class R, int FEAT = FEAT_ALL>
+__device__ __noinline__ Scatter<R> shade
+  (const DScene<R>& S, const Rng rng, uint32_t scatter, int mtl_idx,
+   int medium, double wl, V3<R> wo, V3<R> Ng, int gid, int side, const double* ps,
+   int stride)
 {
   const DMaterial m = S.mtls[mtl_idx];
+  Scatter<R> res;
+  R& prop = res.prop;
+  V3<R>& out = res.out;
+  int& type = res.type;
+  int& next_medium = res.next_medium;
+  res.ok = true;
+  out = mk(R(0), R(0), R(0));
   prop = R(0);
   type = 0;
   next_medium = medium;
   /* src/ssol_material.c:97-101 */
-  if(m.type == MTL_DIELECTRIC && medium != m.out_medium) return false;
+  if((FEAT & FEAT_DIELECTRIC) && m.type == MTL_DIELECTRIC && medium != m.out_medium) {
+    res.ok = false;
+    return res;
+  }
   /* Shading normal: the interpolated vertex normal turned toward the
    * incoming side, else Ng (src/ssol_material.c:630-654); shader values
    * baked per vertex where the material varies over the mesh */
   V3<R> N = Ng;
   int bake = -1;
   R b1 = R(0), b2 = R(0);
-  if(S.tshade && gid >= 0) {
+  if((FEAT & FEAT_ATTRIBUTES) && S.tshade && gid >= 0) {
     const float2 uv = get_uv(ps, stride);
     b1 = (R)uv.x;
     b2 = (R)uv.y;
@@ -752,7 +781,7 @@ __device__ __noinline__ bool shade
     }
   }
   const R cos_i = dot(wo, N);
-  if(!(cos_i > R(0))) return true;
+  if(!(cos_i > R(0))) return res;
   const U32x4 r = rng.get(scatter, RNG_SCATTER);
   switch(m.type) {
     case MTL_MIRROR: {
@@ -800,6 +829,7 @@ __device__ __noinline__ bool shade
       break;
     }
     case MTL_DIELECTRIC: {
+      if(!(FEAT & FEAT_DIELECTRIC)) break;
       const R eta_i = (R)data_value(S, S.media[m.out_medium].refractive_index, wl);
       const R eta_t = (R)data_value(S, S.media[m.in_medium].refractive_index, wl);
       const R eta = eta_i / eta_t;
@@ -821,6 +851,7 @@ __device__ __noinline__ bool shade
       break;
     }
     case MTL_THIN_DIELECTRIC: {
+      if(!(FEAT & FEAT_DIELECTRIC)) break;
       const R eta_i = (R)data_value(S, S.media[m.out_medium].refractive_index, wl);
       const R eta_t = (R)data_value(S, S.media[m.slab_medium].refractive_index, wl);
       const R alpha = (R)data_value(S, S.media[m.slab_medium].extinction, wl);
@@ -853,7 +884,7 @@ __device__ __noinline__ bool shade
   if((cos_out > R(0) && (type & BXDF_TRANSMISSION))
   || (cos_out < R(0) && (type & BXDF_REFLECTION)))
     prop = R(0);
-  return true;
+  return res;
 }
 
 /*******************************************************************************
@@ -875,40 +906,34 @@ enum : int {
  * kept in local memory: only paths reaching several receivers touch them */
 constexpr int MAX_EXTRA = 7;
 
-/* 10 receiver quantities from the 6 accumulated ones, in MC_RECEIVER_DATA
- * order (src/ssol_solver.c:735-755) */
-__device__ __forceinline__ void expand10(const double v[6], double f,
-                                         double out[NRCV_Q])
-{
-  out[0] = f * v[0];
-  out[1] = f * v[1];
-  out[2] = f * v[2];
-  out[3] = f * (v[2] - v[0]);
-  out[4] = f * (v[1] - v[0]);
-  out[5] = f * v[3];
-  out[6] = f * v[4];
-  out[7] = f * v[5];
-  out[8] = f * (v[5] - v[3]);
-  out[9] = f * (v[4] - v[3]);
-}
-
 __device__ __forceinline__ void red_add(double* p, double v)
 {
   if(v != 0.0) atomicAdd(p, v);
 }
 
-__device__ __noinline__ void commit10(double* dst, const double v[6], double f)
+/* (w, w^2) of the 10 receiver quantities of one path, from its 6
+ * accumulated values (MC_RECEIVER_DATA order, src/ssol_solver.c:735-755:
+ * incoming, incoming if no atmosphere loss, if no field loss, lost in the
+ * field, lost in the atmosphere, then the same 5 absorbed), added to dst. The values travel as scalars, so that
+ * none of them goes through local memory. */
+static __device__ __noinline__ void commit10
+  (double* dst, double v0, double v1, double v2, double v3, double v4, double v5,
+   double f)
 {
-  double q[NRCV_Q];
-  expand10(v, f, q);
-#pragma unroll 1
+  const double q[NRCV_Q] = {f * v0, f * v1, f * v2, f * (v2 - v0), f * (v1 - v0),
+                            f * v3, f * v4, f * v5, f * (v5 - v3), f * (v4 - v3)};
+#pragma unroll
   for(int k = 0; k < NRCV_Q; ++k) {
     red_add(dst + 2 * k, q[k]);
     red_add(dst + 2 * k + 1, q[k] * q[k]);
   }
 }
+__device__ __forceinline__ void commit10(double* dst, const double v[6], double f)
+{
+  commit10(dst, v[0], v[1], v[2], v[3], v[4], v[5], f);
+}
 
-__device__ __noinline__ void flush_racc(double* dst, const double* racc)
+static __device__ __noinline__ void flush_racc(double* dst, const double* racc)
 {
 #pragma unroll 1
   for(int k = 0; k < 2 * NRCV_Q; ++k) red_add(dst + k, racc[k]);
@@ -950,7 +975,7 @@ __device__ __forceinline__ int sample_prim(const DScene<R>& S, const U32x4& r0)
 
 /* point_init (src/ssol_solver.c:207-352) up to the shadow ray; `draw` is the
  * realisation's primary draw when the caller already has it */
-template<class R>
+template<class R, int FEAT = FEAT_ALL>
 __device__ __forceinline__ void init_path
   (const DScene<R>& S, const Rng& rng, PathState<R>& p, double* ps, int stride,
    const U32x4* draw = nullptr)
@@ -963,7 +988,7 @@ __device__ __forceinline__ void init_path
   const R b1 = sa - b2;
   V3<R> pos = ld3(st.v0) + ld3(st.e1) * b1 + ld3(st.e2) * b2;
   const V3<R> nproxy = ld3(st.n);
-  if(S.tshade) put_uv(ps, stride, (float)b1, (float)b2);
+  if((FEAT & FEAT_ATTRIBUTES) && S.tshade) put_uv(ps, stride, (float)b1, (float)b2);
 
   const U32x4 r1 = rng.get(1u, RNG_PRIMARY);
   const V3<R> dir = sample_sun_dir(S, rng, r1);
@@ -971,7 +996,7 @@ __device__ __forceinline__ void init_path
 
   const DShadedInst si = S.sinsts[st.sinst];
   V3<R> N = nproxy;
-  if(si.is_punched) {
+  if((FEAT & FEAT_QUADRIC) && si.is_punched) {
     /* punched_shape_project_point (src/ssol_shape.c:1408-1447) */
     const DQuadric<R>& Q = S.quads[si.quadric];
     V3<R> pl = xform_point(Q.w2l, pos);
@@ -996,7 +1021,8 @@ __device__ __forceinline__ void init_path
 
   const DMaterial m = S.mtls[si.mtl[side - 1]];
   p.medium = S.air_medium;
-  if(m.type == MTL_DIELECTRIC || m.type == MTL_THIN_DIELECTRIC)
+  if((FEAT & FEAT_DIELECTRIC)
+  && (m.type == MTL_DIELECTRIC || m.type == MTL_THIN_DIELECTRIC))
     p.medium = side == 1 ? m.in_medium : m.out_medium;
 
   p.sinst = st.sinst;
@@ -1053,7 +1079,7 @@ __device__ __forceinline__ void add_entry
 /* One surface interaction (src/ssol_solver.c:939-1011): extinction of the
  * incoming segment, virtual pass-through or BSDF sample, receiver tallies,
  * then either the next ray or the end of the path */
-template<class R>
+template<class R, int FEAT = FEAT_ALL>
 __device__ int interact
   (const DScene<R>& S, const Rng& rng, PathState<R>& p, V3<R> pos, V3<R> dir,
    uint32_t& bounces, unsigned long long max_segments, double* ps, int stride,
@@ -1077,13 +1103,14 @@ __device__ int interact
     kabs = 0;
     out0 = inc0; out1 = inc1; out2 = inc2;
   } else {
-    R prop;
-    V3<R> ndir;
-    int type;
     ++bounces;
-    if(!shade(S, rng, p.scatter++, si.mtl[p.side - 1], p.medium, p.wl, -dir,
-              p.N, prop, ndir, type, out_medium, p.gid, p.side, ps, stride))
-      return END_FAIL;
+    const Scatter<R> sc = shade<R, FEAT>(S, rng, p.scatter++, si.mtl[p.side - 1], p.medium,
+                                         p.wl, -dir, p.N, p.gid, p.side, ps, stride);
+    if(!sc.ok) return END_FAIL;
+    const R prop = sc.prop;
+    const V3<R> ndir = sc.out;
+    const int type = sc.type;
+    out_medium = sc.next_medium;
     const double pr = (double)prop;
     kabs = 1.0 - pr;
     out0 = inc0 * pr;
@@ -1123,37 +1150,59 @@ __device__ int interact
   return END_NONE;
 }
 
-/* Commit a finished path: FP64 (w, w^2) of its totals, x 2^score for
- * roulette survivors (src/ssol_solver.c:1087-1108) */
+/* What commit_path reads of a finished path, passed by value so that the
+ * path state itself never has to live in memory across the call */
+struct PathEnd {
+  int end; /* END_* */
+  int samp, score, nent, r0, p0;
+  bool overflow;
+  double w_end; /* weight shadowed (END_SHADOW) or missing (END_MISS) */
+};
+
 template<class R>
-__device__ __noinline__ void commit_path
-  (const DScene<R>& S, const DTallies& T, PathState<R>& p, int end,
-   double* acc, double* ps, int stride, double* smem_rcv, const int* xr,
-   const int* xp, const double (*xv)[6], double* racc = nullptr,
-   int* racc_slot = nullptr, const DControl* ctl = nullptr)
+__device__ __forceinline__ PathEnd path_end(const PathState<R>& p, int end)
 {
-  atomicAdd(&T.nb_samples[p.samp], 1ull);
-  if(p.overflow) end = END_FAIL;
+  PathEnd e;
+  e.end = p.overflow ? END_FAIL : end;
+  e.samp = p.samp;
+  e.score = p.score;
+  e.nent = p.nent;
+  e.r0 = p.r0;
+  e.p0 = p.p0;
+  e.overflow = p.overflow;
+  e.w_end = end == END_MISS && p.virt ? p.inc0 : p.prev[0];
+  return e;
+}
+
+/* Commit a finished path: FP64 (w, w^2) of its totals, x 2^score for
+ * roulette survivors (src/ssol_solver.c:1087-1108). Returns the receiver
+ * side of the thread's running sums `racc` after the commit. */
+template<class R>
+__device__ __noinline__ int commit_path
+  (const DScene<R>& S, const DTallies& T, const PathEnd pe, double* acc,
+   double* ps, int stride, double* smem_rcv, const int* xr, const int* xp,
+   const double (*xv)[6], double* racc, int racc_slot, const DControl* ctl)
+{
+  const int end = pe.end;
+  atomicAdd(&T.nb_samples[pe.samp], 1ull);
   if(end == END_FAIL) {
     /* The failure that reaches the limit stops the launch's work fetch
      * (src/ssol_solver.c:1240-1245) */
     const unsigned long long nf = atomicAdd(&T.counters[0], 1ull) + 1ull;
     if(ctl && ctl->stop && nf >= ctl->max_failed) atomicExch(ctl->stop, 1ull);
-    if(p.overflow) atomicAdd(&T.counters[2], 1ull);
-    return;
+    if(pe.overflow) atomicAdd(&T.counters[2], 1ull);
+    return racc_slot;
   }
   if(end == END_KILL) {
     atomicAdd(&T.counters[1], 1ull);
-    return;
+    return racc_slot;
   }
-  const double f = (double)(1ull << p.score);
-  double g[NGLOBAL];
-  g[G_COS] = ps[PS_COS * stride];
-  g[G_ABS_RCV] = ps[PS_ABS * stride];
-  g[G_SHADOW] = end == END_SHADOW ? p.prev[0] : 0.0;
-  g[G_MISSING] = end == END_MISS ? (p.virt ? p.inc0 : p.prev[0]) : 0.0;
-  g[G_ATM] = ps[PS_ATM * stride];
-  g[G_OTHER] = ps[PS_OTHER * stride];
+  const double f = (double)(1ull << pe.score);
+  const double g[NGLOBAL] = {
+    ps[PS_COS * stride], ps[PS_ABS * stride],
+    end == END_SHADOW ? pe.w_end : 0.0,
+    end == END_MISS ? pe.w_end : 0.0,
+    ps[PS_ATM * stride], ps[PS_OTHER * stride]};
   if(acc) {
 #pragma unroll
     for(int q = 0; q < NGLOBAL; ++q) {
@@ -1164,60 +1213,68 @@ __device__ __noinline__ void commit_path
   }
   {
     const double wc = f * g[G_COS], ws = f * g[G_SHADOW];
-    double* sp = T.samp + (size_t)p.samp * 4;
+    double* sp = T.samp + (size_t)pe.samp * 4;
     red_add(sp + 0, wc);
     red_add(sp + 1, wc * wc);
     red_add(sp + 2, ws);
     red_add(sp + 3, ws * ws);
   }
-  if(p.nent == 0) return;
-  double v0[6];
-  for(int q = 0; q < 6; ++q) v0[q] = ps[(PS_V0 + q) * stride];
+  if(pe.nent == 0) return racc_slot;
   double* rbase = smem_rcv ? smem_rcv : T.rcv;
-  if(p.nent == 1) {
+  if(pe.nent == 1) {
+    const double a0 = ps[(PS_V0 + 0) * stride], a1 = ps[(PS_V0 + 1) * stride];
+    const double a2 = ps[(PS_V0 + 2) * stride], a3 = ps[(PS_V0 + 3) * stride];
+    const double a4 = ps[(PS_V0 + 4) * stride], a5 = ps[(PS_V0 + 5) * stride];
     if(racc) {
       /* The thread's running sums of one receiver side, flushed when the
        * side changes: no atomics while its paths keep reaching it */
-      if(*racc_slot != p.r0) {
-        if(*racc_slot >= 0) flush_racc(rbase + (size_t)*racc_slot * NRCV_Q * 2, racc);
-        *racc_slot = p.r0;
+      if(racc_slot != pe.r0) {
+        if(racc_slot >= 0) flush_racc(rbase + (size_t)racc_slot * NRCV_Q * 2, racc);
+        racc_slot = pe.r0;
+#pragma unroll
         for(int k = 0; k < 2 * NRCV_Q; ++k) racc[k] = 0.0;
       }
-      double q[NRCV_Q];
-      expand10(v0, f, q);
+      const double q[NRCV_Q] = {f * a0, f * a1, f * a2, f * (a2 - a0), f * (a1 - a0),
+                                f * a3, f * a4, f * a5, f * (a5 - a3), f * (a4 - a3)};
+#pragma unroll
       for(int k = 0; k < NRCV_Q; ++k) {
         racc[2 * k] += q[k];
         racc[2 * k + 1] += q[k] * q[k];
       }
     } else {
-      commit10(rbase + (size_t)p.r0 * NRCV_Q * 2, v0, f);
+      commit10(rbase + (size_t)pe.r0 * NRCV_Q * 2, a0, a1, a2, a3, a4, a5, f);
     }
-    commit10(T.samp_rcv + ((size_t)p.samp * S.nrcv + p.r0) * NRCV_Q * 2, v0, f);
-    if(p.p0 >= 0) commit10(T.prim + (size_t)p.p0 * NRCV_Q * 2, v0, f);
-    return;
+    commit10(T.samp_rcv + ((size_t)pe.samp * S.nrcv + pe.r0) * NRCV_Q * 2,
+             a0, a1, a2, a3, a4, a5, f);
+    if(pe.p0 >= 0)
+      commit10(T.prim + (size_t)pe.p0 * NRCV_Q * 2, a0, a1, a2, a3, a4, a5, f);
+    return racc_slot;
   }
+  double v0[6];
+  for(int q = 0; q < 6; ++q) v0[q] = ps[(PS_V0 + q) * stride];
   /* Several entries: sum per receiver side and per primitive before
    * squaring (deferred mc_data semantics) */
-  const int n = p.nent;
+  const int n = pe.nent;
   for(int e = 0; e < n; ++e) {
-    const int re = e == 0 ? p.r0 : xr[e - 1];
+    const int re = e == 0 ? pe.r0 : xr[e - 1];
     bool seen = false;
-    for(int k = 0; k < e && !seen; ++k) seen = (k == 0 ? p.r0 : xr[k - 1]) == re;
+    for(int k = 0; k < e && !seen; ++k) seen = (k == 0 ? pe.r0 : xr[k - 1]) == re;
     if(!seen) {
       double v[6] = {0, 0, 0, 0, 0, 0};
       for(int k = e; k < n; ++k) {
-        if((k == 0 ? p.r0 : xr[k - 1]) != re) continue;
+        if((k == 0 ? pe.r0 : xr[k - 1]) != re) continue;
         for(int q = 0; q < 6; ++q) v[q] += k == 0 ? v0[q] : xv[k - 1][q];
       }
       commit10(rbase + (size_t)re * NRCV_Q * 2, v, f);
-      commit10(T.samp_rcv + ((size_t)p.samp * S.nrcv + re) * NRCV_Q * 2, v, f);
+      commit10(T.samp_rcv + ((size_t)pe.samp * S.nrcv + re) * NRCV_Q * 2, v, f);
     }
-    const int pe = e == 0 ? p.p0 : xp[e - 1];
-    if(pe >= 0) {
+    const int prim = e == 0 ? pe.p0 : xp[e - 1];
+    if(prim >= 0) {
       /* (receiver side, primitive) keys are unique among the entries */
-      commit10(T.prim + (size_t)pe * NRCV_Q * 2, e == 0 ? v0 : xv[e - 1], f);
+      commit10(T.prim + (size_t)prim * NRCV_Q * 2, e == 0 ? v0 : xv[e - 1], f);
     }
   }
+  return racc_slot;
 }
 
 /*******************************************************************************
@@ -1268,13 +1325,14 @@ __device__ __forceinline__ void track_vertex
   ++p.tseq;
 }
 
-template<class R, int MINB, bool TRACK>
+template<class R, int MINB, bool TRACK, int FEAT>
 __global__ void __launch_bounds__(MAX_BLOCK, MINB)
 realisation_kernel
-  (const DScene<R> S, const DTallies T, uint64_t seed, uint64_t first,
-   uint64_t count, unsigned long long max_segments,
-   unsigned long long* next_path, const DTrack tr, const uint4* sorted_draw,
-   const uint32_t* sorted_off, uint32_t seg_mul, const DControl ctl)
+  (const __grid_constant__ DScene<R> S, const __grid_constant__ DTallies T,
+   uint64_t seed, uint64_t first, uint64_t count, unsigned long long max_segments,
+   unsigned long long* next_path, const __grid_constant__ DTrack tr,
+   const uint4* sorted_draw, const uint32_t* sorted_off, uint32_t seg_mul,
+   const __grid_constant__ DControl ctl)
 {
   /* Shared memory: per-thread FP64 global sums [12][blockDim], per-thread
    * path sums [10][blockDim], the receiver-side sums, the first traversal
@@ -1321,18 +1379,17 @@ realisation_kernel
     bool start = false;
     uint64_t off = 0;
     U32x4 r0;
-    /* Early stop: the failure limit's device word at every fetch, the
-     * host's abort word (a read across the bus) every 16th; a halted warp
-     * takes no new realisation and ends once its paths in flight end */
+    /* Early stop: every 8th fetch of the warp reads the stop and abort
+     * words (one L2 sector); a halted warp takes no new realisation and ends
+     * once its paths in flight end */
     bool halt = false;
-    if(need && polled) {
+    if(need && polled && (fetches++ & 7u) == 0u) {
       const int leader = __ffs(need) - 1;
       int h = 0;
       if((int)lane == leader) {
         if(ctl.stop && *(volatile const unsigned long long*)ctl.stop) h = 1;
-        if(ctl.abort && (fetches & 15u) == 0u && *ctl.abort) h = 1;
+        if(ctl.abort && *(volatile const unsigned long long*)ctl.abort) h = 1;
       }
-      ++fetches;
       halt = __shfl_sync(0xffffffffu, h, leader) != 0;
     }
     if(halt) {
@@ -1401,7 +1458,7 @@ realisation_kernel
       rng.i_lo = (uint32_t)id;
       rng.i_hi = (uint32_t)(id >> 32);
       if(!sorted_off) r0 = rng.get(0u, RNG_PRIMARY);
-      init_path(S, rng, p, ps, bd, &r0);
+      init_path<R, FEAT>(S, rng, p, ps, bd, &r0);
       ++npaths;
       if(TRACK) {
         p.tslot = off < tr.npaths ? (int)off : -1;
@@ -1426,7 +1483,7 @@ realisation_kernel
       self.side = p.side;
       self.discard_virtual = shadow;
       self.reversed = shadow;
-      found = trace_ray(S, p.org, p.rd, p.tmin, self, shadow, h, cnt, stack, bd);
+      found = trace_ray<R, FEAT>(S, p.org, p.rd, p.tmin, self, shadow, h, cnt, stack, bd);
     }
 
     int end = END_NONE;
@@ -1478,7 +1535,7 @@ realisation_kernel
           dir = p.rd;
           p.N = normalize(h.n);
           pos = p.org + p.rd * h.t;
-          if(S.tshade && h.gid >= 0) {
+          if((FEAT & FEAT_ATTRIBUTES) && S.tshade && h.gid >= 0) {
             const float2 uv = tri_uv(S, h.gid, pos);
             put_uv(ps, bd, uv.x, uv.y);
           }
@@ -1493,7 +1550,7 @@ realisation_kernel
       }
     }
     if(do_interact)
-      end = interact(S, rng, p, pos, dir, bounces, max_segments, ps, bd, xr, xp, xv);
+      end = interact<R, FEAT>(S, rng, p, pos, dir, bounces, max_segments, ps, bd, xr, xp, xv);
     if(end != END_NONE) {
       if(TRACK && p.tslot >= 0 && end != END_KILL) {
         /* src/ssol_solver.c:931, 1092-1094, 1122-1125; killed paths are not
@@ -1502,7 +1559,8 @@ realisation_kernel
           : (end == END_FAIL || p.overflow) ? 3 : (p.nent > 0 ? 2 : 0);
         tr.path_nv[p.tslot] = (int32_t)p.tseq;
       }
-      commit_path(S, T, p, end, acc, ps, bd, smem_rcv, xr, xp, xv, racc, &racc_slot, &ctl);
+      racc_slot = commit_path(S, T, path_end(p, end), acc, ps, bd, smem_rcv, xr, xp, xv,
+                              racc, racc_slot, &ctl);
       p.phase = PH_NONE;
     }
   }
@@ -1539,7 +1597,7 @@ realisation_kernel
  * tallies; the per-thread FP64 global sums are flushed when a thread moves
  * to another item. The launch's total is prefix[nitems], read from device
  * memory so that a captured CUDA graph replays with new budgets. */
-template<class R, int MINB>
+template<class R, int MINB, int FEAT>
 __global__ void __launch_bounds__(MAX_BLOCK, MINB)
 batch_kernel
   (const DScene<R>* __restrict__ scenes, const DTallies* __restrict__ tallies,
@@ -1653,7 +1711,7 @@ batch_kernel
           const uint64_t id = firsts[it] + (g - prefix[it]);
           rng.i_lo = (uint32_t)id;
           rng.i_hi = (uint32_t)(id >> 32);
-          init_path(scene_of(it), rng, p, ps, bd);
+          init_path<R, FEAT>(scene_of(it), rng, p, ps, bd);
           ++npaths;
         }
       }
@@ -1697,7 +1755,7 @@ batch_kernel
       self.side = p.side;
       self.discard_virtual = shadow;
       self.reversed = shadow;
-      found = trace_ray(S, p.org, p.rd, p.tmin, self, shadow, h, cnt, stack, bd);
+      found = trace_ray<R, FEAT>(S, p.org, p.rd, p.tmin, self, shadow, h, cnt, stack, bd);
     }
 
     int end = END_NONE;
@@ -1741,7 +1799,7 @@ batch_kernel
           dir = p.rd;
           p.N = normalize(h.n);
           pos = p.org + p.rd * h.t;
-          if(S.tshade && h.gid >= 0) {
+          if((FEAT & FEAT_ATTRIBUTES) && S.tshade && h.gid >= 0) {
             const float2 uv = tri_uv(S, h.gid, pos);
             put_uv(ps, bd, uv.x, uv.y);
           }
@@ -1754,7 +1812,7 @@ batch_kernel
       }
     }
     if(do_interact)
-      end = interact(S, rng, p, pos, dir, bounces, max_segments, ps, bd, xr, xp, xv);
+      end = interact<R, FEAT>(S, rng, p, pos, dir, bounces, max_segments, ps, bd, xr, xp, xv);
     if(end != END_NONE) {
       double* rb = nullptr;
       if(rcvd) {
@@ -1763,7 +1821,8 @@ batch_kernel
       }
       if(racc_item != it) racc_flush();
       racc_item = it;
-      commit_path(S, tallies[it], p, end, acc, ps, bd, rb, xr, xp, xv, racc, &racc_slot);
+      racc_slot = commit_path(S, tallies[it], path_end(p, end), acc, ps, bd, rb, xr, xp, xv,
+                              racc, racc_slot, (const DControl*)nullptr);
       p.phase = PH_NONE;
     }
   }
@@ -1836,7 +1895,7 @@ __global__ void __launch_bounds__(256) presort_count
 }
 
 /* Exclusive prefix sum of the nb histogram bins, one block of 1024 threads */
-__global__ void __launch_bounds__(1024) presort_scan
+static __global__ void __launch_bounds__(1024) presort_scan
   (const uint32_t* hist, uint32_t* off, int nb)
 {
   __shared__ uint32_t part[1024];
@@ -1867,7 +1926,7 @@ __global__ void __launch_bounds__(1024) presort_scan
  * realisation */
 constexpr int SCATTER_PER = 16;
 
-__global__ void __launch_bounds__(256) presort_scatter
+static __global__ void __launch_bounds__(256) presort_scatter
   (const uint32_t* keys, const uint4* draws, uint32_t n, uint32_t* off,
    uint4* out_draws, uint32_t* out_off, int nb)
 {
@@ -1900,29 +1959,8 @@ __global__ void __launch_bounds__(256) presort_scatter
   }
 }
 
-/* Per-device pool of the sort's scratch: stream-ordered allocations, so
- * that launches on different streams never share a buffer, kept by the pool
- * between launches */
-static cudaMemPool_t sort_pool(int dev)
-{
-  static cudaMemPool_t pools[64] = {};
-  static std::mutex lock;
-  if(dev < 0 || dev >= 64) return nullptr;
-  std::lock_guard<std::mutex> g(lock);
-  if(!pools[dev]) {
-    cudaMemPoolProps props = {};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = dev;
-    if(cudaMemPoolCreate(&pools[dev], &props) != cudaSuccess) {
-      pools[dev] = nullptr;
-      return nullptr;
-    }
-    uint64_t keep = ~0ull;
-    cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
-  }
-  return pools[dev];
-}
+/* Per-device pool of the sort's scratch (kernels_plain.cu) */
+cudaMemPool_t sort_pool(int dev);
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -1943,10 +1981,10 @@ static void raise_smem_limit(K kernel, int dev)
                           160 * 1024) == cudaSuccess && bit)
     done_mask.fetch_or(bit, std::memory_order_acq_rel);
 }
-template<class R, int MINB, bool TRACK> struct RealisationTag {};
-template<class R, int MINB> struct BatchTag {};
+template<class R, int MINB, bool TRACK, int FEAT> struct RealisationTag {};
+template<class R, int MINB, int FEAT> struct BatchTag {};
 
-template<class R, int MINB, bool TRACK>
+template<class R, int MINB, bool TRACK, int FEAT>
 static int launch_variant
   (const DScene<R>& S, const DTallies& T, uint64_t seed, uint64_t first,
    uint64_t count, const LaunchConfig& cfg, void* stream, const DTrack& tr)
@@ -1961,10 +1999,10 @@ static int launch_variant
   const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block + rcv_doubles)
                       * sizeof(double)
                     + (size_t)SMEM_STACK * block * sizeof(int);
-  raise_smem_limit<RealisationTag<R, MINB, TRACK>>(realisation_kernel<R, MINB, TRACK>, dev);
+  raise_smem_limit<RealisationTag<R, MINB, TRACK, FEAT>>(realisation_kernel<R, MINB, TRACK, FEAT>, dev);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor
-    (&per_sm, realisation_kernel<R, MINB, TRACK>, block, smem);
+    (&per_sm, realisation_kernel<R, MINB, TRACK, FEAT>, block, smem);
   if(per_sm < 1) per_sm = 1;
   uint64_t blocks = cfg.grid_blocks > 0
     ? (uint64_t)cfg.grid_blocks
@@ -1978,11 +2016,11 @@ static int launch_variant
   DControl ctl;
   ctl.max_failed = cfg.max_failed;
   ctl.stop = cfg.max_failed != ~0ull ? T.counters + 4 : nullptr;
-  ctl.abort = cfg.abort_word;
+  ctl.abort = cfg.abortable ? T.counters + 5 : nullptr;
   if(!sort) {
     /* Work counter of this launch: counters[3] */
     cudaMemsetAsync(T.counters + 3, 0, sizeof(unsigned long long), st);
-    realisation_kernel<R, MINB, TRACK><<<(unsigned)blocks, block, smem, st>>>
+    realisation_kernel<R, MINB, TRACK, FEAT><<<(unsigned)blocks, block, smem, st>>>
       (S, T, seed, first, count, cfg.max_segments, T.counters + 3, tr, nullptr,
        nullptr, 1u, ctl);
     return (int)cudaGetLastError();
@@ -2022,12 +2060,31 @@ static int launch_variant
     while(nseg > 1 && std::gcd(mul, nseg) != 1u) mul += 2;
     if(nseg <= 1) mul = 1;
     cudaMemsetAsync(T.counters + 3, 0, sizeof(unsigned long long), st);
-    realisation_kernel<R, MINB, TRACK><<<(unsigned)nb, block, smem, st>>>
+    realisation_kernel<R, MINB, TRACK, FEAT><<<(unsigned)nb, block, smem, st>>>
       (S, T, seed, first + c0, n, cfg.max_segments, T.counters + 3, tr, sdraws, soff,
        mul, ctl);
   }
   cudaFreeAsync(buf, st);
   return (int)cudaGetLastError();
+}
+
+/* Feature variants of the FP32 kernel: meshes with mirror and matte
+ * materials only, quadrics and dielectrics, or everything (vertex
+ * attributes); the all-FP64 build, for precision checks, has the last one */
+template<class R, int MINB>
+static int launch_features
+  (const DScene<R>& S, const DTallies& T, uint64_t seed, uint64_t first,
+   uint64_t count, const LaunchConfig& cfg, void* stream)
+{
+  const DTrack none = {};
+  if constexpr(sizeof(R) == sizeof(float)) {
+    if(cfg.features == 0)
+      return launch_variant<R, MINB, false, 0>(S, T, seed, first, count, cfg, stream, none);
+    if(!(cfg.features & FEAT_ATTRIBUTES))
+      return launch_variant<R, MINB, false, FEAT_QUADRIC | FEAT_DIELECTRIC>
+        (S, T, seed, first, count, cfg, stream, none);
+  }
+  return launch_variant<R, MINB, false, FEAT_ALL>(S, T, seed, first, count, cfg, stream, none);
 }
 
 /* Register budget variants: at least MINB blocks of 256 threads per SM */
@@ -2036,16 +2093,16 @@ static int launch_impl
   (const DScene<R>& S, const DTallies& T, uint64_t seed, uint64_t first,
    uint64_t count, const LaunchConfig& cfg, void* stream, const DTrack* track)
 {
-  if(track) return launch_variant<R, 2, true>(S, T, seed, first, count, cfg, stream, *track);
-  const DTrack none = {};
+  if(track)
+    return launch_variant<R, 2, true, FEAT_ALL>(S, T, seed, first, count, cfg, stream, *track);
   switch(cfg.min_blocks) {
-    case 1: return launch_variant<R, 1, false>(S, T, seed, first, count, cfg, stream, none);
-    case 3: return launch_variant<R, 3, false>(S, T, seed, first, count, cfg, stream, none);
-    default: return launch_variant<R, 2, false>(S, T, seed, first, count, cfg, stream, none);
+    case 1: return launch_features<R, 1>(S, T, seed, first, count, cfg, stream);
+    case 3: return launch_features<R, 3>(S, T, seed, first, count, cfg, stream);
+    default: return launch_features<R, 2>(S, T, seed, first, count, cfg, stream);
   }
 }
 
-template<class R, int MINB>
+template<class R, int MINB, int FEAT>
 static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg,
                                 void* stream)
 {
@@ -2059,16 +2116,16 @@ static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg
                     + (size_t)SMEM_STACK * block * sizeof(int)
                     + (size_t)(block / 32) * 2 * (2 * NGLOBAL + cfg.rcv_doubles) * sizeof(double)
                     + (size_t)(block / 32) * 2 * sizeof(DScene<R>);
-  raise_smem_limit<BatchTag<R, MINB>>(batch_kernel<R, MINB>, dev);
+  raise_smem_limit<BatchTag<R, MINB, FEAT>>(batch_kernel<R, MINB, FEAT>, dev);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor
-    (&per_sm, batch_kernel<R, MINB>, block, smem);
+    (&per_sm, batch_kernel<R, MINB, FEAT>, block, smem);
   if(per_sm < 1) per_sm = 1;
   const uint64_t blocks = cfg.grid_blocks > 0
     ? (uint64_t)cfg.grid_blocks
     : (uint64_t)nsm * (uint64_t)per_sm * (uint64_t)(cfg.waves > 0 ? cfg.waves : 1);
   cudaMemsetAsync(b.next_path, 0, sizeof(unsigned long long), (cudaStream_t)stream);
-  batch_kernel<R, MINB><<<(unsigned)blocks, block, smem, (cudaStream_t)stream>>>
+  batch_kernel<R, MINB, FEAT><<<(unsigned)blocks, block, smem, (cudaStream_t)stream>>>
     (b.scenes, b.tallies, b.prefix, b.firsts, b.nitems, b.seed, cfg.max_segments,
      b.next_path, b.stats, cfg.rcv_doubles);
   return (int)cudaGetLastError();
@@ -2078,153 +2135,22 @@ template<class R>
 static int launch_batch_impl(const BatchLaunch<R>& b, const LaunchConfig& cfg,
                              void* stream)
 {
+  /* FP32 batches of meshes with mirror and matte materials only get the
+   * smaller variant */
+  if(sizeof(R) == sizeof(float) && cfg.features == 0) {
+    switch(cfg.min_blocks) {
+      case 1: return launch_batch_variant<R, 1, 0>(b, cfg, stream);
+      case 3: return launch_batch_variant<R, 3, 0>(b, cfg, stream);
+      default: return launch_batch_variant<R, 2, 0>(b, cfg, stream);
+    }
+  }
   switch(cfg.min_blocks) {
-    case 1: return launch_batch_variant<R, 1>(b, cfg, stream);
-    case 3: return launch_batch_variant<R, 3>(b, cfg, stream);
-    default: return launch_batch_variant<R, 2>(b, cfg, stream);
+    case 1: return launch_batch_variant<R, 1, FEAT_ALL>(b, cfg, stream);
+    case 3: return launch_batch_variant<R, 3, FEAT_ALL>(b, cfg, stream);
+    default: return launch_batch_variant<R, 2, FEAT_ALL>(b, cfg, stream);
   }
 }
-
-int launch_batch_f32(const BatchLaunch<float>& b, const LaunchConfig& cfg,
-                     void* stream)
-{ return launch_batch_impl<float>(b, cfg, stream); }
-
-int launch_batch_f64(const BatchLaunch<double>& b, const LaunchConfig& cfg,
-                     void* stream)
-{ return launch_batch_impl<double>(b, cfg, stream); }
-
-/* Scratch of the no-allocation batched launch: one file-scope device array
- * holding the budget prefix sums (NOALLOC_MAX_ITEMS + 1 words), the
- * per-item first realisation ids (NOALLOC_MAX_ITEMS words), the work counter
- * and the launch counters (DStats). Every call on a device shares it. */
-constexpr size_t NOALLOC_PREFIX = 0;
-constexpr size_t NOALLOC_FIRSTS = NOALLOC_MAX_ITEMS + 1;
-constexpr size_t NOALLOC_NEXT = 2 * NOALLOC_MAX_ITEMS + 1;
-constexpr size_t NOALLOC_STATS = 2 * NOALLOC_MAX_ITEMS + 2;
-constexpr size_t NOALLOC_WORDS =
-  NOALLOC_STATS + sizeof(DStats) / sizeof(unsigned long long);
-static __device__ __align__(256) unsigned long long
-  g_noalloc_scratch[NOALLOC_WORDS];
-
-/* Device address of the scratch array, resolved once per device with that
- * device current: the host-side name of a __device__ array is a stand-in,
- * not an address a kernel may be given */
-static int noalloc_scratch_address(unsigned long long** out)
-{
-  /* Atomic entries: two host threads may make their first call on a device
-   * at the same time (both then store the same address) */
-  static std::atomic<unsigned long long*> cache[64] = {};
-  int dev = 0;
-  cudaError_t err = cudaGetDevice(&dev);
-  if(err != cudaSuccess) return (int)err;
-  if(dev < 0 || dev >= 64) return (int)cudaErrorInvalidDevice;
-  unsigned long long* addr = cache[dev].load(std::memory_order_acquire);
-  if(!addr) {
-    void* ptr = nullptr;
-    err = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if(err != cudaSuccess) return (int)err;
-    addr = (unsigned long long*)ptr;
-    cache[dev].store(addr, std::memory_order_release);
-  }
-  *out = addr;
-  return 0;
-}
-
-template<class R, int MINB>
-static int launch_batch_noalloc_variant
-  (const DScene<R>* scenes, const DTallies* tallies, int nitems, uint64_t seed,
-   const unsigned long long* h_prefix, const unsigned long long* h_firsts,
-   const LaunchConfig& cfg, void* stream)
-{
-  if(nitems < 1 || nitems > NOALLOC_MAX_ITEMS) return (int)cudaErrorInvalidValue;
-  unsigned long long* scratch = nullptr;
-  int err = noalloc_scratch_address(&scratch);
-  if(err) return err;
-  const cudaStream_t s = (cudaStream_t)stream;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  int nsm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int block = cfg.block_size > 0 ? cfg.block_size : MAX_BLOCK;
-  if(block > MAX_BLOCK || block % 32) return (int)cudaErrorInvalidValue;
-  const size_t smem = (size_t)((2 * NGLOBAL + PS_COUNT) * block) * sizeof(double)
-                    + (size_t)SMEM_STACK * block * sizeof(int)
-                    + (size_t)(block / 32) * 2 * (2 * NGLOBAL + cfg.rcv_doubles) * sizeof(double)
-                    + (size_t)(block / 32) * 2 * sizeof(DScene<R>);
-  raise_smem_limit<BatchTag<R, MINB>>(batch_kernel<R, MINB>, dev);
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor
-    (&per_sm, batch_kernel<R, MINB>, block, smem);
-  if(per_sm < 1) per_sm = 1;
-  const uint64_t blocks = cfg.grid_blocks > 0
-    ? (uint64_t)cfg.grid_blocks
-    : (uint64_t)nsm * (uint64_t)per_sm * (uint64_t)(cfg.waves > 0 ? cfg.waves : 1);
-  /* Budgets and stream offsets of this call; the work counter and launch
-   * counters start at zero (the array keeps the previous call's values) */
-  cudaError_t e;
-  e = cudaMemcpyAsync(scratch + NOALLOC_PREFIX, h_prefix,
-                      (size_t)(nitems + 1) * sizeof(unsigned long long),
-                      cudaMemcpyHostToDevice, s);
-  if(e != cudaSuccess) return (int)e;
-  e = cudaMemcpyAsync(scratch + NOALLOC_FIRSTS, h_firsts,
-                      (size_t)nitems * sizeof(unsigned long long),
-                      cudaMemcpyHostToDevice, s);
-  if(e != cudaSuccess) return (int)e;
-  e = cudaMemsetAsync(scratch + NOALLOC_NEXT, 0,
-                      (NOALLOC_WORDS - NOALLOC_NEXT) * sizeof(unsigned long long), s);
-  if(e != cudaSuccess) return (int)e;
-  batch_kernel<R, MINB><<<(unsigned)blocks, block, smem, s>>>
-    (scenes, tallies, scratch + NOALLOC_PREFIX, scratch + NOALLOC_FIRSTS, nitems,
-     seed, cfg.max_segments, scratch + NOALLOC_NEXT,
-     reinterpret_cast<DStats*>(scratch + NOALLOC_STATS), cfg.rcv_doubles);
-  return (int)cudaGetLastError();
-}
-
-template<class R>
-static int launch_batch_noalloc_impl
-  (const DScene<R>* scenes, const DTallies* tallies, int nitems, uint64_t seed,
-   const unsigned long long* h_prefix, const unsigned long long* h_firsts,
-   const LaunchConfig& cfg, void* stream)
-{
-  switch(cfg.min_blocks) {
-    case 1: return launch_batch_noalloc_variant<R, 1>
-      (scenes, tallies, nitems, seed, h_prefix, h_firsts, cfg, stream);
-    case 3: return launch_batch_noalloc_variant<R, 3>
-      (scenes, tallies, nitems, seed, h_prefix, h_firsts, cfg, stream);
-    default: return launch_batch_noalloc_variant<R, 2>
-      (scenes, tallies, nitems, seed, h_prefix, h_firsts, cfg, stream);
-  }
-}
-
-int launch_batch_noalloc_f32
-  (const DScene<float>* scenes, const DTallies* tallies, int nitems,
-   uint64_t seed, const unsigned long long* h_prefix,
-   const unsigned long long* h_firsts, const LaunchConfig& cfg, void* stream)
-{
-  return launch_batch_noalloc_impl<float>
-    (scenes, tallies, nitems, seed, h_prefix, h_firsts, cfg, stream);
-}
-
-int launch_batch_noalloc_f64
-  (const DScene<double>* scenes, const DTallies* tallies, int nitems,
-   uint64_t seed, const unsigned long long* h_prefix,
-   const unsigned long long* h_firsts, const LaunchConfig& cfg, void* stream)
-{
-  return launch_batch_noalloc_impl<double>
-    (scenes, tallies, nitems, seed, h_prefix, h_firsts, cfg, stream);
-}
-
-int launch_realisations_f32
-  (const DScene<float>& S, const DTallies& T, uint64_t seed, uint64_t first,
-   uint64_t count, const LaunchConfig& cfg, void* stream, const DTrack* track)
-{ return launch_impl<float>(S, T, seed, first, count, cfg, stream, track); }
-
-int launch_realisations_f64
-  (const DScene<double>& S, const DTallies& T, uint64_t seed, uint64_t first,
-   uint64_t count, const LaunchConfig& cfg, void* stream, const DTrack* track)
-{ return launch_impl<double>(S, T, seed, first, count, cfg, stream, track); }
-
-#include "adjoint.cuh"
-#include "draw.cuh"
 
 } /* namespace ssolb */
+
+#endif /* SSOL_B200_KERNELS_DEVICE_CUH */

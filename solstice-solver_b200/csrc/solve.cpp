@@ -238,10 +238,11 @@ struct ssol_b200_plan {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double kernel_ms = 0;
   bool timing_valid = false;
-  /* Abort word: host memory mapped into the device's address space, set by
-   * ssol_b200_plan_abort and polled by the launches' work fetch */
-  unsigned int* abort_host = nullptr;
-  const unsigned int* abort_dev = nullptr;
+  /* Abort request: ssol_b200_plan_abort copies this pinned word into the
+   * tallies' abort word (counters[5]) on a stream of its own, by the copy
+   * engine, while the plan's kernels run; their work fetch polls it */
+  unsigned long long* abort_host = nullptr;
+  cudaStream_t abort_stream = nullptr;
 };
 
 static TallyLayout tally_layout(int nrcv, int nsampled, int nprim_slots)
@@ -633,6 +634,7 @@ static void plan_release(ssol_b200_plan* p)
   dev_free(p->dev, p->d_tally, p->tl.total);
   if(p->ev0) cudaEventDestroy(p->ev0);
   if(p->ev1) cudaEventDestroy(p->ev1);
+  if(p->abort_stream) cudaStreamDestroy(p->abort_stream);
   if(p->abort_host) cudaFreeHost(p->abort_host);
   if(p->scn) ssol_scene_ref_put(p->scn);
   ssol_device* dev = p->dev;
@@ -720,16 +722,17 @@ extern "C" res_T ssol_b200_plan_create
     return RES_MEM_ERR;
   }
   p->t = bind_tallies(p->tl, (unsigned char*)p->d_tally);
-  void* dptr = nullptr;
-  if(cudaHostAlloc((void**)&p->abort_host, 64, cudaHostAllocMapped) != cudaSuccess
-  || cudaHostGetDevicePointer(&dptr, p->abort_host, 0) != cudaSuccess) {
-    if(p->abort_host) cudaFreeHost(p->abort_host);
+  if(cudaMallocHost((void**)&p->abort_host, sizeof(unsigned long long)) != cudaSuccess) {
     p->abort_host = nullptr;
     plan_release(p);
     return RES_MEM_ERR;
   }
-  p->abort_dev = (const unsigned int*)dptr;
-  *p->abort_host = 0;
+  *p->abort_host = 1;
+  if(cudaStreamCreateWithFlags(&p->abort_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    p->abort_stream = nullptr;
+    plan_release(p);
+    return RES_UNKNOWN_ERR;
+  }
   cudaEventCreate(&p->ev0);
   cudaEventCreate(&p->ev1);
   *out = p;
@@ -743,15 +746,18 @@ static cudaStream_t plan_stream(ssol_b200_plan* p, void* stream)
 
 extern "C" res_T ssol_b200_plan_abort(ssol_b200_plan* p)
 {
-  if(!p || !p->abort_host) return RES_BAD_ARG;
-  __atomic_store_n(p->abort_host, 1u, __ATOMIC_SEQ_CST);
+  if(!p || !p->abort_host || !p->abort_stream) return RES_BAD_ARG;
+  /* A copy, not a kernel: it runs beside the plan's persistent kernels */
+  if(cudaMemcpyAsync(p->t.counters + 5, p->abort_host, sizeof(unsigned long long),
+                     cudaMemcpyHostToDevice, p->abort_stream) != cudaSuccess
+  || cudaStreamSynchronize(p->abort_stream) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
   return RES_OK;
 }
 
 extern "C" res_T ssol_b200_plan_reset(ssol_b200_plan* p, void* stream)
 {
   if(!p) return RES_BAD_ARG;
-  if(p->abort_host) __atomic_store_n(p->abort_host, 0u, __ATOMIC_SEQ_CST);
   if(cudaMemsetAsync(p->d_tally, 0, p->tl.total, plan_stream(p, stream))
      != cudaSuccess)
     return RES_UNKNOWN_ERR;
@@ -775,7 +781,8 @@ static res_T plan_launch
   cfg.max_segments = p->opt.max_segments;
   cfg.min_blocks = p->opt.min_blocks_per_sm;
   cfg.max_failed = max_failed;
-  cfg.abort_word = p->abort_dev;
+  cfg.abortable = true;
+  cfg.features = p->meta.features;
   const uint64_t start = rng->position + first;
   cudaEventRecord(p->ev0, s);
   const int err = p->opt.precision == SSOL_B200_FP32
@@ -831,7 +838,8 @@ extern "C" res_T ssol_b200_plan_finish
   const uint64_t ran = std::min<uint64_t>(nreal, st->paths);
   res_T res = make_estimator(p->dev, p->scn, p->meta, p->tl, h.data(), ran, rng,
                              nreal, st, p->kernel_ms, p->scene_bytes, max_failed, out);
-  if(res == RES_OK && p->abort_host && __atomic_load_n(p->abort_host, __ATOMIC_SEQ_CST)) {
+  const unsigned long long* cnt = (const unsigned long long*)(h.data() + p->tl.counters);
+  if(res == RES_OK && cnt[5]) {
     p->dev->log_error("the solve was aborted: %llu of %llu realisations ran.\n",
                       (unsigned long long)ran, (unsigned long long)nreal);
     res = RES_BAD_OP;
@@ -1056,6 +1064,85 @@ extern "C" res_T ssol_b200_plan_get_stats
   return RES_OK;
 }
 
+/*******************************************************************************
+ * Tallies across GPUs: the FP64 sums region of a tally block runs from its
+ * global sums to the end of its per-primitive sums, the 64-bit counts region
+ * from the per-sampled sample counts to the end of the launch statistics.
+ * Padding between the arrays of a region is zero and stays zero when
+ * regions are added, so that two blocks of the same scene add element-wise.
+ ******************************************************************************/
+static void tally_regions(const TallyLayout& tl, size_t* nsums, size_t* ncounts)
+{
+  *nsums = (tl.nb_samples - tl.global) / sizeof(double);
+  *ncounts = (tl.total - tl.nb_samples) / sizeof(unsigned long long);
+}
+
+extern "C" res_T ssol_b200_plan_get_tallies
+  (ssol_b200_plan* p, double** sums, size_t* nsums, uint64_t** counts,
+   size_t* ncounts)
+{
+  if(!p || !sums || !nsums || !counts || !ncounts) return RES_BAD_ARG;
+  unsigned char* base = (unsigned char*)p->d_tally;
+  *sums = (double*)(base + p->tl.global);
+  *counts = (uint64_t*)(base + p->tl.nb_samples);
+  tally_regions(p->tl, nsums, ncounts);
+  return RES_OK;
+}
+
+/* Host snapshot metadata of `scn` (receiver slots, sampled instances,
+ * primitive ranges): what gives a tally block its layout */
+static res_T scene_meta(ssol_scene* scn, FlatMeta& meta, TallyLayout& tl)
+{
+  BvhBuildParams bp;
+  bp.threads = host_threads();
+  FlatScene<float> f;
+  res_T res = flatten_scene(scn, bp, f);
+  if(res != RES_OK) return res;
+  meta = f.meta;
+  tl = tally_layout((int)meta.rcv.size(), (int)meta.sampled.size(), meta.nprim_slots);
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_tallies_size
+  (ssol_scene* scn, size_t* nsums, size_t* ncounts)
+{
+  if(!scn || !nsums || !ncounts) return RES_BAD_ARG;
+  FlatMeta meta;
+  TallyLayout tl;
+  const res_T res = scene_meta(scn, meta, tl);
+  if(res != RES_OK) return res;
+  tally_regions(tl, nsums, ncounts);
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_estimator_create_from_tallies
+  (ssol_scene* scn, const ssp_rng* rng, const uint64_t nreal,
+   const size_t max_failed, const double* sums, const size_t nsums,
+   const uint64_t* counts, const size_t ncounts, ssol_estimator** out)
+{
+  if(!scn || !rng || !sums || !counts || !out) return RES_BAD_ARG;
+  *out = nullptr;
+  FlatMeta meta;
+  TallyLayout tl;
+  res_T res = scene_meta(scn, meta, tl);
+  if(res != RES_OK) return res;
+  size_t ns = 0, nc = 0;
+  tally_regions(tl, &ns, &nc);
+  if(nsums != ns || ncounts != nc) {
+    scn->dev->log_error("tallies of %zu sums and %zu counts; this scene's have "
+                        "%zu and %zu.\n", nsums, ncounts, ns, nc);
+    return RES_BAD_ARG;
+  }
+  std::vector<unsigned char> block(tl.total, 0);
+  std::memcpy(block.data() + tl.global, sums, nsums * sizeof(double));
+  std::memcpy(block.data() + tl.nb_samples, counts, ncounts * sizeof(uint64_t));
+  const DStats* st = (const DStats*)(block.data() + tl.stats);
+  /* As ssol_b200_plan_finish: realisations that ran, when counted */
+  const uint64_t ran = st->paths ? std::min<uint64_t>(nreal, st->paths) : nreal;
+  return make_estimator(scn->dev, scn, meta, tl, block.data(), ran, rng, nreal, st,
+                        0.0, 0, max_failed, out);
+}
+
 
 /*******************************************************************************
  * Batches: many scenes, one persistent launch (see ssol_b200.h)
@@ -1162,6 +1249,8 @@ static res_T batch_upload(ssol_b200_batch* b, std::vector<FlatScene<R>>& f)
   return RES_OK;
 }
 
+static res_T batch_tallies(ssol_b200_batch* b);
+
 extern "C" res_T ssol_b200_batch_create
   (ssol_scene* const* scenes, const size_t nscenes,
    const ssol_b200_options* options, ssol_b200_batch** out)
@@ -1222,8 +1311,17 @@ extern "C" res_T ssol_b200_batch_create
   if(res == RES_OK)
     res = opt.precision == SSOL_B200_FP32 ? batch_upload(b, f32) : batch_upload(b, f64);
   if(res != RES_OK) { batch_release(b); return res; }
+  res = batch_tallies(b);
+  if(res != RES_OK) { batch_release(b); return res; }
+  *out = b;
+  return ssol_b200_batch_reset(b, nullptr);
+}
 
-  /* Tallies of every item, then the batch bookkeeping */
+/* Tallies of every item (b->meta filled), then the batch bookkeeping */
+static res_T batch_tallies(ssol_b200_batch* b)
+{
+  ssol_device* dev = b->dev;
+  const size_t nscenes = b->scenes.size();
   size_t off = 0;
   for(size_t i = 0; i < nscenes; ++i) {
     const FlatMeta& m = b->meta[i];
@@ -1245,7 +1343,6 @@ extern "C" res_T ssol_b200_batch_create
   off += (sizeof(DStats) + 255) & ~size_t(255);
   if(dev_alloc(dev, &b->d_tally, off) != cudaSuccess) {
     b->d_tally = nullptr;
-    batch_release(b);
     return RES_MEM_ERR;
   }
   b->tally_alloc = off;
@@ -1261,15 +1358,257 @@ extern "C" res_T ssol_b200_batch_create
   const cudaStream_t s = (cudaStream_t)dev->stream;
   if(cudaMemcpyAsync((void*)b->d_tallies, T.data(), nscenes * sizeof(DTallies),
                      cudaMemcpyHostToDevice, s) != cudaSuccess
-  || cudaStreamSynchronize(s) != cudaSuccess) {
-    batch_release(b);
+  || cudaStreamSynchronize(s) != cudaSuccess)
     return RES_UNKNOWN_ERR;
-  }
   b->done.assign(nscenes, 0);
   b->h_prefix.assign(nscenes + 1, 0);
   b->h_firsts.assign(nscenes, 0);
   cudaEventCreate(&b->ev0);
   cudaEventCreate(&b->ev1);
+  return RES_OK;
+}
+
+/* Tracking batches (see ssol_b200_batch_create_tracking): one snapshot of
+ * the scene uploaded once; per item (sun position) device copies of its
+ * triangles, sampled triangles and BVH nodes, the tracked heliostats turned
+ * toward the item's sun and the BVH refitted on the device; every other
+ * array is shared by the items */
+template<class R>
+static res_T tracking_upload
+  (ssol_b200_batch* b, FlatScene<R>& f, ssol_instance* const* helio, size_t nhelio,
+   const double* aims, const std::vector<double>& dirs, const ssol_b200_sun_position* suns)
+{
+  ssol_device* dev = b->dev;
+  const size_t nitems = b->scenes.size();
+  /* Tracked triangles: each heliostat's mesh ranges, with local vertices */
+  std::vector<double> helio_data(6 * nhelio);
+  std::vector<int32_t> tri_helio, tri_index, tri_samp;
+  std::vector<double> local;
+  for(size_t h = 0; h < nhelio; ++h) {
+    const ssol_instance* inst = helio[h];
+    for(int c = 0; c < 3; ++c) {
+      helio_data[6 * h + c] = inst->transform[9 + c];
+      helio_data[6 * h + 3 + c] = aims[3 * h + c];
+    }
+    bool found = false;
+    for(const FlatMeta::MeshRange& m : f.meta.meshes) {
+      if(m.inst != inst) continue;
+      found = true;
+      for(int t = 0; t < m.ntris; ++t) {
+        tri_helio.push_back((int32_t)h);
+        tri_index.push_back(m.tri_first + t);
+        tri_samp.push_back(m.samp_first >= 0 ? m.samp_first + t : -1);
+        for(int k = 0; k < 3; ++k) {
+          const uint32_t id = m.shape->ids[(size_t)t * 3 + k];
+          for(int c = 0; c < 3; ++c) local.push_back(m.shape->pos[(size_t)id * 3 + c]);
+        }
+      }
+    }
+    if(!found) {
+      dev->log_error("tracking: heliostat %zu is not a mesh instance of the scene.\n", h);
+      return RES_BAD_ARG;
+    }
+  }
+  /* BVH nodes grouped by depth, deepest first */
+  const size_t nnodes = f.nodes.size();
+  std::vector<int> depth(nnodes, 0);
+  int maxd = 0;
+  for(size_t i = 0; i < nnodes; ++i)
+    for(int k = 0; k < 2; ++k)
+      if(f.nodes[i].count[k] == 0) {
+        const int c = f.nodes[i].child[k];
+        depth[c] = depth[i] + 1;
+        maxd = std::max(maxd, depth[c]);
+      }
+  std::vector<int32_t> level_first(1, 0), level_nodes;
+  for(int d = maxd; d >= 0; --d) {
+    for(size_t i = 0; i < nnodes; ++i) if(depth[i] == d) level_nodes.push_back((int32_t)i);
+    level_first.push_back((int32_t)level_nodes.size());
+  }
+
+  /* One device block: the snapshot, the items' copies, the DScene array and
+   * the inputs of the tracking kernels */
+  Blob blob;
+  add_scene(blob, f);
+  const size_t ntri = f.tris.size(), nsamp = f.samp.size();
+  size_t total = (blob.host.size() + 255) & ~size_t(255);
+  auto take = [&](size_t bytes) { const size_t o = total; total = (total + bytes + 255) & ~size_t(255); return o; };
+  const size_t o_tris = take(nitems * ntri * sizeof(DTri<R>));
+  const size_t o_samp = take(nitems * nsamp * sizeof(DSampTri<R>));
+  const size_t o_nodes = take(nitems * nnodes * sizeof(DNode<R>));
+  const size_t o_scenes = take(nitems * sizeof(DScene<R>));
+  const size_t o_helio = take(helio_data.size() * sizeof(double));
+  const size_t o_sun = take(3 * nitems * sizeof(double));
+  const size_t o_th = take(tri_helio.size() * sizeof(int32_t));
+  const size_t o_ti = take(tri_index.size() * sizeof(int32_t));
+  const size_t o_ts = take(tri_samp.size() * sizeof(int32_t));
+  const size_t o_loc = take(local.size() * sizeof(double));
+  const size_t o_ln = take(level_nodes.size() * sizeof(int32_t));
+  const size_t o_lf = take(level_first.size() * sizeof(int32_t));
+  if(dev_alloc(dev, &b->d_scene, total + 256) != cudaSuccess) {
+    b->d_scene = nullptr;
+    return RES_MEM_ERR;
+  }
+  b->scene_alloc = total + 256;
+  unsigned char* base = (unsigned char*)b->d_scene;
+  const cudaStream_t st = (cudaStream_t)dev->stream;
+  std::vector<double> to_sun(3 * nitems);
+  for(size_t i = 0; i < nitems; ++i)
+    for(int c = 0; c < 3; ++c) to_sun[3 * i + c] = -dirs[3 * i + c];
+  auto up = [&](size_t off, const void* src, size_t bytes) {
+    return !bytes || cudaMemcpyAsync(base + off, src, bytes, cudaMemcpyHostToDevice, st)
+                       == cudaSuccess;
+  };
+  bool ok = up(0, blob.host.data(), blob.host.size())
+    && up(o_helio, helio_data.data(), helio_data.size() * sizeof(double))
+    && up(o_sun, to_sun.data(), to_sun.size() * sizeof(double))
+    && up(o_th, tri_helio.data(), tri_helio.size() * sizeof(int32_t))
+    && up(o_ti, tri_index.data(), tri_index.size() * sizeof(int32_t))
+    && up(o_ts, tri_samp.data(), tri_samp.size() * sizeof(int32_t))
+    && up(o_loc, local.data(), local.size() * sizeof(double))
+    && up(o_ln, level_nodes.data(), level_nodes.size() * sizeof(int32_t))
+    && up(o_lf, level_first.data(), level_first.size() * sizeof(int32_t));
+  DScene<R> S0;
+  bind_scene(S0, f, blob, base);
+  /* Each item starts from the snapshot's arrays */
+  for(size_t i = 0; i < nitems && ok; ++i) {
+    ok = cudaMemcpyAsync(base + o_tris + i * ntri * sizeof(DTri<R>), S0.tris,
+                         ntri * sizeof(DTri<R>), cudaMemcpyDeviceToDevice, st) == cudaSuccess
+      && (!nsamp || cudaMemcpyAsync(base + o_samp + i * nsamp * sizeof(DSampTri<R>), S0.samp,
+                                    nsamp * sizeof(DSampTri<R>), cudaMemcpyDeviceToDevice, st)
+                    == cudaSuccess)
+      && cudaMemcpyAsync(base + o_nodes + i * nnodes * sizeof(DNode<R>), S0.nodes,
+                         nnodes * sizeof(DNode<R>), cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+  }
+  if(!ok) return RES_UNKNOWN_ERR;
+  TrackArgs A;
+  A.nitems = (int)nitems;
+  A.ntracked = (int)tri_helio.size();
+  A.nlevels = (int)level_first.size() - 1;
+  A.helio = (const double*)(base + o_helio);
+  A.to_sun = (const double*)(base + o_sun);
+  A.tri_helio = (const int32_t*)(base + o_th);
+  A.tri_index = (const int32_t*)(base + o_ti);
+  A.tri_samp = (const int32_t*)(base + o_ts);
+  A.local = (const double*)(base + o_loc);
+  A.tris = base + o_tris; A.tri_stride = ntri;
+  A.samp = base + o_samp; A.samp_stride = nsamp;
+  A.nodes = base + o_nodes; A.node_stride = nnodes;
+  A.primrefs = S0.primrefs;
+  A.level_nodes = (const int32_t*)(base + o_ln);
+  A.level_first = (const int32_t*)(base + o_lf);
+  const int err = sizeof(R) == sizeof(float) ? launch_track_f32(A, st) : launch_track_f64(A, st);
+  if(err) {
+    dev->log_error("tracking kernels: %s\n", cudaGetErrorString((cudaError_t)err));
+    return RES_UNKNOWN_ERR;
+  }
+  /* The items' records: the snapshot's, with their own triangles, sampled
+   * triangles, nodes and sun */
+  std::vector<DScene<R>> S(nitems, S0);
+  for(size_t i = 0; i < nitems; ++i) {
+    S[i].tris = (const DTri<R>*)(base + o_tris) + i * ntri;
+    S[i].samp = (const DSampTri<R>*)(base + o_samp) + i * nsamp;
+    S[i].nodes = (const DNode<R>*)(base + o_nodes) + i * nnodes;
+    double B[9];
+    sun_frame(&dirs[3 * i], B);
+    for(int c = 0; c < 3; ++c) S[i].sun_dir[c] = (R)dirs[3 * i + c];
+    for(int c = 0; c < 9; ++c) S[i].sun_basis[c] = (R)B[c];
+    S[i].dni = suns[i].dni;
+  }
+  if(!up(o_scenes, S.data(), nitems * sizeof(DScene<R>))
+  || cudaStreamSynchronize(st) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  b->scene_bytes = blob.host.size() + local.size() * sizeof(double);
+  b->d_scenes = base + o_scenes;
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_batch_create_tracking
+  (ssol_scene* scn, ssol_instance* const* heliostats, const size_t nhelio,
+   const double* aims, const ssol_b200_sun_position* suns, const size_t nsuns,
+   const ssol_b200_options* options, ssol_b200_batch** out)
+{
+  if(!scn || (nhelio && (!heliostats || !aims)) || !suns || !nsuns || !out
+  || nsuns > (size_t)INT32_MAX)
+    return RES_BAD_ARG;
+  ssol_b200_options opt = options ? *options : SSOL_B200_OPTIONS_DEFAULT;
+  if(opt.precision != SSOL_B200_FP32 && opt.precision != SSOL_B200_FP64)
+    return RES_BAD_ARG;
+  if(opt.block_size < 0 || opt.block_size > 256 || opt.grid_blocks < 0
+  || opt.waves < 0 || opt.bvh_leaf_size < 0 || opt.min_blocks_per_sm < 0
+  || opt.min_blocks_per_sm > 3)
+    return RES_BAD_ARG;
+  if(opt.block_size == 0) opt.block_size = 256;
+  if(opt.block_size % 32) return RES_BAD_ARG;
+  if(opt.bvh_leaf_size == 0) opt.bvh_leaf_size = 1;
+  if(opt.max_segments == 0) opt.max_segments = 1000000ull;
+  if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = 2;
+  /* Sun directions normalised as ssol_sun_set_direction does */
+  std::vector<double> dirs(3 * nsuns);
+  for(size_t i = 0; i < nsuns; ++i) {
+    const double* d = suns[i].direction;
+    const double len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if(!(len > 0) || !(suns[i].dni > 0)) return RES_BAD_ARG;
+    for(int c = 0; c < 3; ++c) dirs[3 * i + c] = d[c] / len;
+  }
+  for(size_t h = 0; h < nhelio; ++h) {
+    if(!heliostats[h]) return RES_BAD_ARG;
+    for(const ShadedShape& ss : heliostats[h]->object->shaded)
+      if(ss.shape->kind != SHAPE_MESH) {
+        scn->dev->log_error("tracking: heliostat %zu has a punched surface; only "
+                            "meshes are re-aimed on the device.\n", h);
+        return RES_BAD_ARG;
+      }
+  }
+
+  ssol_device* dev = scn->dev;
+  ssol_b200_batch* b = new (std::nothrow) ssol_b200_batch();
+  if(!b) return RES_MEM_ERR;
+  ssol_device_ref_get(dev);
+  b->dev = dev;
+  for(size_t i = 0; i < nsuns; ++i) {
+    ssol_scene_ref_get(scn);
+    b->scenes.push_back(scn);
+  }
+  b->opt = opt;
+  BvhBuildParams bp;
+  bp.max_leaf = opt.bvh_leaf_size;
+  bp.threads = host_threads();
+  res_T res;
+  FlatScene<float> f32;
+  FlatScene<double> f64;
+  if(opt.precision == SSOL_B200_FP32) {
+    res = flatten_scene(scn, bp, f32);
+    if(res == RES_OK && !validate(f32)) res = RES_UNKNOWN_ERR;
+  } else {
+    res = flatten_scene(scn, bp, f64);
+    if(res == RES_OK && !validate(f64)) res = RES_UNKNOWN_ERR;
+  }
+  if(res != RES_OK) { batch_release(b); return res; }
+  const FlatMeta& meta = opt.precision == SSOL_B200_FP32 ? f32.meta : f64.meta;
+  if(meta.features & FEAT_ATTRIBUTES) {
+    dev->log_error("tracking: scenes with vertex normals or shaders baked per "
+                   "vertex are not re-aimed on the device.\n");
+    batch_release(b);
+    return RES_BAD_ARG;
+  }
+  for(size_t h = 0; h < nhelio; ++h) {
+    bool found = false;
+    for(const FlatMeta::MeshRange& m : meta.meshes) found = found || m.inst == heliostats[h];
+    if(!found) {
+      dev->log_error("tracking: heliostat %zu is not an instance of the scene.\n", h);
+      batch_release(b);
+      return RES_BAD_ARG;
+    }
+  }
+  b->meta.assign(nsuns, meta);
+  res = device_bind(dev);
+  if(res == RES_OK)
+    res = opt.precision == SSOL_B200_FP32
+      ? tracking_upload(b, f32, heliostats, nhelio, aims, dirs, suns)
+      : tracking_upload(b, f64, heliostats, nhelio, aims, dirs, suns);
+  if(res == RES_OK) res = batch_tallies(b);
+  if(res != RES_OK) { batch_release(b); return res; }
   *out = b;
   return ssol_b200_batch_reset(b, nullptr);
 }
@@ -1300,7 +1639,11 @@ static LaunchConfig batch_config(const ssol_b200_batch* b)
   cfg.max_segments = b->opt.max_segments;
   cfg.min_blocks = b->opt.min_blocks_per_sm;
   size_t nrcv = 0;
-  for(const FlatMeta& m : b->meta) nrcv = std::max(nrcv, m.rcv.size());
+  cfg.features = 0;
+  for(const FlatMeta& m : b->meta) {
+    nrcv = std::max(nrcv, m.rcv.size());
+    cfg.features |= m.features;
+  }
   const size_t rcvd = nrcv * NRCV_Q * 2;
   const size_t warps = (size_t)(cfg.block_size > 0 ? cfg.block_size : 256) / 32;
   cfg.rcv_doubles = warps * 2 * rcvd * sizeof(double) <= 16 * 1024 ? (int)rcvd : 0;
@@ -1375,7 +1718,7 @@ extern "C" res_T ssol_b200_batch_launch
 
 /* The no-allocation launch (declared in ssol_b200.h): same kernel and
  * results as ssol_b200_batch_launch, without the graph and with the
- * launch's scratch in a static device array (kernels.cu) */
+ * launch's scratch in a static device array (kernels_batch.cu) */
 extern "C" res_T ssol_b200_batch_launch_noalloc
   (ssol_b200_batch* b, const ssp_rng* rng, const uint64_t* budgets, void* stream)
 {

@@ -158,6 +158,10 @@ class B200Options(C.Structure):
                 ("max_segments", C.c_ulonglong), ("min_blocks_per_sm", C.c_int)]
 
 
+class SunPosition(C.Structure):
+    _fields_ = [("direction", C.c_double * 3), ("dni", C.c_double)]
+
+
 class B200Stats(C.Structure):
     _fields_ = [("kernel_ms", C.c_double)] + [(n, C.c_ulonglong) for n in (
         "rays", "node_visits", "triangle_tests", "quadric_tests", "bounces", "paths",
@@ -263,6 +267,12 @@ _OPTIONAL = {
     "ssol_b200_plan_ref_put": [VP],
     "ssol_b200_plan_reset": [VP, VP],
     "ssol_b200_plan_abort": [VP],
+    "ssol_b200_plan_get_tallies": [VP, PVP, C.POINTER(C.c_size_t), PVP,
+                                   C.POINTER(C.c_size_t)],
+    "ssol_b200_tallies_size": [VP, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)],
+    "ssol_b200_estimator_create_from_tallies": [VP, VP, C.c_uint64, C.c_size_t,
+                                                C.POINTER(C.c_double), C.c_size_t,
+                                                C.POINTER(C.c_uint64), C.c_size_t, PVP],
     "ssol_b200_plan_launch": [VP, VP, C.c_uint64, C.c_uint64, VP],
     "ssol_b200_plan_finish": [VP, VP, C.c_uint64, C.c_size_t, VP, PVP],
     "ssol_b200_batch_create": [PVP, C.c_size_t, C.POINTER(B200Options), PVP],
@@ -271,6 +281,9 @@ _OPTIONAL = {
     "ssol_b200_batch_launch": [VP, VP, C.POINTER(C.c_uint64), VP],
     "ssol_b200_batch_finish": [VP, VP, C.c_size_t, VP, PVP],
     "ssol_b200_batch_launch_noalloc": [VP, VP, C.POINTER(C.c_uint64), VP],
+    "ssol_b200_batch_create_tracking": [VP, PVP, C.c_size_t, C.POINTER(C.c_double),
+                                        C.POINTER(SunPosition), C.c_size_t,
+                                        C.POINTER(B200Options), PVP],
     "ssol_b200_autotune": [VP, VP, C.c_uint64, C.POINTER(B200Options),
                            C.POINTER(C.c_double)],
     "ssol_b200_draw_draft_device": [VP, VP, C.c_size_t, C.c_size_t, C.c_size_t,
@@ -294,7 +307,9 @@ class Lib:
         self.has_b200 = hasattr(self.dll, "ssol_b200_plan_create")
         if self.has_b200:
             for name, args in _OPTIONAL.items():
-                f = getattr(self.dll, name)
+                f = getattr(self.dll, name, None)
+                if f is None:  # an older build of the library
+                    continue
                 f.argtypes = args
                 f.restype = C.c_int
         self.dll.ssol_param_buffer_create.argtypes = [VP, C.c_size_t, PVP]
@@ -814,6 +829,27 @@ class Batch:
         lib.call("ssol_b200_batch_create", C.cast(arr, PVP), len(scenes),
                  C.byref(opts) if opts is not None else None, C.byref(self.h))
 
+    @classmethod
+    def tracking(cls, scene, heliostats, aims, suns, opts=None):
+        """One item per sun of `scene` with `heliostats` (instance handles)
+        turned toward it and aimed at `aims` (one (x, y, z) each)
+        (ssol_b200_batch_create_tracking); suns: [(direction, dni), ...]."""
+        self = cls.__new__(cls)
+        self.lib = scene.lib
+        self.scenes = [scene] * len(suns)
+        hel = (C.c_void_p * max(1, len(heliostats)))(*[x.value for x in heliostats])
+        flat = [float(c) for a in aims for c in a]
+        aa = (C.c_double * max(1, len(flat)))(*flat)
+        sp = (SunPosition * len(suns))()
+        for i, (d, dni) in enumerate(suns):
+            sp[i].direction[:] = [float(c) for c in d]
+            sp[i].dni = float(dni)
+        self.h = C.c_void_p()
+        self.lib.call("ssol_b200_batch_create_tracking", scene.scn, C.cast(hel, PVP),
+                      len(heliostats), aa, sp, len(suns),
+                      C.byref(opts) if opts is not None else None, C.byref(self.h))
+        return self
+
     def reset(self, stream=None):
         self.lib.call("ssol_b200_batch_reset", self.h, stream)
 
@@ -844,6 +880,44 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class DeviceArray:
+    """A device buffer of the library seen through __cuda_array_interface__,
+    so that torch.as_tensor(DeviceArray(...), device="cuda") shares it."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 3}
+
+
+def plan_tallies(lib, plan):
+    """(sums, counts) of a plan (ssol_b200_plan_get_tallies) as DeviceArray
+    views: FP64 sums and 64-bit counts (viewed as int64, which adds alike)."""
+    sp, cp = C.c_void_p(), C.c_void_p()
+    ns, nc = C.c_size_t(), C.c_size_t()
+    lib.call("ssol_b200_plan_get_tallies", plan, C.byref(sp), C.byref(ns), C.byref(cp),
+             C.byref(nc))
+    return DeviceArray(sp.value, ns.value, "<f8"), DeviceArray(cp.value, nc.value, "<i8")
+
+
+def tallies_size(scene):
+    ns, nc = C.c_size_t(), C.c_size_t()
+    scene.lib.call("ssol_b200_tallies_size", scene.scn, C.byref(ns), C.byref(nc))
+    return ns.value, nc.value
+
+
+def estimator_from_tallies(scene, rng, n, sums, counts, max_failed=0):
+    """Estimator of `n` realisations of `scene` from host tallies (sequences
+    of floats and of non-negative ints)."""
+    sa = (C.c_double * len(sums))(*[float(x) for x in sums])
+    ca = (C.c_uint64 * len(counts))(*[int(x) & 0xffffffffffffffff for x in counts])
+    est = C.c_void_p()
+    res = scene.lib.raw("ssol_b200_estimator_create_from_tallies", scene.scn, rng, int(n),
+                        max_failed, sa, len(sums), ca, len(counts), C.byref(est))
+    if res not in (RES_OK, RES_BAD_OP):
+        raise SsolError("ssol_b200_estimator_create_from_tallies", res)
+    return Estimator(scene, est, res)
 
 
 def options(precision=FP32, block_size=256, grid_blocks=0, waves=1, leaf=0,

@@ -185,6 +185,18 @@ def sun_grid(n_el=16, n_az=16, el_range=(5.0, 85.0), seed=0, dni_range=(300.0, 1
     return suns
 
 
+def tracking_inputs(h, suns, aim=(0.0, 0.0, 100.0)):
+    """Arguments of a tracking batch (pyssol.Batch.tracking) for the
+    heliostats of a heliostat_field scene `h` and sun_grid entries: every
+    heliostat aims at `aim`; per sun the direction from the sun toward the
+    scene and the DNI. The device turns the heliostats with the rule
+    heliostat_field follows, so item i is the field heliostat_field builds
+    for sun i."""
+    aims = [aim] * len(h["heliostats"])
+    sp = [(tuple(-c for c in to_sun(sn["elevation"], sn["azimuth"])), sn["dni"]) for sn in suns]
+    return h["heliostats"], aims, sp
+
+
 def batched_fields(lib, suns, n_helio=1000, receiver_cells=64):
     """One heliostat_field scene per sun, heliostats re-aimed for that sun."""
     out = []

@@ -182,3 +182,35 @@ def test_native_constant_shaders(product):
     assert tuple(out) == (0.6, 0.0, 0.8)
     product.call("ssol_param_buffer_ref_put", buf)
     s.close()
+
+
+def test_tracking_batch_argument_checks(product):
+    """ssol_b200_batch_create_tracking refuses bad arguments on the host,
+    before any device work: no suns, a DNI <= 0, a zero direction, a punched
+    heliostat, a heliostat outside the scene."""
+    import workloads as W
+    s, h = W.heliostat_field(product, n_helio=10, receiver_cells=2)
+    hel, aims, sp = W.tracking_inputs(h, [{"elevation": 40.0, "azimuth": 90.0, "dni": 800.0}])
+    ha = (C.c_void_p * len(hel))(*[x.value for x in hel])
+    aa = (C.c_double * (3 * len(aims)))(*[c for a in aims for c in a])
+    out = C.c_void_p()
+
+    def call(suns, heliostats=ha, n=len(hel)):
+        arr = (P.SunPosition * max(1, len(suns)))()
+        for i, (d, dni) in enumerate(suns):
+            arr[i].direction[:] = d
+            arr[i].dni = dni
+        return product.raw("ssol_b200_batch_create_tracking", s.scn, C.cast(heliostats, P.PVP),
+                           n, aa, arr, len(suns), None, C.byref(out))
+    assert call([]) == P.RES_BAD_ARG
+    assert call([(sp[0][0], 0.0)]) == P.RES_BAD_ARG
+    assert call([((0.0, 0.0, 0.0), 900.0)]) == P.RES_BAD_ARG
+    other = P.Scene(product)
+    stray = other.instance(other.object([(other.rectangle(1, 1), other.matte(0.0),
+                                          other.matte(0.0))]))
+    assert call(sp, (C.c_void_p * 1)(stray.value), 1) == P.RES_BAD_ARG
+    poly = [(-1, -1), (-1, 1), (1, 1), (1, -1)]
+    par = s.instance(s.object([(s.punched(P.Q_PARABOL, (10.0,), [(P.SSOL_AND, poly)]),
+                                s.mirror(0.9, 0.0), s.matte(0.0))]),
+                     P.transform_from(None, (0, 300, 5)), sample=0)
+    assert call(sp, (C.c_void_p * 1)(par.value), 1) == P.RES_BAD_ARG

@@ -147,6 +147,7 @@ def test_host_abort_of_a_running_plan(product):
     """ssol_b200_plan_abort while a long launch runs: its warps stop taking
     realisations within milliseconds, ssol_b200_plan_finish returns
     RES_BAD_OP with the estimator of what ran, and a reset clears it."""
+    import threading
     import time
     s, h = W.single_mirror(product)
     plan = P.C.c_void_p()
@@ -154,9 +155,14 @@ def test_host_abort_of_a_running_plan(product):
     rng = s.rng(seed=4)
     n = 8_000_000_000
     t0 = time.perf_counter()
-    product.call("ssol_b200_plan_launch", plan, rng, 0, n, None)
-    time.sleep(0.05)
+    # The launch enqueues its chunks of 2^24 realisations from this thread
+    # (it may block on the launch queue); the abort comes from another one
+    th = threading.Thread(target=product.call,
+                          args=("ssol_b200_plan_launch", plan, rng, 0, n, None))
+    th.start()
+    time.sleep(0.2)
     product.call("ssol_b200_plan_abort", plan)
+    th.join()
     est = P.C.c_void_p()
     res = product.raw("ssol_b200_plan_finish", plan, rng, n, 0, None, P.C.byref(est))
     dt = time.perf_counter() - t0
@@ -164,7 +170,7 @@ def test_host_abort_of_a_running_plan(product):
     assert res == P.RES_BAD_OP
     ran = e.count("realisation_count")
     assert 0 < ran < n // 2, ran
-    assert dt < 3.0, dt
+    assert dt < 5.0, dt
     g = e.globals()
     assert g["cos_factor"][0] > 0
     del e

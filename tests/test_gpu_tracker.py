@@ -60,7 +60,12 @@ def test_tracked_field_paths(product, oracle):
     po = so.solve(n, seed=8, tracker=(50.0, 50.0)).paths()
     # FP32 geometry may flip the discrete outcome of a rare path
     compare_paths(pg, po, 1e-4, max_mismatch=n // 200)
+    # The tracking kernel and the plain one trace the same realisations, but
+    # they are separately compiled variants (the plain one without the code
+    # of the features this scene lacks) and may contract some FP32 products
+    # into FMAs differently: weights may differ in their last bits. 1e-9
+    # still detects one path of the 2000 with another outcome (~5e-4).
     plain = sg.solve(n, seed=8)
     a, b = eg.globals(), plain.globals()
     for k in a:
-        assert a[k][0] == pytest.approx(b[k][0], rel=1e-12, abs=1e-9), k
+        assert a[k][0] == pytest.approx(b[k][0], rel=1e-9, abs=1e-9), k

@@ -2,7 +2,9 @@
 with the oracle standing in for each rank's GPU: the disjoint realisation
 ranges of the ranks, all-reduced, give the same sums as one solve of all of
 them (the realisation streams are keyed by realisation id), and the timing
-reduction takes the max over ranks."""
+reduction takes the max over ranks. Then the library's own merge: the
+ranks' tally vectors all-reduced over gloo and turned into one estimator by
+ssol_b200_estimator_create_from_tallies, which needs no GPU."""
 import os
 import socket
 import sys
@@ -78,3 +80,68 @@ def test_two_ranks_match_one_solve(oracle):
         assert a == pytest.approx(b, rel=1e-9, abs=1e-6)
     assert ms == 20.0
     assert cover == [1] * 256
+
+
+def _merge_rank(rank, world, port, product_path, q):
+    """One rank of the tally merge through the library's own entries: the
+    rank's tally vectors (pairs of sum w and sum w^2, here drawn from seeded
+    weights, as a GPU's plan would hold them) are all-reduced over gloo and
+    rank 0 builds the merged estimator with
+    ssol_b200_estimator_create_from_tallies."""
+    import random
+    import torch
+    import torch.distributed as dist
+    import pyssol as P
+    import workloads as W
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port,
+                            rank=rank, world_size=world)
+    lib = P.Lib(product_path)
+    s, h = W.heliostat_field(lib, n_helio=30, receiver_cells=4)
+    ns, nc = P.tallies_size(s)
+    rnd = random.Random(1000 + rank)
+    sums = []
+    for _ in range(ns // 2):
+        w = [rnd.uniform(0.0, 10.0) for _ in range(3)]
+        sums += [sum(w), sum(x * x for x in w)]
+    t = torch.tensor(sums, dtype=torch.float64)
+    c = torch.zeros(nc, dtype=torch.int64)
+    gathered = [torch.zeros_like(t) for _ in range(world)]
+    dist.all_gather(gathered, t)
+    dist.all_reduce(t)
+    dist.all_reduce(c)
+    if rank == 0:
+        rng = s.rng(seed=3)
+        n_rank = 1000
+        merged = P.estimator_from_tallies(s, rng, world * n_rank, t.tolist(), c.tolist())
+        parts = [P.estimator_from_tallies(s, rng, n_rank, g.tolist(), c.tolist())
+                 for g in gathered]
+        q.put((merged.count("realisation_count"), merged.globals(),
+               merged.receiver(h["receiver"]), [p.globals() for p in parts],
+               [p.receiver(h["receiver"]) for p in parts], t[:12].tolist(), n_rank))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_ranks_merge_tallies_through_the_library(product):
+    """The merged estimator of two ranks' all-reduced tallies: N = N0 + N1
+    realisations, E the pooled mean (N0 E0 + N1 E1) / N, and every global
+    estimate equal to the one computed from the summed vectors."""
+    import torch.multiprocessing as mp
+    import pyssol as P
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_merge_rank, args=(r, 2, port, P.PRODUCT_LIB, q))
+             for r in range(2)]
+    for p in procs:
+        p.start()
+    count, g, rcv, pg, prcv, gsum, n = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert count == 2 * n
+    for i, k in enumerate(P.GLOBAL_FIELDS):
+        assert g[k][0] == pytest.approx(gsum[2 * i] / (2 * n), rel=1e-12)
+        assert g[k][0] == pytest.approx((pg[0][k][0] + pg[1][k][0]) / 2, rel=1e-12)
+    for k in rcv:
+        assert rcv[k][0] == pytest.approx((prcv[0][k][0] + prcv[1][k][0]) / 2, rel=1e-12)
