@@ -157,14 +157,20 @@ SSOL_API res_T ssol_b200_autotune
  * bilinear weights on the cell centres. Parameters: for each listed
  * heliostat, rotations theta_x, theta_y about its instance's local x and y
  * axes through its translation, at theta = 0. Gradients follow the paths
- * (reparameterised sampling, replayed from the Philox keys of `rng`); the
- * changes of shadowing, blocking and the receiver's edges are not
- * differentiated. */
+ * (reparameterised sampling, replayed from the Philox keys of `rng`).
+ * The receiver's boundary, taken as the map's rectangle (so the map should
+ * cover the receiver exactly), is differentiated through a smoothed
+ * receiver: a linear ramp of width `edge_band` across each side, so that
+ * the reflected rays that cross the receiver's plane within half a band of
+ * its boundary, unblocked, carry the derivative of the flux entering or
+ * leaving it (bias O(edge_band); 0 selects half a map cell). The changes of
+ * shadowing and blocking are not differentiated. */
 struct ssol_b200_adjoint_map {
   struct ssol_instance* receiver; /* a mesh instance */
   double lower[2], upper[2]; /* receiver-local x, y extent of the grid */
   unsigned nx, ny;
   double target; /* uniform target flux density, W/m^2 */
+  double edge_band; /* width of the boundary ramp, m; 0 => half a cell */
 };
 
 struct ssol_b200_adjoint_result {

@@ -10,8 +10,8 @@
   optimised with torch.
 - `finite_difference_check`: central differences with common random numbers
   (the same Philox keys for +h and -h) against the adjoint, which reports the
-  bias from the shadowing, blocking and receiver-edge terms the adjoint does
-  not differentiate.
+  bias from the shadowing and blocking terms the adjoint does not
+  differentiate (its receiver-edge term is smoothed over a band).
 """
 import ctypes as C
 import math
@@ -22,7 +22,7 @@ import pyssol as P
 class AdjointMap(C.Structure):
     _fields_ = [("receiver", C.c_void_p), ("lower", C.c_double * 2),
                 ("upper", C.c_double * 2), ("nx", C.c_uint), ("ny", C.c_uint),
-                ("target", C.c_double)]
+                ("target", C.c_double), ("edge_band", C.c_double)]
 
 
 class AdjointResult(C.Structure):

@@ -243,23 +243,52 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
     const V3<R> rd = mk((R)out.x.v, (R)out.y.v, (R)out.z.v);
     self.discard_virtual = false;
     self.reversed = false;
-    if(!trace_ray(S, pos, rd, R(0), self, false, h, cnt, stack, stride)) continue;
-    const DShadedInst hs = S.sinsts[h.sinst];
-    if(hs.instance != A.rcv_instance || hs.is_punched) continue;
-    const int hside = dot(rd, h.n) < R(0) ? 1 : 2;
-    if(!(hs.receiver_mask & hside)) continue;
-    const DMaterial hm = S.mtls[hs.mtl[hside - 1]];
-    if(hm.type != MTL_MIRROR && hm.type != MTL_MATTE) continue;
-    const int hbake = S.tshade ? S.tshade[h.gid].bake[hside - 1] : -1;
-    float2 huv = make_float2(0.f, 0.f);
-    if(hbake >= 0) huv = tri_uv(S, h.gid, pos + rd * h.t);
-    const double kabs = 1.0 - (double)(hbake >= 0
-      ? baked_value(S, hbake, 0, wl, (R)huv.x, (R)huv.y) : shader_value(S, hm, 0, wl));
-
-    /* Distance to the hit triangle's plane and hit point, with tangents */
-    const DTri<R>& T = S.tris[h.gid];
-    const V3<double> ng = vd(h.n);
-    const Dd t = (dd(dot(ng, vd(ld3(T.v0)))) - ddot(x, ng)) / ddot(out, ng);
+    const bool found = trace_ray(S, pos, rd, R(0), self, false, h, cnt, stack, stride);
+    bool on_rcv = false;
+    int hside = 1;
+    if(found) {
+      const DShadedInst hs = S.sinsts[h.sinst];
+      hside = dot(rd, h.n) < R(0) ? 1 : 2;
+      on_rcv = hs.instance == A.rcv_instance && !hs.is_punched && (hs.receiver_mask & hside);
+      if(on_rcv) {
+        const DMaterial hm = S.mtls[hs.mtl[hside - 1]];
+        on_rcv = hm.type == MTL_MIRROR || hm.type == MTL_MATTE;
+      }
+    }
+    /* Pass 1 also follows rays that cross the receiver's plane just outside
+     * it, unblocked: the ramp that smooths the receiver's boundary gives
+     * them the derivative of the hits that would enter it */
+    Dd tpl = dd(0.0);
+    bool edge_only = false;
+    if(!on_rcv) {
+      if(PASS == 0) continue;
+      const Dd zx = x.x * A.w2l[8] + x.y * A.w2l[9] + x.z * A.w2l[10] + A.w2l[11];
+      const Dd zo = out.x * A.w2l[8] + out.y * A.w2l[9] + out.z * A.w2l[10];
+      /* crossing toward the receiving side: from +z for the front */
+      if(A.rcv_side == 1 ? !(zx.v > 0.0 && zo.v < 0.0) : !(zx.v < 0.0 && zo.v > 0.0))
+        continue;
+      tpl = -zx / zo;
+      if(found && (double)h.t < tpl.v) continue; /* blocked before the plane */
+      edge_only = true;
+    }
+    double kabs;
+    Dd t;
+    if(!edge_only) {
+      const DShadedInst hs = S.sinsts[h.sinst];
+      const DMaterial hm = S.mtls[hs.mtl[hside - 1]];
+      const int hbake = S.tshade ? S.tshade[h.gid].bake[hside - 1] : -1;
+      float2 huv = make_float2(0.f, 0.f);
+      if(hbake >= 0) huv = tri_uv(S, h.gid, pos + rd * h.t);
+      kabs = 1.0 - (double)(hbake >= 0
+        ? baked_value(S, hbake, 0, wl, (R)huv.x, (R)huv.y) : shader_value(S, hm, 0, wl));
+      /* Distance to the hit triangle's plane, with tangents */
+      const DTri<R>& T = S.tris[h.gid];
+      const V3<double> ng = vd(h.n);
+      t = (dd(dot(ng, vd(ld3(T.v0)))) - ddot(x, ng)) / ddot(out, ng);
+    } else {
+      kabs = 1.0 - (double)shader_value(S, S.mtls[A.rcv_mtl], 0, wl);
+      t = tpl;
+    }
     const DV p = x + out * t;
     const double kext = data_value(S, S.media[S.air_medium].extinction, wl);
     if(kext > 0.0) w = w * dexp(t * (-kext));
@@ -272,6 +301,17 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
       s_w2 += w.v * w.v;
       s_hit += 1.0;
     } else {
+      /* Smoothed receiver: a ramp of width `edge` across each side of the
+       * map's rectangle, 1 inside, 0 outside; on the hits of the receiver
+       * away from its boundary it is 1 with no tangent */
+      auto ramp = [&](Dd q, double lo, double hi) -> Dd {
+        const Dd d = q.v - lo < hi - q.v ? q - lo : dd(hi) - q;
+        const Dd r = d * (1.0 / A.edge) + 0.5;
+        return r.v >= 1.0 ? dd(1.0) : r.v <= 0.0 ? dd(0.0) : r;
+      };
+      const Dd sm = ramp(u, A.lower[0], A.upper[0]) * ramp(v, A.lower[1], A.upper[1]);
+      if(edge_only && !(sm.v > 0.0)) continue;
+      w = w * sm;
       atomicAdd(A.grad_abs + 2 * slot, w.a * A.inv_n);
       atomicAdd(A.grad_abs + 2 * slot + 1, w.b * A.inv_n);
     }

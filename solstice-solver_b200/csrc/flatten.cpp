@@ -604,6 +604,7 @@ static res_T flatten_impl
   for(size_t ii = 0; ii < scn->instances.size(); ++ii) {
     ssol_instance* inst = scn->instances[ii];
     const ssol_object* obj = inst->object;
+    if(obj->shaded.empty()) out.meta.inst_mtl.push_back({-1, -1});
     int rcv_slot[2] = {-1, -1};
     for(int side = 0; side < 2; ++side) {
       if(inst->receiver_mask & (side == 0 ? SSOL_FRONT : SSOL_BACK)) {
@@ -627,6 +628,7 @@ static res_T flatten_impl
       si.instance = (int32_t)ii;
       si.mtl[0] = material_id(ss.front);
       si.mtl[1] = material_id(ss.back);
+      if(out.meta.inst_mtl.size() == ii) out.meta.inst_mtl.push_back({si.mtl[0], si.mtl[1]});
       si.receiver_mask = inst->receiver_mask & (SSOL_FRONT | SSOL_BACK);
       si.rcv_slot[0] = rcv_slot[0];
       si.rcv_slot[1] = rcv_slot[1];

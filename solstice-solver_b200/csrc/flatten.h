@@ -16,6 +16,7 @@
 #include "device_scene.h"
 #include "objects.h"
 
+#include <array>
 #include <vector>
 
 namespace ssolb {
@@ -48,6 +49,9 @@ struct FlatMeta {
     int tri_first, ntris, samp_first;
   };
   std::vector<MeshRange> meshes;
+  /* Per instance (attach order): device material indices of the front and
+   * back of its first shaded shape, -1 if it has none */
+  std::vector<std::array<int, 2>> inst_mtl;
 };
 
 template<class R> struct FlatScene {

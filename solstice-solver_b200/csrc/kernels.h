@@ -118,7 +118,11 @@ struct AdjointArgs {
   const int* inst_slot;
   const double* axes;
   int rcv_instance;
-  double w2l[8]; /* rows x and y of the receiver's world -> local transform */
+  int rcv_side; /* the receiver's receiving side: 1 front (+z), 2 back */
+  int rcv_mtl; /* material of that side (device index) */
+  double w2l[12]; /* the receiver's world -> local transform, rows x, y, z */
+  double upper[2]; /* far corner of the map (its near corner is `lower`) */
+  double edge; /* width of the ramp that smooths the receiver's boundary */
   double lower[2], inv_cell[2];
   int nx, ny;
   double* map;

@@ -927,7 +927,8 @@ extern "C" res_T ssol_solve_adjoint
   if(!scn || !rng || !n || !map || !map->receiver || !result) return RES_BAD_ARG;
   if(nh && (!helios || !d_absorbed || !d_spillage)) return RES_BAD_ARG;
   if(!map->nx || !map->ny || !(map->upper[0] > map->lower[0])
-  || !(map->upper[1] > map->lower[1]))
+  || !(map->upper[1] > map->lower[1]) || !(map->edge_band >= 0)
+  || !map->receiver->receiver_mask)
     return RES_BAD_ARG;
   /* Instance indices in attach order, as the device scene numbers them */
   const std::vector<ssol_instance*>& insts = scn->instances;
@@ -979,11 +980,22 @@ extern "C" res_T ssol_solve_adjoint
   A.inst_slot = d_slot;
   A.axes = d_axes;
   A.rcv_instance = rcv_index;
-  for(int q = 0; q < 8; ++q) A.w2l[q] = W[q];
+  A.rcv_side = (map->receiver->receiver_mask & SSOL_FRONT) ? 1 : 2;
+  A.rcv_mtl = (size_t)rcv_index < plan->meta.inst_mtl.size()
+    ? plan->meta.inst_mtl[rcv_index][A.rcv_side - 1] : -1;
+  if(A.rcv_mtl < 0) {
+    ssol_b200_plan_ref_put(plan);
+    cudaFree(dbuf);
+    return RES_BAD_ARG;
+  }
+  for(int q = 0; q < 12; ++q) A.w2l[q] = W[q];
   const double cw = (map->upper[0] - map->lower[0]) / map->nx;
   const double ch = (map->upper[1] - map->lower[1]) / map->ny;
   A.lower[0] = map->lower[0];
   A.lower[1] = map->lower[1];
+  A.upper[0] = map->upper[0];
+  A.upper[1] = map->upper[1];
+  A.edge = map->edge_band > 0 ? map->edge_band : 0.5 * std::min(cw, ch);
   A.inv_cell[0] = 1.0 / cw;
   A.inv_cell[1] = 1.0 / ch;
   A.nx = (int)map->nx;
