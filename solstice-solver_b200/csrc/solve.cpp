@@ -238,11 +238,6 @@ struct ssol_b200_plan {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double kernel_ms = 0;
   bool timing_valid = false;
-  /* Abort request: ssol_b200_plan_abort copies this pinned word into the
-   * tallies' abort word (counters[5]) on a stream of its own, by the copy
-   * engine, while the plan's kernels run; their work fetch polls it */
-  unsigned long long* abort_host = nullptr;
-  cudaStream_t abort_stream = nullptr;
 };
 
 static TallyLayout tally_layout(int nrcv, int nsampled, int nprim_slots)
@@ -634,8 +629,6 @@ static void plan_release(ssol_b200_plan* p)
   dev_free(p->dev, p->d_tally, p->tl.total);
   if(p->ev0) cudaEventDestroy(p->ev0);
   if(p->ev1) cudaEventDestroy(p->ev1);
-  if(p->abort_stream) cudaStreamDestroy(p->abort_stream);
-  if(p->abort_host) cudaFreeHost(p->abort_host);
   if(p->scn) ssol_scene_ref_put(p->scn);
   ssol_device* dev = p->dev;
   delete p;
@@ -722,17 +715,6 @@ extern "C" res_T ssol_b200_plan_create
     return RES_MEM_ERR;
   }
   p->t = bind_tallies(p->tl, (unsigned char*)p->d_tally);
-  if(cudaMallocHost((void**)&p->abort_host, sizeof(unsigned long long)) != cudaSuccess) {
-    p->abort_host = nullptr;
-    plan_release(p);
-    return RES_MEM_ERR;
-  }
-  *p->abort_host = 1;
-  if(cudaStreamCreateWithFlags(&p->abort_stream, cudaStreamNonBlocking) != cudaSuccess) {
-    p->abort_stream = nullptr;
-    plan_release(p);
-    return RES_UNKNOWN_ERR;
-  }
   cudaEventCreate(&p->ev0);
   cudaEventCreate(&p->ev1);
   *out = p;
@@ -744,15 +726,56 @@ static cudaStream_t plan_stream(ssol_b200_plan* p, void* stream)
   return stream ? (cudaStream_t)stream : (cudaStream_t)p->dev->stream;
 }
 
+/* What an abort request copies: a pinned word holding 1 and a non-blocking
+ * stream, per device, made on the first request, so that plans themselves
+ * allocate nothing for it */
+struct AbortChannel {
+  unsigned long long* one = nullptr;
+  cudaStream_t stream = nullptr;
+};
+
+static bool abort_channel(int dev, AbortChannel& out)
+{
+  static AbortChannel channels[64];
+  static std::mutex lock;
+  if(dev < 0 || dev >= 64) return false;
+  std::lock_guard<std::mutex> g(lock);
+  AbortChannel& c = channels[dev];
+  if(!c.one) {
+    if(cudaMallocHost((void**)&c.one, sizeof(unsigned long long)) != cudaSuccess) {
+      c.one = nullptr;
+      return false;
+    }
+    *c.one = 1;
+  }
+  if(!c.stream && cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    c.stream = nullptr;
+    return false;
+  }
+  out = c;
+  return true;
+}
+
 extern "C" res_T ssol_b200_plan_abort(ssol_b200_plan* p)
 {
-  if(!p || !p->abort_host || !p->abort_stream) return RES_BAD_ARG;
-  /* A copy, not a kernel: it runs beside the plan's persistent kernels */
-  if(cudaMemcpyAsync(p->t.counters + 5, p->abort_host, sizeof(unsigned long long),
-                     cudaMemcpyHostToDevice, p->abort_stream) != cudaSuccess
-  || cudaStreamSynchronize(p->abort_stream) != cudaSuccess)
+  if(!p) return RES_BAD_ARG;
+  /* The plan's device, whatever device is current on the calling thread */
+  const int dev = p->dev->cuda_device;
+  int cur = -1;
+  if(cudaGetDevice(&cur) != cudaSuccess) return RES_UNKNOWN_ERR;
+  if(cur != dev && cudaSetDevice(dev) != cudaSuccess) return RES_UNKNOWN_ERR;
+  AbortChannel c;
+  const bool ok = abort_channel(dev, c);
+  if(!ok) {
+    if(cur != dev) cudaSetDevice(cur);
     return RES_UNKNOWN_ERR;
-  return RES_OK;
+  }
+  /* A copy, not a kernel: it runs beside the plan's persistent kernels */
+  const bool copied = cudaMemcpyAsync(p->t.counters + 5, c.one, sizeof(unsigned long long),
+                                      cudaMemcpyHostToDevice, c.stream) == cudaSuccess
+    && cudaStreamSynchronize(c.stream) == cudaSuccess;
+  if(cur != dev) cudaSetDevice(cur);
+  return copied ? RES_OK : RES_UNKNOWN_ERR;
 }
 
 extern "C" res_T ssol_b200_plan_reset(ssol_b200_plan* p, void* stream)
