@@ -39,10 +39,10 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 
 
 # DRAM bytes per path of the realisation kernel, from ncu captures of launches
-# of the same scenes (field: one sorted chunk of 2^24 paths; beam-down: 4e6
-# paths) (dram__bytes_read.sum + dram__bytes_write.sum);
+# of the same scenes (field: one sorted chunk of 2^24 paths at 3 blocks per SM;
+# beam-down: 4e6 paths) (dram__bytes_read.sum + dram__bytes_write.sum);
 # the traffic scales with the paths traced (per-thread frames written back)
-DRAM_BYTES_PER_PATH = {"field": (416.7e6 + 3763.9e6) / 16777216,
+DRAM_BYTES_PER_PATH = {"field": (3161.0e6 + 16181.7e6) / 16777216,
                        "beamdown": (73.9e6 + 387.0e6) / 4e6}  # beam-down: id order
 
 # Kernels of one plain launch of n realisations: below 2^24 the realisation
