@@ -807,7 +807,8 @@ def run_adjoint(args):
     (snapshot, upload, both passes, read-back). Then central finite differences
     with common random numbers on 32 seeded random parameters, at h = 1e-4
     and 1e-3 rad, and the relative error of the adjoint against them (the
-    bias of the shadowing, blocking and receiver-edge terms it leaves out)."""
+    bias of the shadowing and blocking terms it leaves out; its receiver-edge
+    term is smoothed over half a map cell)."""
     import random
     import torch
     import pyssol as P
