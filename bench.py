@@ -641,18 +641,21 @@ def suns_comparison(args, lib, opt, stream, sp, flush, dist, local, rank, world,
     # target SE with the plain kernel must.
     budgets = [100000 for _ in suns]
 
-    def needed(est, done_n):
-        a = est.globals()["absorbed_by_receivers"]
+    def needed_g(g, done_n):
+        a = g["absorbed_by_receivers"]
         rse = a[2] / a[0] if a[0] > 0 else 1.0
         return int(min(max(done_n * (rse / target) ** 2, done_n), 1e8))
+
+    def needed(est, done_n):
+        return needed_g(est.globals(), done_n)
 
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     bt = tracking_batch()
     bt.launch(rng, budgets, sp)
-    es = bt.finish(rng, 0, sp)
-    more = [needed(e, b) - b for e, b in zip(es, budgets)]
-    del es
+    # the pilot needs each sun's absorbed-power SE only: the per-item global
+    # estimates, read without building estimators
+    more = [needed_g(g, b) - b for g, b in zip(bt.globals(sp), budgets)]
     bt.launch(rng, more, sp)
     es = bt.finish(rng, 0, sp)
     del es

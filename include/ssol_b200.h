@@ -34,7 +34,7 @@ struct ssol_b200_options {
   int bvh_leaf_size; /* primitives per BVH leaf; 0 => 1 */
   unsigned long long max_segments; /* path segment budget; 0 => 1e6 */
   int min_blocks_per_sm; /* register budget of the kernel variant: 1, 2, 3;
-                          * 0 => 2 */
+                          * 0 => 3 in FP32, 2 in FP64 */
 };
 #define SSOL_B200_OPTIONS_DEFAULT__ { SSOL_B200_FP32, 256, 0, 1, 0, 0, 0 }
 static const struct ssol_b200_options SSOL_B200_OPTIONS_DEFAULT =
@@ -258,6 +258,12 @@ SSOL_API res_T ssol_b200_batch_launch
 SSOL_API res_T ssol_b200_batch_launch_noalloc
   (struct ssol_b200_batch* batch, const struct ssp_rng* rng,
    const uint64_t* budgets, void* stream);
+/* The global estimates of every item (nscenes entries), as
+ * ssol_estimator_get_mc_global gives them on the item's estimator, without
+ * building estimators: a device gather and a read of 13 doubles per item.
+ * For pilots that size each item's next budget. */
+SSOL_API res_T ssol_b200_batch_get_mc_global
+  (struct ssol_b200_batch* batch, void* stream, struct ssol_mc_global* globals);
 /* One estimator per item (nscenes entries), as ssol_solve would return for
  * the realisations the item received */
 SSOL_API res_T ssol_b200_batch_finish

@@ -82,6 +82,10 @@ int launch_batch_noalloc_f64
 int launch_batch_f64(const BatchLaunch<double>& b, const LaunchConfig& cfg,
                      void* stream);
 
+/* Per item of a batch, its 12 global sums and its failure count (as a
+ * double), 13 doubles per item into `out` (device) */
+int launch_gather_globals(const DTallies* tallies, int nitems, double* out, void* stream);
+
 /* Tracking batches (one snapshot, one item per sun position): per item,
  * each tracked heliostat turns toward the item's sun, its triangles and
  * sampled triangles are rewritten, and the BVH is refitted. Device arrays:

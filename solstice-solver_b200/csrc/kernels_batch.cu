@@ -313,6 +313,25 @@ __global__ void __launch_bounds__(256) track_refit_kernel(const TrackArgs A)
   }
 }
 
+__global__ void __launch_bounds__(256) gather_globals_kernel
+  (const DTallies* tallies, int nitems, double* out)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int item = k / 13, q = k % 13;
+  if(item >= nitems) return;
+  const DTallies& T = tallies[item];
+  out[k] = q < 2 * NGLOBAL ? T.global[q] : (double)T.counters[0];
+}
+
+int launch_gather_globals(const DTallies* tallies, int nitems, double* out, void* stream)
+{
+  const int total = 13 * nitems;
+  if(total > 0)
+    gather_globals_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>
+      (tallies, nitems, out);
+  return (int)cudaGetLastError();
+}
+
 template<class R>
 static int launch_track(const TrackArgs& A, void* stream)
 {

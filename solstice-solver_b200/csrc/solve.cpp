@@ -240,6 +240,15 @@ struct ssol_b200_plan {
   bool timing_valid = false;
 };
 
+/* Default register budget: 3 blocks of 256 threads per SM (80 registers) in
+ * FP32, whose feature variants spill little there and gain from 24 warps
+ * per SM (field 532 against 483 Mpaths/s at 2, beam-down 174 against 167);
+ * 2 in FP64, whose registers are twice as wide */
+static int default_min_blocks(ssol_b200_precision p)
+{
+  return p == SSOL_B200_FP32 ? 3 : 2;
+}
+
 static TallyLayout tally_layout(int nrcv, int nsampled, int nprim_slots)
 {
   TallyLayout tl;
@@ -664,7 +673,7 @@ extern "C" res_T ssol_b200_plan_create
   if(opt.bvh_leaf_size == 0) opt.bvh_leaf_size = 1;
   if(opt.max_segments == 0) opt.max_segments = 1000000ull;
   if(opt.min_blocks_per_sm < 0 || opt.min_blocks_per_sm > 3) return RES_BAD_ARG;
-  if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = 2;
+  if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = default_min_blocks(opt.precision);
 
   BvhBuildParams bp;
   bp.max_leaf = opt.bvh_leaf_size;
@@ -1199,6 +1208,7 @@ struct ssol_b200_batch {
   unsigned long long* d_firsts = nullptr;
   unsigned long long* d_next = nullptr;
   DStats* d_stats = nullptr;
+  double* d_gather = nullptr; /* per item: global sums and failures */
   const void* d_scenes = nullptr;
   const DTallies* d_tallies = nullptr;
   std::vector<unsigned long long> done; /* realisations launched per item */
@@ -1304,7 +1314,7 @@ extern "C" res_T ssol_b200_batch_create
   if(opt.block_size % 32) return RES_BAD_ARG;
   if(opt.bvh_leaf_size == 0) opt.bvh_leaf_size = 1;
   if(opt.max_segments == 0) opt.max_segments = 1000000ull;
-  if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = 2;
+  if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = default_min_blocks(opt.precision);
 
   ssol_device* dev = scenes[0]->dev;
   ssol_b200_batch* b = new (std::nothrow) ssol_b200_batch();
@@ -1376,6 +1386,8 @@ static res_T batch_tallies(ssol_b200_batch* b)
   off += 256;
   const size_t o_stats = off;
   off += (sizeof(DStats) + 255) & ~size_t(255);
+  const size_t o_gather = off;
+  off += (13 * nscenes * sizeof(double) + 255) & ~size_t(255);
   if(dev_alloc(dev, &b->d_tally, off) != cudaSuccess) {
     b->d_tally = nullptr;
     return RES_MEM_ERR;
@@ -1390,6 +1402,7 @@ static res_T batch_tallies(ssol_b200_batch* b)
   b->d_firsts = (unsigned long long*)(base + o_firsts);
   b->d_next = (unsigned long long*)(base + o_next);
   b->d_stats = (DStats*)(base + o_stats);
+  b->d_gather = (double*)(base + o_gather);
   const cudaStream_t s = (cudaStream_t)dev->stream;
   if(cudaMemcpyAsync((void*)b->d_tallies, T.data(), nscenes * sizeof(DTallies),
                      cudaMemcpyHostToDevice, s) != cudaSuccess
@@ -1577,7 +1590,7 @@ extern "C" res_T ssol_b200_batch_create_tracking
   if(opt.block_size % 32) return RES_BAD_ARG;
   if(opt.bvh_leaf_size == 0) opt.bvh_leaf_size = 1;
   if(opt.max_segments == 0) opt.max_segments = 1000000ull;
-  if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = 2;
+  if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = default_min_blocks(opt.precision);
   /* Sun directions normalised as ssol_sun_set_direction does */
   std::vector<double> dirs(3 * nsuns);
   for(size_t i = 0; i < nsuns; ++i) {
@@ -1801,6 +1814,43 @@ extern "C" res_T ssol_b200_batch_launch_noalloc
   /* The host budget arrays are read by the copies: wait for them */
   if(cudaStreamSynchronize(s) != cudaSuccess) return RES_UNKNOWN_ERR;
   for(size_t i = 0; i < n; ++i) b->done[i] += budgets[i];
+  return RES_OK;
+}
+
+extern "C" res_T ssol_b200_batch_get_mc_global
+  (ssol_b200_batch* b, void* stream, ssol_mc_global* out)
+{
+  if(!b || !out) return RES_BAD_ARG;
+  const cudaStream_t s = stream ? (cudaStream_t)stream : (cudaStream_t)b->dev->stream;
+  const size_t n = b->scenes.size();
+  std::vector<double> h(13 * n);
+  if(launch_gather_globals(b->d_tallies, (int)n, b->d_gather, s) != 0
+  || cudaMemcpyAsync(h.data(), b->d_gather, h.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, s) != cudaSuccess
+  || cudaStreamSynchronize(s) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  /* As ssol_estimator_get_mc_global on the item's estimator: realisations
+   * launched minus failed ones */
+  auto mc = [](const double* w, double nr) {
+    ssol_mc_result r;
+    if(nr <= 0) { r.E = r.V = r.SE = 0; return r; }
+    r.E = w[0] / nr;
+    r.V = w[1] / nr - r.E * r.E;
+    r.V = r.V > 0 ? r.V : 0;
+    r.SE = std::sqrt(r.V / nr);
+    return r;
+  };
+  for(size_t i = 0; i < n; ++i) {
+    const double* g = h.data() + 13 * i;
+    const double failed = std::min(g[12], (double)b->done[i]);
+    const double nr = (double)b->done[i] - failed;
+    out[i].cos_factor = mc(g + 0, nr);
+    out[i].absorbed_by_receivers = mc(g + 2, nr);
+    out[i].shadowed = mc(g + 4, nr);
+    out[i].missing = mc(g + 6, nr);
+    out[i].extinguished_by_atmosphere = mc(g + 8, nr);
+    out[i].other_absorbed = mc(g + 10, nr);
+  }
   return RES_OK;
 }
 

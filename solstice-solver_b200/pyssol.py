@@ -281,6 +281,7 @@ _OPTIONAL = {
     "ssol_b200_batch_launch": [VP, VP, C.POINTER(C.c_uint64), VP],
     "ssol_b200_batch_finish": [VP, VP, C.c_size_t, VP, PVP],
     "ssol_b200_batch_launch_noalloc": [VP, VP, C.POINTER(C.c_uint64), VP],
+    "ssol_b200_batch_get_mc_global": [VP, VP, C.POINTER(McGlobal)],
     "ssol_b200_batch_create_tracking": [VP, PVP, C.c_size_t, C.POINTER(C.c_double),
                                         C.POINTER(SunPosition), C.c_size_t,
                                         C.POINTER(B200Options), PVP],
@@ -860,6 +861,13 @@ class Batch:
     def launch_noalloc(self, rng, budgets, stream=None):
         b = (C.c_uint64 * len(budgets))(*[int(x) for x in budgets])
         self.lib.call("ssol_b200_batch_launch_noalloc", self.h, rng, b, stream)
+
+    def globals(self, stream=None):
+        """Per item, the global estimates (ssol_b200_batch_get_mc_global)."""
+        n = len(self.scenes)
+        arr = (McGlobal * n)()
+        self.lib.call("ssol_b200_batch_get_mc_global", self.h, stream, arr)
+        return [{k: mc(getattr(g, k)) for k in GLOBAL_FIELDS} for g in arr]
 
     def finish(self, rng, max_failed=0, stream=None):
         n = len(self.scenes)

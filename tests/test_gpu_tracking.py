@@ -92,3 +92,21 @@ def test_tracking_noalloc_launch(product):
             assert close(gx[q], gy[q]), q
     a.close()
     b.close()
+
+
+def test_batch_globals_equal_the_estimators(product):
+    """ssol_b200_batch_get_mc_global gives, item by item, the global
+    estimates of the estimators ssol_b200_batch_finish builds."""
+    suns = _suns(4)
+    s, h = W.heliostat_field(product, n_helio=100, receiver_cells=8)
+    batch = P.Batch.tracking(s, *W.tracking_inputs(h, suns))
+    rng = s.rng(seed=3)
+    batch.launch(rng, [50000, 10000, 30000, 20000])
+    batch.launch(rng, [5000, 0, 7000, 1000])
+    quick = batch.globals()
+    full = batch.finish(rng)
+    for g, e in zip(quick, full):
+        for k, v in e.globals().items():
+            assert g[k][0] == pytest.approx(v[0], rel=1e-14, abs=1e-12), k
+            assert g[k][2] == pytest.approx(v[2], rel=1e-12, abs=1e-12), k
+    batch.close()
