@@ -242,11 +242,12 @@ SSOL_API res_T ssol_b200_batch_launch
  * allocating (an allocation can block, or fail, at any time). The batch
  * (scenes in, tallies out) is created beforehand; this call allocates
  * nothing: no cudaMalloc/cudaFree and no CUDA graph. The kernel's scratch
- * (budget prefix sums, per-item first realisation ids, the work counter and
- * launch counters) lives in a static device array sized for at most 4096
- * items, which every GPU that loads the library keeps until the process
- * exits; batches with more items get RES_BAD_ARG. The first call on a device
- * looks up that array's device address, with that device current, and keeps
+ * (budget prefix sums, per-item first realisation ids, per-item work
+ * counters and launch counters) lives in a static device array sized for
+ * at most 4096 items (96 KiB), which every GPU that loads the library keeps
+ * until the process exits; batches with more items get RES_BAD_ARG. The
+ * first call on a device looks up that array's device address, with that
+ * device current, and keeps
  * it for later calls (make that first call before any stream capture; after
  * a cudaDeviceReset the kept address is stale and the process must not call
  * this entry point again on that device). All calls share the array, so

@@ -56,7 +56,7 @@ template<class R> struct BatchLaunch {
   const unsigned long long* firsts;
   int nitems;
   uint64_t seed;
-  unsigned long long* next_path; /* work counter (scratch) */
+  unsigned long long* next_items; /* per-item work counters (scratch) */
   DStats* stats;
 };
 

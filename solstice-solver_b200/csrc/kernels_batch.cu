@@ -16,12 +16,13 @@ int launch_batch_f64(const BatchLaunch<double>& b, const LaunchConfig& cfg,
 
 /* Scratch of the no-allocation batched launch: one file-scope device array
  * holding the budget prefix sums (NOALLOC_MAX_ITEMS + 1 words), the
- * per-item first realisation ids (NOALLOC_MAX_ITEMS words), the work counter
- * and the launch counters (DStats). Every call on a device shares it. */
+ * per-item first realisation ids (NOALLOC_MAX_ITEMS words), the per-item
+ * work counters (NOALLOC_MAX_ITEMS words) and the launch counters (DStats):
+ * 96 KiB. Every call on a device shares it. */
 constexpr size_t NOALLOC_PREFIX = 0;
 constexpr size_t NOALLOC_FIRSTS = NOALLOC_MAX_ITEMS + 1;
 constexpr size_t NOALLOC_NEXT = 2 * NOALLOC_MAX_ITEMS + 1;
-constexpr size_t NOALLOC_STATS = 2 * NOALLOC_MAX_ITEMS + 2;
+constexpr size_t NOALLOC_STATS = 3 * NOALLOC_MAX_ITEMS + 1;
 constexpr size_t NOALLOC_WORDS =
   NOALLOC_STATS + sizeof(DStats) / sizeof(unsigned long long);
 static __device__ __align__(256) unsigned long long

@@ -1596,7 +1596,7 @@ batch_kernel
   (const DScene<R>* __restrict__ scenes, const DTallies* __restrict__ tallies,
    const unsigned long long* __restrict__ prefix,
    const unsigned long long* __restrict__ firsts, int nitems, uint64_t seed,
-   unsigned long long max_segments, unsigned long long* next_path,
+   unsigned long long max_segments, unsigned long long* next_items,
    DStats* stats, int rcvd)
 {
   extern __shared__ double smem[];
@@ -1634,14 +1634,33 @@ batch_kernel
                                                                    : scenes[item];
   };
 
-  const unsigned long long count = prefix[nitems];
+  /* Work: every item has its own counter (next_items). A warp takes its
+   * realisations from one item at a time, starting in the item where its
+   * block's share of the launch begins (so warps spread over the items in
+   * proportion to their budgets), and moves on to the next item with work
+   * left when its item is exhausted. Warps thus stay long on one item: its
+   * scene arrays stay warm in the caches and the item tags rarely change.
+   * (With one counter over all items, every warp moved to the next item at
+   * the same time, each item's arrays were cold for all of them, and a
+   * batch of 1e5 realisations per item ran at 204 Mpaths/s.) */
+  const unsigned long long total = prefix[nitems];
+  int wit = 0;
+  {
+    const unsigned long long g0 = total * (unsigned long long)blockIdx.x / gridDim.x;
+    int lo = 0, hi = nitems;
+    while(hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if(prefix[mid] <= g0) lo = mid; else hi = mid;
+    }
+    wit = lo;
+  }
   Rng rng;
   rng.k0 = (uint32_t)seed;
   rng.k1 = (uint32_t)(seed >> 32);
   PathState<R> p;
   p.phase = PH_NONE;
   int it = 0;
-  bool done = false;
+  bool done = total == 0;
   Counters cnt = {0, 0, 0, 0};
   uint32_t bounces = 0, npaths = 0;
   int xr[MAX_EXTRA], xp[MAX_EXTRA];
@@ -1664,28 +1683,29 @@ batch_kernel
     if(need) {
       const int leader = __ffs(need) - 1;
       unsigned long long base = 0;
-      if((int)lane == leader)
-        base = atomicAdd(next_path, (unsigned long long)__popc(need));
+      int item = wit, got = 0;
+      if((int)lane == leader) {
+        /* The warp's item, or the next ones in turn, until one has work */
+        for(int k = 0; k < nitems; ++k) {
+          const unsigned long long budget = prefix[item + 1] - prefix[item];
+          if(*(volatile const unsigned long long*)(next_items + item) < budget) {
+            base = atomicAdd(next_items + item, (unsigned long long)__popc(need));
+            if(base < budget) { got = 1; break; }
+          }
+          item = item + 1 == nitems ? 0 : item + 1;
+        }
+      }
+      got = __shfl_sync(0xffffffffu, got, leader);
+      item = __shfl_sync(0xffffffffu, item, leader);
       base = __shfl_sync(0xffffffffu, base, leader);
+      if(got) wit = item;
       if(p.phase == PH_NONE && !done) {
         const unsigned long long g = base + __popc(need & ((1u << lane) - 1u));
-        if(g >= count) {
+        if(!got) {
           done = true;
-        } else {
-          /* The work index only grows, so the item follows from the lane's
-           * previous one, usually in zero or one step; a binary search
-           * covers long jumps. prefix[it] <= g < prefix[it + 1]. */
-          if(prefix[it] > g) it = 0;
-          int steps = 0;
-          while(prefix[it + 1] <= g && steps < 4) { ++it; ++steps; }
-          if(prefix[it + 1] <= g) {
-            int lo = it, hi = nitems;
-            while(hi - lo > 1) {
-              const int mid = (lo + hi) >> 1;
-              if(prefix[mid] <= g) lo = mid; else hi = mid;
-            }
-            it = lo;
-          }
+        } else if(g < prefix[item + 1] - prefix[item]) {
+          /* lanes past the item's end take work at the next fetch */
+          it = item;
           if(it != acc_item) {
             if(acc_item >= 0) {
               double* sl = acc_item == stag[cur] ? wslots + cur * ss
@@ -1701,7 +1721,7 @@ batch_kernel
             }
             acc_item = it;
           }
-          const uint64_t id = firsts[it] + (g - prefix[it]);
+          const uint64_t id = firsts[it] + g;
           rng.i_lo = (uint32_t)id;
           rng.i_hi = (uint32_t)(id >> 32);
           init_path<R, FEAT>(scene_of(it), rng, p, ps, bd);
@@ -1709,9 +1729,8 @@ batch_kernel
         }
       }
       {
-        /* Converged: the newest item fetched becomes the current slot */
-        const bool fetched = (need >> lane) & 1u && !done;
-        const int newest = __reduce_max_sync(0xffffffffu, fetched ? it : -1);
+        /* Converged: the item fetched becomes the current slot */
+        const int newest = got ? wit : -1;
         if(newest >= 0 && newest != stag[cur]) {
           const int prv = cur ^ 1;
           double* sl = wslots + prv * ss;
@@ -2117,10 +2136,11 @@ static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg
   const uint64_t blocks = cfg.grid_blocks > 0
     ? (uint64_t)cfg.grid_blocks
     : (uint64_t)nsm * (uint64_t)per_sm * (uint64_t)(cfg.waves > 0 ? cfg.waves : 1);
-  cudaMemsetAsync(b.next_path, 0, sizeof(unsigned long long), (cudaStream_t)stream);
+  cudaMemsetAsync(b.next_items, 0, (size_t)b.nitems * sizeof(unsigned long long),
+                  (cudaStream_t)stream);
   batch_kernel<R, MINB, FEAT><<<(unsigned)blocks, block, smem, (cudaStream_t)stream>>>
     (b.scenes, b.tallies, b.prefix, b.firsts, b.nitems, b.seed, cfg.max_segments,
-     b.next_path, b.stats, cfg.rcv_doubles);
+     b.next_items, b.stats, cfg.rcv_doubles);
   return (int)cudaGetLastError();
 }
 

@@ -1206,7 +1206,7 @@ struct ssol_b200_batch {
                               work counter and launch stats */
   unsigned long long* d_prefix = nullptr;
   unsigned long long* d_firsts = nullptr;
-  unsigned long long* d_next = nullptr;
+  unsigned long long* d_next = nullptr; /* per-item work counters */
   DStats* d_stats = nullptr;
   double* d_gather = nullptr; /* per item: global sums and failures */
   const void* d_scenes = nullptr;
@@ -1383,7 +1383,7 @@ static res_T batch_tallies(ssol_b200_batch* b)
   const size_t o_firsts = off;
   off = (off + nscenes * sizeof(unsigned long long) + 255) & ~size_t(255);
   const size_t o_next = off;
-  off += 256;
+  off = (off + nscenes * sizeof(unsigned long long) + 255) & ~size_t(255);
   const size_t o_stats = off;
   off += (sizeof(DStats) + 255) & ~size_t(255);
   const size_t o_gather = off;
