@@ -589,9 +589,13 @@ __device__ __forceinline__ bool slab
 /* The builder bounds the BVH depth to 30, so a traversal never holds more
  * than 30 deferred nodes. The first SMEM_STACK entries live in shared
  * memory; the rare deeper ones in a per-thread array (local memory), which
- * leaves shared memory to the L1 cache that holds the BVH. */
+ * leaves shared memory to the L1 cache that holds the BVH. With 5 entries
+ * three blocks of 256 threads of the realisation kernel (53.4 KB each, plus
+ * the 1 KB the SM reserves per block) fit the 164 KB shared-memory
+ * configuration of the SM, which leaves 92 KB of L1 instead of 60: field
+ * 535 -> 550 Mpaths/s (8 entries needed the 196 KB configuration). */
 constexpr int STACK_SIZE = 32;
-constexpr int SMEM_STACK = 8;
+constexpr int SMEM_STACK = 5;
 
 /* Closest accepted hit, or the first accepted hit when `any` (shadow rays).
  * Deferred node i < SMEM_STACK of this thread is stack[i * stride] in shared
@@ -1288,6 +1292,12 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 
 constexpr int SMEM_RCV_MAX = 16;
 constexpr int MAX_BLOCK = 256;
+/* SMs per item group of the batched kernel's work order: small items
+ * (fewer than BATCH_LARGE_ITEM realisations on average) by groups of 8 SMs,
+ * larger ones by 16. Measured on 256 field items (Mpaths/s, groups of 8 /
+ * 16 / 37 SMs): 1e5 each 437 / 420 / 345, 1e6 each 482 / 489 / 485. */
+constexpr int BATCH_GROUP_SMALL = 8, BATCH_GROUP_LARGE = 16;
+constexpr unsigned long long BATCH_LARGE_ITEM = 400000;
 /* Coherent order (see presort_count) */
 constexpr int SORT_MAX_BINS = 12288; /* shared-memory histogram of primitives */
 constexpr uint64_t SORT_CHUNK = 1ull << 24; /* realisations per sorted chunk */
@@ -1634,26 +1644,30 @@ batch_kernel
                                                                    : scenes[item];
   };
 
-  /* Work: every item has its own counter (next_items). A warp takes its
-   * realisations from one item at a time, starting in the item where its
-   * block's share of the launch begins (so warps spread over the items in
-   * proportion to their budgets), and moves on to the next item with work
-   * left when its item is exhausted. Warps thus stay long on one item: its
-   * scene arrays stay warm in the caches and the item tags rarely change.
-   * (With one counter over all items, every warp moved to the next item at
-   * the same time, each item's arrays were cold for all of them, and a
-   * batch of 1e5 realisations per item ran at 204 Mpaths/s.) */
+  /* Work: every item has its own counter (next_items). The SMs form groups
+   * of group_sms; group g works through its own items g, g + G, g + 2G, ...
+   * in turn, then through the next groups' lists, taking its realisations
+   * from the first item of the sequence with work left. The warps of an SM
+   * thus stay long on one item (its scene arrays stay warm in L1 and the
+   * item tags rarely change), and only about G items are open at a time
+   * (their arrays and tallies stay in L2). Positions q of the sequence map
+   * to items (q % L) x G + q / L, L = ceil(nitems / G); those past the last
+   * item are skipped. Measured on 256 field items: with one counter over
+   * all items (every warp moved to the next item at the same time, its
+   * arrays cold for all of them) 1e5 realisations per item ran at 199
+   * Mpaths/s; with every SM starting on its own item 416, and 1e6 per item
+   * 436 (about 150 items open). */
   const unsigned long long total = prefix[nitems];
+  unsigned smid, nsmid;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+  asm volatile("mov.u32 %0, %%nsmid;" : "=r"(nsmid));
+  const unsigned group_sms = total < BATCH_LARGE_ITEM * (unsigned long long)nitems
+                            ? BATCH_GROUP_SMALL : BATCH_GROUP_LARGE;
+  const int ngroups = min(nitems, max(1, (int)(nsmid / group_sms)));
+  const int seq_len = (nitems + ngroups - 1) / ngroups;
+  const int npos = ngroups * seq_len;
+  int wq = (int)(min(smid, nsmid - 1) * (unsigned)ngroups / nsmid) * seq_len;
   int wit = 0;
-  {
-    const unsigned long long g0 = total * (unsigned long long)blockIdx.x / gridDim.x;
-    int lo = 0, hi = nitems;
-    while(hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if(prefix[mid] <= g0) lo = mid; else hi = mid;
-    }
-    wit = lo;
-  }
   Rng rng;
   rng.k0 = (uint32_t)seed;
   rng.k1 = (uint32_t)(seed >> 32);
@@ -1683,22 +1697,27 @@ batch_kernel
     if(need) {
       const int leader = __ffs(need) - 1;
       unsigned long long base = 0;
-      int item = wit, got = 0;
+      int item = wit, got = 0, q = wq;
       if((int)lane == leader) {
-        /* The warp's item, or the next ones in turn, until one has work */
-        for(int k = 0; k < nitems; ++k) {
-          const unsigned long long budget = prefix[item + 1] - prefix[item];
-          if(*(volatile const unsigned long long*)(next_items + item) < budget) {
-            base = atomicAdd(next_items + item, (unsigned long long)__popc(need));
-            if(base < budget) { got = 1; break; }
+        /* The warp's position, or the next ones in turn, until an item has
+         * work */
+        for(int k = 0; k < npos; ++k) {
+          item = (q % seq_len) * ngroups + q / seq_len;
+          if(item < nitems) {
+            const unsigned long long budget = prefix[item + 1] - prefix[item];
+            if(*(volatile const unsigned long long*)(next_items + item) < budget) {
+              base = atomicAdd(next_items + item, (unsigned long long)__popc(need));
+              if(base < budget) { got = 1; break; }
+            }
           }
-          item = item + 1 == nitems ? 0 : item + 1;
+          q = q + 1 == npos ? 0 : q + 1;
         }
       }
       got = __shfl_sync(0xffffffffu, got, leader);
       item = __shfl_sync(0xffffffffu, item, leader);
+      q = __shfl_sync(0xffffffffu, q, leader);
       base = __shfl_sync(0xffffffffu, base, leader);
-      if(got) wit = item;
+      if(got) { wit = item; wq = q; }
       if(p.phase == PH_NONE && !done) {
         const unsigned long long g = base + __popc(need & ((1u << lane) - 1u));
         if(!got) {
@@ -1741,6 +1760,9 @@ batch_kernel
             const int nd = rcvd ? scenes[stag[prv]].nrcv * NRCV_Q * 2 : 0;
             for(int i = (int)lane; i < nd; i += 32) red_add(dst + i, sl[2 * NGLOBAL + i]);
           }
+          /* The lanes clear other entries than they flushed: every read of
+           * the slot before any clear */
+          __syncwarp();
           for(int i = (int)lane; i < ss; i += 32) sl[i] = 0;
           {
             const int* src = reinterpret_cast<const int*>(scenes + newest);
