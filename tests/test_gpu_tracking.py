@@ -110,3 +110,37 @@ def test_batch_globals_equal_the_estimators(product):
             assert g[k][0] == pytest.approx(v[0], rel=1e-14, abs=1e-12), k
             assert g[k][2] == pytest.approx(v[2], rel=1e-12, abs=1e-12), k
     batch.close()
+
+
+def test_tracking_receiver_sums_repeat(product):
+    """Receiver sums go through per-warp shared-memory slots that are
+    flushed and cleared whenever a warp moves to another item. Many small
+    items of ragged budgets make many such moves; three launches of the
+    same realisations must give the same receiver sums (to the order of the
+    FP64 additions) and the same per-primitive map."""
+    suns = W.sun_grid()[::4]
+    kw = dict(n_helio=300, receiver_cells=16)
+    s, h = W.heliostat_field(product, **kw)
+    hel, aims, sp = W.tracking_inputs(h, suns)
+    budgets = [20000 + 7919 * (i % 13) for i in range(len(suns))]
+    runs = []
+    for rep in range(3):
+        batch = P.Batch.tracking(s, hel, aims, sp)
+        rng = s.rng(seed=21)
+        batch.launch(rng, budgets)
+        ests = batch.finish(rng)
+        runs.append([(e.receiver(h["receiver"]),
+                      [c["incoming_flux"][0] for c in e.primitives(h["receiver"],
+                                                                   h["receiver_shape"])])
+                     for e in ests])
+        del ests
+        batch.close()
+    for i in range(len(suns)):
+        r0, m0 = runs[0][i]
+        for rep in (1, 2):
+            r, m = runs[rep][i]
+            for q in r0:
+                assert abs(r[q][0] - r0[q][0]) <= 1e-9 * max(1.0, abs(r0[q][0])), \
+                    (i, rep, q, r[q], r0[q])
+            assert max(abs(a - b) for a, b in zip(m, m0)) <= 1e-9 * max(1.0, max(map(abs, m0)))
+    s.close()
