@@ -42,7 +42,7 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 # of the same scenes (field: one sorted chunk of 2^24 paths at 3 blocks per SM;
 # beam-down: 4e6 paths) (dram__bytes_read.sum + dram__bytes_write.sum);
 # the traffic scales with the paths traced (per-thread frames written back)
-DRAM_BYTES_PER_PATH = {"field": (2602.7e6 + 16181.7e6) / 16777216,
+DRAM_BYTES_PER_PATH = {"field": (2811.7e6 + 16377.0e6) / 16777216,
                        "beamdown": (73.9e6 + 387.0e6) / 4e6}  # beam-down: id order
 
 # Kernels of one plain launch of n realisations: below 2^24 the realisation

@@ -633,23 +633,27 @@ __device__ bool trace_ray
         && N.count[0] >= 0;
     h[1] = slab(N.lo[1], N.hi[1], inv, oinv, tmin, best.t, te[1])
         && N.count[1] >= 0;
-    for(int k = 0; k < 2; ++k) {
-      if(!h[k]) continue;
-      if(N.count[k] > 0) {
-        for(int p = 0; p < N.count[k]; ++p) {
-          const uint32_t ref = N.count[k] == 1 ? (uint32_t)N.child[k]
-                                               : S.primrefs[N.child[k] + p];
-          if(!(FEAT & FEAT_QUADRIC) || primref_kind(ref) == PRIM_TRIANGLE) {
-            ++cnt.tris;
-            test_triangle(S, (int)primref_index(ref), o, d, sh, tmin, eps,
-                          self, best, found);
-          } else {
-            ++cnt.quads;
-            test_quadric(S, (int)primref_index(ref), o, d, tmin, self,
-                         best, found);
-          }
-          if(any && found) return true;
+    /* The hit leaves, slot 0 then slot 1, through one loop so that the
+     * primitive tests are inlined once (a loop over k would be unrolled
+     * and hold two copies of each) */
+    unsigned leaves = (h[0] && N.count[0] > 0 ? 1u : 0u) | (h[1] && N.count[1] > 0 ? 2u : 0u);
+    while(leaves) {
+      const bool k1 = (leaves & 1u) == 0u;
+      leaves &= leaves - 1u;
+      const int lc = k1 ? N.count[1] : N.count[0];
+      const int first = k1 ? N.child[1] : N.child[0];
+      for(int p = 0; p < lc; ++p) {
+        const uint32_t ref = lc == 1 ? (uint32_t)first : S.primrefs[first + p];
+        if(!(FEAT & FEAT_QUADRIC) || primref_kind(ref) == PRIM_TRIANGLE) {
+          ++cnt.tris;
+          test_triangle(S, (int)primref_index(ref), o, d, sh, tmin, eps,
+                        self, best, found);
+        } else {
+          ++cnt.quads;
+          test_quadric(S, (int)primref_index(ref), o, d, tmin, self,
+                       best, found);
         }
+        if(any && found) return true;
       }
     }
     const bool in0 = h[0] && N.count[0] == 0, in1 = h[1] && N.count[1] == 0;
