@@ -312,8 +312,8 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
       const Dd sm = ramp(u, A.lower[0], A.upper[0]) * ramp(v, A.lower[1], A.upper[1]);
       if(edge_only && !(sm.v > 0.0)) continue;
       w = w * sm;
-      atomicAdd(A.grad_abs + 2 * slot, w.a * A.inv_n);
-      atomicAdd(A.grad_abs + 2 * slot + 1, w.b * A.inv_n);
+      red_add_global(A.grad_abs + 2 * slot, w.a * A.inv_n);
+      red_add_global(A.grad_abs + 2 * slot + 1, w.b * A.inv_n);
     }
     /* Bilinear splat on the cell centres */
     const Dd fx = (u - A.lower[0]) * A.inv_cell[0] - 0.5;
@@ -332,7 +332,7 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
         const Dd c = w * (kx * ky);
         const int cell = cj * A.nx + ci;
         if(PASS == 0) {
-          atomicAdd(A.map + cell, c.v);
+          red_add_global(A.map + cell, c.v);
         } else {
           const double r = 2.0 * (A.map[cell] * A.map_scale - A.target);
           ga += r * c.a;
@@ -341,8 +341,8 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
       }
     }
     if(PASS == 1) {
-      atomicAdd(A.grad_spill + 2 * slot, ga * A.map_scale);
-      atomicAdd(A.grad_spill + 2 * slot + 1, gb * A.map_scale);
+      red_add_global(A.grad_spill + 2 * slot, ga * A.map_scale);
+      red_add_global(A.grad_spill + 2 * slot + 1, gb * A.map_scale);
     }
   }
   if(PASS == 0) {
@@ -352,9 +352,9 @@ adjoint_kernel(const DScene<R> S, const AdjointArgs A, uint64_t seed, uint64_t f
       s_hit += __shfl_down_sync(0xffffffffu, s_hit, o);
     }
     if((threadIdx.x & 31u) == 0) {
-      red_add(A.sums + 0, s_w);
-      red_add(A.sums + 1, s_w2);
-      red_add(A.sums + 2, s_hit);
+      red_add_global(A.sums + 0, s_w);
+      red_add_global(A.sums + 1, s_w2);
+      red_add_global(A.sums + 2, s_hit);
     }
   }
   unsigned long long c4[4] = {cnt.rays, cnt.nodes, cnt.tris, cnt.quads};

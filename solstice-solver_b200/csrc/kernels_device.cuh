@@ -901,12 +901,27 @@ __device__ __forceinline__ void red_add(double* p, double v)
 {
   if(v != 0.0) atomicAdd(p, v);
 }
+/* The same into device memory, as a reduction (no value comes back): an
+ * atomicAdd through a pointer that may address shared memory is a generic
+ * atomic whose sector returns to L1 */
+__device__ __forceinline__ void red_add_global(double* p, double v)
+{
+  if(v != 0.0)
+    asm volatile("red.global.add.f64 [%0], %1;"
+                 :: "l"(__cvta_generic_to_global(p)), "d"(v) : "memory");
+}
+__device__ __forceinline__ void red_inc_global(unsigned long long* p)
+{
+  asm volatile("red.global.add.u64 [%0], 1;"
+               :: "l"(__cvta_generic_to_global(p)) : "memory");
+}
 
 /* (w, w^2) of the 10 receiver quantities of one path, from its 6
  * accumulated values (MC_RECEIVER_DATA order, src/ssol_solver.c:735-755:
  * incoming, incoming if no atmosphere loss, if no field loss, lost in the
  * field, lost in the atmosphere, then the same 5 absorbed), added to dst. The values travel as scalars, so that
  * none of them goes through local memory. */
+template<bool GLOBAL>
 static __device__ __noinline__ void commit10
   (double* dst, double v0, double v1, double v2, double v3, double v4, double v5,
    double f)
@@ -915,13 +930,20 @@ static __device__ __noinline__ void commit10
                             f * v3, f * v4, f * v5, f * (v5 - v3), f * (v4 - v3)};
 #pragma unroll
   for(int k = 0; k < NRCV_Q; ++k) {
-    red_add(dst + 2 * k, q[k]);
-    red_add(dst + 2 * k + 1, q[k] * q[k]);
+    if(GLOBAL) {
+      red_add_global(dst + 2 * k, q[k]);
+      red_add_global(dst + 2 * k + 1, q[k] * q[k]);
+    } else {
+      red_add(dst + 2 * k, q[k]);
+      red_add(dst + 2 * k + 1, q[k] * q[k]);
+    }
   }
 }
+/* GLOBAL: dst is device memory (else shared or device memory) */
+template<bool GLOBAL>
 __device__ __forceinline__ void commit10(double* dst, const double v[6], double f)
 {
-  commit10(dst, v[0], v[1], v[2], v[3], v[4], v[5], f);
+  commit10<GLOBAL>(dst, v[0], v[1], v[2], v[3], v[4], v[5], f);
 }
 
 static __device__ __noinline__ void flush_racc(double* dst, const double* racc)
@@ -1173,7 +1195,7 @@ __device__ __noinline__ int commit_path_pe
    const double (*xv)[6], double* racc, int racc_slot, const DControl* ctl)
 {
   const int end = pe.end;
-  atomicAdd(&T.nb_samples[pe.samp], 1ull);
+  red_inc_global(&T.nb_samples[pe.samp]);
   if(end == END_FAIL) {
     /* The failure that reaches the limit stops the launch's work fetch
      * (src/ssol_solver.c:1240-1245) */
@@ -1203,10 +1225,10 @@ __device__ __noinline__ int commit_path_pe
   {
     const double wc = f * g[G_COS], ws = f * g[G_SHADOW];
     double* sp = T.samp + (size_t)pe.samp * 4;
-    red_add(sp + 0, wc);
-    red_add(sp + 1, wc * wc);
-    red_add(sp + 2, ws);
-    red_add(sp + 3, ws * ws);
+    red_add_global(sp + 0, wc);
+    red_add_global(sp + 1, wc * wc);
+    red_add_global(sp + 2, ws);
+    red_add_global(sp + 3, ws * ws);
   }
   if(pe.nent == 0) return racc_slot;
   double* rbase = smem_rcv ? smem_rcv : T.rcv;
@@ -1231,12 +1253,12 @@ __device__ __noinline__ int commit_path_pe
         racc[2 * k + 1] += q[k] * q[k];
       }
     } else {
-      commit10(rbase + (size_t)pe.r0 * NRCV_Q * 2, a0, a1, a2, a3, a4, a5, f);
+      commit10<false>(rbase + (size_t)pe.r0 * NRCV_Q * 2, a0, a1, a2, a3, a4, a5, f);
     }
-    commit10(T.samp_rcv + ((size_t)pe.samp * S.nrcv + pe.r0) * NRCV_Q * 2,
-             a0, a1, a2, a3, a4, a5, f);
+    commit10<true>(T.samp_rcv + ((size_t)pe.samp * S.nrcv + pe.r0) * NRCV_Q * 2,
+                   a0, a1, a2, a3, a4, a5, f);
     if(pe.p0 >= 0)
-      commit10(T.prim + (size_t)pe.p0 * NRCV_Q * 2, a0, a1, a2, a3, a4, a5, f);
+      commit10<true>(T.prim + (size_t)pe.p0 * NRCV_Q * 2, a0, a1, a2, a3, a4, a5, f);
     return racc_slot;
   }
   double v0[6];
@@ -1254,13 +1276,13 @@ __device__ __noinline__ int commit_path_pe
         if((k == 0 ? pe.r0 : xr[k - 1]) != re) continue;
         for(int q = 0; q < 6; ++q) v[q] += k == 0 ? v0[q] : xv[k - 1][q];
       }
-      commit10(rbase + (size_t)re * NRCV_Q * 2, v, f);
-      commit10(T.samp_rcv + ((size_t)pe.samp * S.nrcv + re) * NRCV_Q * 2, v, f);
+      commit10<false>(rbase + (size_t)re * NRCV_Q * 2, v, f);
+      commit10<true>(T.samp_rcv + ((size_t)pe.samp * S.nrcv + re) * NRCV_Q * 2, v, f);
     }
     const int prim = e == 0 ? pe.p0 : xp[e - 1];
     if(prim >= 0) {
       /* (receiver side, primitive) keys are unique among the entries */
-      commit10(T.prim + (size_t)prim * NRCV_Q * 2, e == 0 ? v0 : xv[e - 1], f);
+      commit10<true>(T.prim + (size_t)prim * NRCV_Q * 2, e == 0 ? v0 : xv[e - 1], f);
     }
   }
   return racc_slot;
@@ -1592,9 +1614,9 @@ realisation_kernel
   if(tid < 2 * NGLOBAL) {
     double v = 0;
     for(int w = 0; w < (bd >> 5); ++w) v += red[w][tid];
-    red_add(T.global + tid, v);
+    red_add_global(T.global + tid, v);
   }
-  for(int i = tid; i < rcv_doubles; i += bd) red_add(T.rcv + i, smem_rcv[i]);
+  for(int i = tid; i < rcv_doubles; i += bd) red_add_global(T.rcv + i, smem_rcv[i]);
 }
 
 /* Batched form: several scenes (e.g. one re-aimed field per sun position)
@@ -1879,10 +1901,12 @@ batch_kernel
   __syncwarp();
   for(int k = 0; k < 2; ++k) {
     if(stag[k] < 0) continue;
-    if((int)lane < 2 * NGLOBAL) red_add(tallies[stag[k]].global + lane, wslots[k * ss + lane]);
+    if((int)lane < 2 * NGLOBAL)
+      red_add(tallies[stag[k]].global + lane, wslots[k * ss + lane]);
     double* dst = tallies[stag[k]].rcv;
     const int nd = rcvd ? scenes[stag[k]].nrcv * NRCV_Q * 2 : 0;
-    for(int i = (int)lane; i < nd; i += 32) red_add(dst + i, wslots[k * ss + 2 * NGLOBAL + i]);
+    for(int i = (int)lane; i < nd; i += 32)
+      red_add(dst + i, wslots[k * ss + 2 * NGLOBAL + i]);
   }
   unsigned long long c[6] = {cnt.rays, cnt.nodes, cnt.tris, cnt.quads,
                              bounces, npaths};
