@@ -910,6 +910,12 @@ __device__ __forceinline__ void red_add_global(double* p, double v)
     asm volatile("red.global.add.f64 [%0], %1;"
                  :: "l"(__cvta_generic_to_global(p)), "d"(v) : "memory");
 }
+__device__ __forceinline__ void red_add_shared(double* p, double v)
+{
+  if(v != 0.0)
+    asm volatile("red.shared.add.f64 [%0], %1;"
+                 :: "r"((unsigned)__cvta_generic_to_shared(p)), "d"(v) : "memory");
+}
 __device__ __forceinline__ void red_inc_global(unsigned long long* p)
 {
   asm volatile("red.global.add.u64 [%0], 1;"
@@ -946,10 +952,16 @@ __device__ __forceinline__ void commit10(double* dst, const double v[6], double 
   commit10<GLOBAL>(dst, v[0], v[1], v[2], v[3], v[4], v[5], f);
 }
 
-static __device__ __noinline__ void flush_racc(double* dst, const double* racc)
+/* dst: shared memory when `shared`, else device memory */
+static __device__ __noinline__ void flush_racc(double* dst, const double* racc, bool shared)
 {
+  if(shared) {
 #pragma unroll 1
-  for(int k = 0; k < 2 * NRCV_Q; ++k) red_add(dst + k, racc[k]);
+    for(int k = 0; k < 2 * NRCV_Q; ++k) red_add_shared(dst + k, racc[k]);
+  } else {
+#pragma unroll 1
+    for(int k = 0; k < 2 * NRCV_Q; ++k) red_add_global(dst + k, racc[k]);
+  }
 }
 
 template<class R> struct PathState {
@@ -1240,7 +1252,8 @@ __device__ __noinline__ int commit_path_pe
       /* The thread's running sums of one receiver side, flushed when the
        * side changes: no atomics while its paths keep reaching it */
       if(racc_slot != pe.r0) {
-        if(racc_slot >= 0) flush_racc(rbase + (size_t)racc_slot * NRCV_Q * 2, racc);
+        if(racc_slot >= 0)
+          flush_racc(rbase + (size_t)racc_slot * NRCV_Q * 2, racc, smem_rcv != nullptr);
         racc_slot = pe.r0;
 #pragma unroll
         for(int k = 0; k < 2 * NRCV_Q; ++k) racc[k] = 0.0;
@@ -1595,7 +1608,8 @@ realisation_kernel
   }
 
   if(racc_slot >= 0)
-    flush_racc((use_smem_rcv ? smem_rcv : T.rcv) + (size_t)racc_slot * NRCV_Q * 2, racc);
+    flush_racc((use_smem_rcv ? smem_rcv : T.rcv) + (size_t)racc_slot * NRCV_Q * 2, racc,
+               use_smem_rcv);
 
   /* Warp then block reduction of the global sums, one commit per block */
   const int warp = tid >> 5;
@@ -1711,10 +1725,11 @@ batch_kernel
   int racc_slot = -1, racc_item = -1;
   auto racc_flush = [&]() {
     if(racc_slot < 0) return;
+    const bool in_slot = rcvd && (racc_item == stag[cur] || racc_item == stag[cur ^ 1]);
     double* dst = rcvd && racc_item == stag[cur] ? wslots + cur * ss + 2 * NGLOBAL
       : rcvd && racc_item == stag[cur ^ 1] ? wslots + (cur ^ 1) * ss + 2 * NGLOBAL
       : tallies[racc_item].rcv;
-    flush_racc(dst + (size_t)racc_slot * NRCV_Q * 2, racc);
+    flush_racc(dst + (size_t)racc_slot * NRCV_Q * 2, racc, in_slot);
     racc_slot = -1;
   };
 
