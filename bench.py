@@ -42,7 +42,7 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 # of the same scenes (field: one sorted chunk of 2^24 paths at 3 blocks per SM;
 # beam-down: 4e6 paths) (dram__bytes_read.sum + dram__bytes_write.sum);
 # the traffic scales with the paths traced (per-thread frames written back)
-DRAM_BYTES_PER_PATH = {"field": (2811.7e6 + 16377.0e6) / 16777216,
+DRAM_BYTES_PER_PATH = {"field": (2160.9e6 + 15301.9e6) / 16777216,
                        "beamdown": (73.9e6 + 387.0e6) / 4e6}  # beam-down: id order
 
 # Kernels of one plain launch of n realisations: below 2^24 the realisation
@@ -57,7 +57,7 @@ def launches_per_plain_launch(n):
 # Both passes of the adjoint kernel on the field, from a capture of 4e6 paths
 ADJOINT_DRAM_BYTES_PER_PATH = (2.34e6 + 21.63e6 + 6.28e6 + 54.82e6) / 4e6
 # Same for the batched kernel, from a capture of 32 suns (32245124 paths)
-BATCH_DRAM_BYTES_PER_PATH = (4412.5e6 + 22741.5e6) / 32245124
+BATCH_DRAM_BYTES_PER_PATH = (4249.9e6 + 22363.6e6) / 32245124
 
 
 def flops_per_run(st):
