@@ -55,7 +55,7 @@ SORT_MIN, SORT_CHUNK = 1 << 24, 1 << 24
 def launches_per_plain_launch(n):
     return 1 if n < SORT_MIN else 4 * ((n + SORT_CHUNK - 1) // SORT_CHUNK)
 # Both passes of the adjoint kernel on the field, from a capture of 4e6 paths
-ADJOINT_DRAM_BYTES_PER_PATH = (2.34e6 + 21.63e6 + 6.28e6 + 54.82e6) / 4e6
+ADJOINT_DRAM_BYTES_PER_PATH = (2.76e6 + 26.97e6 + 5.95e6 + 52.99e6) / 4e6
 # Same for the batched kernel, from a capture of 32 suns (32245124 paths)
 BATCH_DRAM_BYTES_PER_PATH = (4249.9e6 + 22363.6e6) / 32245124
 
