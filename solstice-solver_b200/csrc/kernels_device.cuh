@@ -549,8 +549,11 @@ __device__ __forceinline__ void test_quadric
   const R c = kx * ol.x * ol.x + ky * ol.y * ol.y + kz * zz * zz + lz * ol.z + m;
   R roots[2];
   const int n = solve_quadratic(a, b, c, roots);
+  /* Not unrolled: one inlined copy of the refinement, carving and normal
+   * code for both roots */
+#pragma unroll 1
   for(int k = 0; k < n; ++k) {
-    const R t = refine_root_general(Q.gen, ol, dl, roots[k]);
+    const R t = refine_root_general(Q.gen, ol, dl, k == 0 ? roots[0] : roots[1]);
     if(t <= tmin) continue;
     if(!(t < best.t)) break;
     const V3<R> pl = ol + dl * t;
@@ -790,7 +793,8 @@ __device__ __noinline__ bool shade
          * reflection falls below the surface */
         U32x4 rr = r;
         bool ok = false;
-        for(uint32_t k = 0; k < 16 && !ok; ++k) {
+#pragma unroll 1
+        for(uint32_t k = 0; k < 16; ++k) {
           if(k) rr = rng.get((scatter << 6) | k, RNG_RETRY);
           const R u0 = uni<R>(rr.v[0]);
           const R tan2 = m.distrib == DISTRIB_BECKMANN
@@ -804,6 +808,7 @@ __device__ __noinline__ bool shade
           if(!(wh > R(0))) continue;
           out = h * (R(2) * wh) - wo;
           ok = dot(out, N) > R(0);
+          if(ok) break;
         }
         prop = ok ? refl : R(0);
       }
