@@ -80,6 +80,8 @@ class Clocks:
         self.lines = []
 
     def start(self):
+        """Start sampling; returns once the first sample is in, so that the
+        timed region that follows is covered from its start."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
@@ -89,6 +91,11 @@ class Clocks:
             self.thread.start()
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 3.0 and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.mark = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -97,6 +104,13 @@ class Clocks:
     def stop(self):
         if not self.proc:
             return None
+        # A region shorter than the sampling period may hold no sample: then
+        # the samples just before and just after it bracket it
+        mark = getattr(self, "mark", 0)
+        t0 = time.time()
+        while len(self.lines) <= mark and time.time() - t0 < 0.5 and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.lines = self.lines[max(0, mark - 1):]
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
