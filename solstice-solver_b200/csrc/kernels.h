@@ -49,6 +49,29 @@ int launch_realisations_f64
 /* Batched launch: device arrays of per-item scenes and tallies, the item
  * budgets as an inclusive prefix (nitems + 1 entries; the last one is the
  * launch total) and the first realisation index of each item */
+/* Realisations per warp segment of the coherent order */
+constexpr uint32_t SORT_SEGMENT = 256;
+
+/* Coherent order of a batched launch (sorted_off null: id order). Per item,
+ * from prefix[item] on, sorted_off / sorted_draw hold its realisations'
+ * offsets in the item and primary draws (4 words each) in the order of their
+ * sampled primitive; seg_mul[item] is the stride of the order in which its
+ * warp segments are handed out (coprime with its number of full segments);
+ * bin_base[item] is its first histogram bin, nbins the bins of all items.
+ * keys, draws, hist and bin_off are the presort's scratch (launch total,
+ * launch total x 4 words, nbins, nbins). */
+struct BatchOrder {
+  uint32_t* sorted_off = nullptr;
+  uint32_t* sorted_draw = nullptr;
+  uint32_t* keys = nullptr;
+  uint32_t* draws = nullptr;
+  uint32_t* hist = nullptr;
+  uint32_t* bin_off = nullptr;
+  const uint32_t* bin_base = nullptr;
+  const uint32_t* seg_mul = nullptr;
+  uint32_t nbins = 0;
+};
+
 template<class R> struct BatchLaunch {
   const DScene<R>* scenes;
   const DTallies* tallies;
@@ -58,6 +81,7 @@ template<class R> struct BatchLaunch {
   uint64_t seed;
   unsigned long long* next_items; /* per-item work counters (scratch) */
   DStats* stats;
+  BatchOrder order;
 };
 
 int launch_batch_f32(const BatchLaunch<float>& b, const LaunchConfig& cfg,

@@ -98,7 +98,8 @@ static int launch_batch_noalloc_variant
   batch_kernel<R, MINB, FEAT><<<(unsigned)blocks, block, smem, s>>>
     (scenes, tallies, scratch + NOALLOC_PREFIX, scratch + NOALLOC_FIRSTS, nitems,
      seed, cfg.max_segments, scratch + NOALLOC_NEXT,
-     reinterpret_cast<DStats*>(scratch + NOALLOC_STATS), cfg.rcv_doubles);
+     reinterpret_cast<DStats*>(scratch + NOALLOC_STATS), cfg.rcv_doubles,
+     nullptr, nullptr, nullptr); /* id order: the coherent order needs scratch */
   return (int)cudaGetLastError();
 }
 

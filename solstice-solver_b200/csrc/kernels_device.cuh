@@ -1350,7 +1350,7 @@ constexpr uint64_t SORT_CHUNK = 1ull << 24; /* realisations per sorted chunk */
  * pay (4e6 paths: 442 sorted against 451 Mpaths/s; a loop of 256 per-sun
  * launches of ~1e6 paths took 0.75 s instead of 0.62) */
 constexpr uint64_t SORT_MIN = 1ull << 24;
-constexpr uint32_t SORT_SEG = 256; /* sorted realisations per warp segment */
+constexpr uint32_t SORT_SEG = SORT_SEGMENT; /* sorted realisations per warp segment */
 
 /* Append one vertex of a tracked path (src/ssol_solver.c:909-922, 1014-1019,
  * 1080-1083: the sun end, the sampled point, every hit and the end at
@@ -1652,7 +1652,8 @@ batch_kernel
    const unsigned long long* __restrict__ prefix,
    const unsigned long long* __restrict__ firsts, int nitems, uint64_t seed,
    unsigned long long max_segments, unsigned long long* next_items,
-   DStats* stats, int rcvd)
+   DStats* stats, int rcvd, const uint32_t* __restrict__ sorted_off,
+   const uint4* __restrict__ sorted_draw, const uint32_t* __restrict__ seg_mul)
 {
   extern __shared__ double smem[];
   const int bd = blockDim.x, tid = threadIdx.x;
@@ -1786,10 +1787,29 @@ batch_kernel
             }
             acc_item = it;
           }
-          const uint64_t id = firsts[it] + g;
+          /* Coherent order: the item's full warp segments of SORT_SEG
+           * sorted realisations in a strided order (so that the warps of an
+           * item group spread over its primitives), the ragged last one
+           * last; each record gives the realisation and its primary draw */
+          uint64_t off = g;
+          U32x4 r0;
+          if(sorted_off) {
+            const unsigned long long nfull = (prefix[it + 1] - prefix[it]) / SORT_SEG;
+            unsigned long long sg = g / SORT_SEG;
+            if(sg < nfull)
+              sg = nfull < 65536ull
+                ? (unsigned long long)((uint32_t)sg * seg_mul[it] % (uint32_t)nfull)
+                : sg * seg_mul[it] % nfull;
+            const unsigned long long rec = prefix[it] + sg * SORT_SEG + g % SORT_SEG;
+            off = sorted_off[rec];
+            const uint4 d = sorted_draw[rec];
+            r0 = {{d.x, d.y, d.z, d.w}};
+          }
+          const uint64_t id = firsts[it] + off;
           rng.i_lo = (uint32_t)id;
           rng.i_hi = (uint32_t)(id >> 32);
-          init_path<R, FEAT>(scene_of(it), rng, p, ps, bd);
+          if(!sorted_off) r0 = rng.get(0u, RNG_PRIMARY);
+          init_path<R, FEAT>(scene_of(it), rng, p, ps, bd, &r0);
           ++npaths;
         }
       }
@@ -2041,6 +2061,67 @@ static __global__ void __launch_bounds__(256) presort_scatter
   }
 }
 
+/* Coherent order of a batched launch. Every size comes from the launch's
+ * device arrays (prefix: the budgets' inclusive prefix, prefix[nitems] the
+ * total), so that a captured graph serves any budgets. Item of realisation
+ * j: prefix[item] <= j < prefix[item + 1]. */
+__device__ __forceinline__ int batch_item_of
+  (const unsigned long long* prefix, int nitems, unsigned long long j, int hint)
+{
+  if(prefix[hint] <= j && j < prefix[hint + 1]) return hint;
+  int lo = 0, hi = nitems;
+  while(hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if(prefix[mid] <= j) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+/* Primary draw and sampled primitive of every realisation of the launch,
+ * counted in one histogram whose bins run item by item (bin_base) */
+template<class R>
+__global__ void __launch_bounds__(256) batch_presort_count
+  (const DScene<R>* scenes, const unsigned long long* prefix,
+   const unsigned long long* firsts, int nitems, uint64_t seed,
+   const uint32_t* bin_base, uint32_t* keys, uint4* draws, uint32_t* hist)
+{
+  const unsigned long long total = prefix[nitems];
+  Rng rng;
+  rng.k0 = (uint32_t)seed;
+  rng.k1 = (uint32_t)(seed >> 32);
+  int item = 0;
+  for(unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+      j < total; j += (unsigned long long)gridDim.x * blockDim.x) {
+    item = batch_item_of(prefix, nitems, j, item);
+    const uint64_t id = firsts[item] + (j - prefix[item]);
+    rng.i_lo = (uint32_t)id;
+    rng.i_hi = (uint32_t)(id >> 32);
+    const U32x4 r0 = rng.get(0u, RNG_PRIMARY);
+    const int k = sample_prim(scenes[item], r0);
+    keys[j] = (uint32_t)k;
+    draws[j] = make_uint4(r0.v[0], r0.v[1], r0.v[2], r0.v[3]);
+    atomicAdd(&hist[bin_base[item] + (uint32_t)k], 1u);
+  }
+}
+
+/* Each realisation to the next free place of its (item, primitive) range,
+ * with its offset in the item */
+static __global__ void __launch_bounds__(256) batch_presort_scatter
+  (const unsigned long long* prefix, int nitems, const uint32_t* bin_base,
+   const uint32_t* keys, const uint4* draws, uint32_t* bin_off,
+   uint32_t* sorted_off, uint4* sorted_draw)
+{
+  const unsigned long long total = prefix[nitems];
+  int item = 0;
+  for(unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+      j < total; j += (unsigned long long)gridDim.x * blockDim.x) {
+    item = batch_item_of(prefix, nitems, j, item);
+    const uint32_t pos = atomicAdd(&bin_off[bin_base[item] + keys[j]], 1u);
+    sorted_off[pos] = (uint32_t)(j - prefix[item]);
+    sorted_draw[pos] = draws[j];
+  }
+}
+
 /* Per-device pool of the sort's scratch (kernels_plain.cu) */
 cudaMemPool_t sort_pool(int dev);
 
@@ -2206,11 +2287,24 @@ static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg
   const uint64_t blocks = cfg.grid_blocks > 0
     ? (uint64_t)cfg.grid_blocks
     : (uint64_t)nsm * (uint64_t)per_sm * (uint64_t)(cfg.waves > 0 ? cfg.waves : 1);
-  cudaMemsetAsync(b.next_items, 0, (size_t)b.nitems * sizeof(unsigned long long),
-                  (cudaStream_t)stream);
-  batch_kernel<R, MINB, FEAT><<<(unsigned)blocks, block, smem, (cudaStream_t)stream>>>
+  const cudaStream_t st = (cudaStream_t)stream;
+  const BatchOrder& o = b.order;
+  if(o.sorted_off) {
+    const unsigned sort_blocks = (unsigned)nsm * 8u;
+    cudaMemsetAsync(o.hist, 0, (size_t)o.nbins * sizeof(uint32_t), st);
+    batch_presort_count<R><<<sort_blocks, 256, 0, st>>>
+      (b.scenes, b.prefix, b.firsts, b.nitems, b.seed, o.bin_base, o.keys,
+       reinterpret_cast<uint4*>(o.draws), o.hist);
+    presort_scan<<<1, 1024, 0, st>>>(o.hist, o.bin_off, (int)o.nbins);
+    batch_presort_scatter<<<sort_blocks, 256, 0, st>>>
+      (b.prefix, b.nitems, o.bin_base, o.keys, reinterpret_cast<const uint4*>(o.draws),
+       o.bin_off, o.sorted_off, reinterpret_cast<uint4*>(o.sorted_draw));
+  }
+  cudaMemsetAsync(b.next_items, 0, (size_t)b.nitems * sizeof(unsigned long long), st);
+  batch_kernel<R, MINB, FEAT><<<(unsigned)blocks, block, smem, st>>>
     (b.scenes, b.tallies, b.prefix, b.firsts, b.nitems, b.seed, cfg.max_segments,
-     b.next_items, b.stats, cfg.rcv_doubles);
+     b.next_items, b.stats, cfg.rcv_doubles, o.sorted_off,
+     reinterpret_cast<const uint4*>(o.sorted_draw), o.seg_mul);
   return (int)cudaGetLastError();
 }
 

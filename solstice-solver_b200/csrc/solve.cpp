@@ -24,6 +24,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <numeric>
 #include <atomic>
 #include <thread>
 
@@ -1222,6 +1223,20 @@ struct ssol_b200_batch {
   uint64_t h_seed = 0;
   void* h_tally = nullptr; /* pinned tally read-back, allocated on first finish */
   size_t scene_alloc = 0, tally_alloc = 0; /* bytes of d_scene, d_tally */
+  /* Coherent order: sampled triangles per item, their histogram bins (all
+   * items), per item its first bin and its segment stride (in d_tally), and
+   * the presort's scratch (40 B per realisation, grown on demand) */
+  std::vector<uint32_t> nsamp;
+  uint32_t nbins = 0;
+  uint32_t* d_bin_base = nullptr;
+  uint32_t* d_hist = nullptr;
+  uint32_t* d_bin_off = nullptr;
+  uint32_t* d_mul = nullptr;
+  std::vector<uint32_t> h_mul;
+  void* d_sort = nullptr;
+  size_t sort_alloc = 0;
+  unsigned long long sort_cap = 0; /* realisations the scratch holds */
+  bool graph_sorted = false; /* order the captured graph runs in */
 };
 
 static void batch_release(ssol_b200_batch* b)
@@ -1230,6 +1245,7 @@ static void batch_release(ssol_b200_batch* b)
   if(b->graph) cudaGraphDestroy(b->graph);
   dev_free(b->dev, b->d_scene, b->scene_alloc);
   dev_free(b->dev, b->d_tally, b->tally_alloc);
+  dev_free(b->dev, b->d_sort, b->sort_alloc);
   host_free(b->dev, b->h_tally, b->tally_total);
   if(b->ev0) cudaEventDestroy(b->ev0);
   if(b->ev1) cudaEventDestroy(b->ev1);
@@ -1351,6 +1367,7 @@ extern "C" res_T ssol_b200_batch_create
   for(size_t i = 0; i < nscenes; ++i) {
     if(item_res[i] != RES_OK) { batch_release(b); return item_res[i]; }
     b->meta.push_back(f32.empty() ? f64[i].meta : f32[i].meta);
+    b->nsamp.push_back((uint32_t)(f32.empty() ? f64[i].samp.size() : f32[i].samp.size()));
   }
   res = device_bind(dev);
   if(res == RES_OK)
@@ -1388,6 +1405,24 @@ static res_T batch_tallies(ssol_b200_batch* b)
   off += (sizeof(DStats) + 255) & ~size_t(255);
   const size_t o_gather = off;
   off += (13 * nscenes * sizeof(double) + 255) & ~size_t(255);
+  /* Coherent order: per item its first histogram bin and segment stride,
+   * then the histogram and its ranges */
+  std::vector<uint32_t> bin_base(nscenes, 0);
+  uint64_t nbins = 0;
+  for(size_t i = 0; i < nscenes; ++i) {
+    bin_base[i] = (uint32_t)nbins;
+    nbins += i < b->nsamp.size() ? b->nsamp[i] : 0;
+  }
+  if(nbins > 0x7fffffffull) nbins = 0; /* no coherent order */
+  b->nbins = (uint32_t)nbins;
+  const size_t o_bin_base = off;
+  off += (nscenes * sizeof(uint32_t) + 255) & ~size_t(255);
+  const size_t o_mul = off;
+  off += (nscenes * sizeof(uint32_t) + 255) & ~size_t(255);
+  const size_t o_hist = off;
+  off += ((size_t)nbins * sizeof(uint32_t) + 255) & ~size_t(255);
+  const size_t o_bin_off = off;
+  off += ((size_t)nbins * sizeof(uint32_t) + 255) & ~size_t(255);
   if(dev_alloc(dev, &b->d_tally, off) != cudaSuccess) {
     b->d_tally = nullptr;
     return RES_MEM_ERR;
@@ -1403,8 +1438,15 @@ static res_T batch_tallies(ssol_b200_batch* b)
   b->d_next = (unsigned long long*)(base + o_next);
   b->d_stats = (DStats*)(base + o_stats);
   b->d_gather = (double*)(base + o_gather);
+  b->d_bin_base = (uint32_t*)(base + o_bin_base);
+  b->d_mul = (uint32_t*)(base + o_mul);
+  b->d_hist = (uint32_t*)(base + o_hist);
+  b->d_bin_off = (uint32_t*)(base + o_bin_off);
+  b->h_mul.assign(nscenes, 1u);
   const cudaStream_t s = (cudaStream_t)dev->stream;
   if(cudaMemcpyAsync((void*)b->d_tallies, T.data(), nscenes * sizeof(DTallies),
+                     cudaMemcpyHostToDevice, s) != cudaSuccess
+  || cudaMemcpyAsync(b->d_bin_base, bin_base.data(), nscenes * sizeof(uint32_t),
                      cudaMemcpyHostToDevice, s) != cudaSuccess
   || cudaStreamSynchronize(s) != cudaSuccess)
     return RES_UNKNOWN_ERR;
@@ -1650,6 +1692,8 @@ extern "C" res_T ssol_b200_batch_create_tracking
     }
   }
   b->meta.assign(nsuns, meta);
+  b->nsamp.assign(nsuns, (uint32_t)(opt.precision == SSOL_B200_FP32 ? f32.samp.size()
+                                                                     : f64.samp.size()));
   res = device_bind(dev);
   if(res == RES_OK)
     res = opt.precision == SSOL_B200_FP32
@@ -1698,9 +1742,30 @@ static LaunchConfig batch_config(const ssol_b200_batch* b)
   return cfg;
 }
 
-static res_T batch_graph(ssol_b200_batch* b, const ssp_rng* rng, cudaStream_t s)
+/* The launch's coherent order over the sort scratch (b->sort_cap
+ * realisations), or none */
+static BatchOrder batch_order(const ssol_b200_batch* b, bool sorted)
 {
-  if(b->graph_exec && b->graph_stream == s) return RES_OK;
+  BatchOrder o;
+  if(!sorted) return o;
+  const unsigned long long cap = b->sort_cap;
+  unsigned char* p = (unsigned char*)b->d_sort;
+  o.keys = (uint32_t*)p;
+  o.sorted_off = (uint32_t*)(p + cap * 4);
+  o.draws = (uint32_t*)(p + cap * 8);
+  o.sorted_draw = (uint32_t*)(p + cap * 24);
+  o.hist = b->d_hist;
+  o.bin_off = b->d_bin_off;
+  o.bin_base = b->d_bin_base;
+  o.seg_mul = b->d_mul;
+  o.nbins = b->nbins;
+  return o;
+}
+
+static res_T batch_graph(ssol_b200_batch* b, const ssp_rng* rng, cudaStream_t s,
+                         bool sorted)
+{
+  if(b->graph_exec && b->graph_stream == s && b->graph_sorted == sorted) return RES_OK;
   if(b->graph_exec) { cudaGraphExecDestroy(b->graph_exec); b->graph_exec = nullptr; }
   if(b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
   const LaunchConfig cfg = batch_config(b);
@@ -1710,12 +1775,12 @@ static res_T batch_graph(ssol_b200_batch* b, const ssp_rng* rng, cudaStream_t s)
   if(b->opt.precision == SSOL_B200_FP32) {
     BatchLaunch<float> L = {(const DScene<float>*)b->d_scenes, b->d_tallies,
       b->d_prefix, b->d_firsts, (int)b->scenes.size(), rng->seed, b->d_next,
-      b->d_stats};
+      b->d_stats, batch_order(b, sorted)};
     err = launch_batch_f32(L, cfg, s);
   } else {
     BatchLaunch<double> L = {(const DScene<double>*)b->d_scenes, b->d_tallies,
       b->d_prefix, b->d_firsts, (int)b->scenes.size(), rng->seed, b->d_next,
-      b->d_stats};
+      b->d_stats, batch_order(b, sorted)};
     err = launch_batch_f64(L, cfg, s);
   }
   const cudaError_t e2 = cudaStreamEndCapture(s, &b->graph);
@@ -1723,7 +1788,50 @@ static res_T batch_graph(ssol_b200_batch* b, const ssp_rng* rng, cudaStream_t s)
   if(cudaGraphInstantiate(&b->graph_exec, b->graph, 0) != cudaSuccess)
     return RES_UNKNOWN_ERR;
   b->graph_stream = s;
+  b->graph_sorted = sorted;
   return RES_OK;
+}
+
+/* Launches of at least BATCH_SORT_MIN realisations run in the coherent order
+ * (up to BATCH_SORT_MAX: the scratch takes 40 B per realisation, and the
+ * sorted offsets are 32-bit) */
+constexpr unsigned long long BATCH_SORT_MIN = 1ull << 22;
+constexpr unsigned long long BATCH_SORT_MAX = 1ull << 29;
+
+/* Whether this launch runs in the coherent order; grows the scratch (and
+ * drops the captured graph, which holds its address) as needed */
+static bool batch_prepare_order(ssol_b200_batch* b, unsigned long long total)
+{
+  if(!b->nbins || total < BATCH_SORT_MIN || total > BATCH_SORT_MAX) return false;
+  for(const uint32_t n : b->nsamp) if(n < 2) return false;
+  if(total > b->sort_cap) {
+    /* one allocation for several launches: a quarter more than asked */
+    unsigned long long cap = total + total / 4;
+    if(cap > BATCH_SORT_MAX) cap = BATCH_SORT_MAX;
+    /* a multiple of 256 keeps every array of the scratch 16-byte aligned */
+    cap = (cap + 255) & ~255ull;
+    void* p = nullptr;
+    if(dev_alloc(b->dev, &p, (size_t)cap * 40) != cudaSuccess) return false;
+    if(b->graph_exec) { cudaGraphExecDestroy(b->graph_exec); b->graph_exec = nullptr; }
+    dev_free(b->dev, b->d_sort, b->sort_alloc);
+    b->d_sort = p;
+    b->sort_alloc = (size_t)cap * 40;
+    b->sort_cap = cap;
+  }
+  /* Per item, the stride of its full segments' order: near n / golden
+   * ratio, coprime with n, below n */
+  const size_t n = b->scenes.size();
+  for(size_t i = 0; i < n; ++i) {
+    const unsigned long long nfull = (b->h_prefix[i + 1] - b->h_prefix[i]) / SORT_SEGMENT;
+    unsigned long long mul = 1;
+    if(nfull > 1) {
+      mul = (unsigned long long)(0.6180339887 * (double)nfull) | 1ull;
+      while(std::gcd(mul, nfull) != 1ull) mul += 2;
+      mul %= nfull;
+    }
+    b->h_mul[i] = (uint32_t)mul;
+  }
+  return true;
 }
 
 extern "C" res_T ssol_b200_batch_launch
@@ -1746,12 +1854,15 @@ extern "C" res_T ssol_b200_batch_launch
     b->graph_exec = nullptr;
   }
   b->h_seed = rng->seed;
-  res_T res = batch_graph(b, rng, s);
+  const bool sorted = batch_prepare_order(b, total);
+  res_T res = batch_graph(b, rng, s, sorted);
   if(res != RES_OK) return res;
   if(cudaMemcpyAsync(b->d_prefix, b->h_prefix.data(), (n + 1) * sizeof(unsigned long long),
                      cudaMemcpyHostToDevice, s) != cudaSuccess
   || cudaMemcpyAsync(b->d_firsts, b->h_firsts.data(), n * sizeof(unsigned long long),
-                     cudaMemcpyHostToDevice, s) != cudaSuccess)
+                     cudaMemcpyHostToDevice, s) != cudaSuccess
+  || (sorted && cudaMemcpyAsync(b->d_mul, b->h_mul.data(), n * sizeof(uint32_t),
+                                cudaMemcpyHostToDevice, s) != cudaSuccess))
     return RES_UNKNOWN_ERR;
   cudaEventRecord(b->ev0, s);
   if(cudaGraphLaunch(b->graph_exec, s) != cudaSuccess) return RES_UNKNOWN_ERR;

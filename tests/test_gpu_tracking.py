@@ -25,8 +25,9 @@ def _suns(k):
     return [grid[i * 16 + (i * 7) % 16] for i in range(0, 16, 16 // k)]
 
 
-@pytest.mark.parametrize("precision", [P.FP32, P.FP64])
-def test_tracking_items_equal_host_built_fields(product, precision):
+@pytest.mark.parametrize("precision,scale", [(P.FP32, 1), (P.FP64, 1), (P.FP32, 2)])
+def test_tracking_items_equal_host_built_fields(product, precision, scale):
+    """scale 2 takes the launch above 2^22 realisations: the coherent order"""
     suns = _suns(8)
     kw = dict(n_helio=300, receiver_cells=16)
     s, h = W.heliostat_field(product, **kw)
@@ -34,7 +35,7 @@ def test_tracking_items_equal_host_built_fields(product, precision):
     opts = P.options(precision)
     batch = P.Batch.tracking(s, hel, aims, sp, opts)
     rng = s.rng(seed=5)
-    budgets = [300000 + 50000 * i for i in range(len(suns))]
+    budgets = [scale * (300000 + 50000 * i) for i in range(len(suns))]
     batch.launch(rng, budgets)
     ests = batch.finish(rng)
     for sun, est, n in zip(suns, ests, budgets):
