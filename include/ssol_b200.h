@@ -234,7 +234,7 @@ SSOL_API res_T ssol_b200_batch_reset(struct ssol_b200_batch* batch, void* stream
  * the last reset). Returns when the launch has completed. A launch of at
  * least 2^22 and at most 2^29 realisations in all runs them in the order of
  * their sampled primitives (the same paths, only the order of the FP64 sums
- * changes); for that the batch keeps a device scratch of 40 bytes per
+ * changes); for that the batch keeps a device scratch of 20 bytes per
  * realisation of its largest such launch (plus a quarter), released with
  * the batch. */
 SSOL_API res_T ssol_b200_batch_launch

@@ -58,13 +58,10 @@ constexpr uint32_t SORT_SEGMENT = 256;
  * sampled primitive; seg_mul[item] is the stride of the order in which its
  * warp segments are handed out (coprime with its number of full segments);
  * bin_base[item] is its first histogram bin, nbins the bins of all items.
- * keys, draws, hist and bin_off are the presort's scratch (launch total,
- * launch total x 4 words, nbins, nbins). */
+ * hist and bin_off are the presort's histogram and ranges (nbins each). */
 struct BatchOrder {
   uint32_t* sorted_off = nullptr;
   uint32_t* sorted_draw = nullptr;
-  uint32_t* keys = nullptr;
-  uint32_t* draws = nullptr;
   uint32_t* hist = nullptr;
   uint32_t* bin_off = nullptr;
   const uint32_t* bin_base = nullptr;

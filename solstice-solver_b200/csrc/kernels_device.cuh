@@ -2077,13 +2077,39 @@ __device__ __forceinline__ int batch_item_of
   return lo;
 }
 
-/* Primary draw and sampled primitive of every realisation of the launch,
- * counted in one histogram whose bins run item by item (bin_base) */
+/* Sampled primitive of every realisation of the launch, counted in one
+ * histogram whose bins run item by item (bin_base) */
 template<class R>
 __global__ void __launch_bounds__(256) batch_presort_count
   (const DScene<R>* scenes, const unsigned long long* prefix,
    const unsigned long long* firsts, int nitems, uint64_t seed,
-   const uint32_t* bin_base, uint32_t* keys, uint4* draws, uint32_t* hist)
+   const uint32_t* bin_base, uint32_t* hist)
+{
+  const unsigned long long total = prefix[nitems];
+  Rng rng;
+  rng.k0 = (uint32_t)seed;
+  rng.k1 = (uint32_t)(seed >> 32);
+  int item = 0;
+  for(unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+      j < total; j += (unsigned long long)gridDim.x * blockDim.x) {
+    item = batch_item_of(prefix, nitems, j, item);
+    const uint64_t id = firsts[item] + (j - prefix[item]);
+    rng.i_lo = (uint32_t)id;
+    rng.i_hi = (uint32_t)(id >> 32);
+    const int k = sample_prim(scenes[item], rng.get(0u, RNG_PRIMARY));
+    atomicAdd(&hist[bin_base[item] + (uint32_t)k], 1u);
+  }
+}
+
+/* Each realisation to the next free place of its (item, primitive) range,
+ * with its offset in the item and its primary draw (drawn again: the
+ * scratch keeps only the sorted records, 20 B per realisation) */
+template<class R>
+__global__ void __launch_bounds__(256) batch_presort_scatter
+  (const DScene<R>* scenes, const unsigned long long* prefix,
+   const unsigned long long* firsts, int nitems, uint64_t seed,
+   const uint32_t* bin_base, uint32_t* bin_off, uint32_t* sorted_off,
+   uint4* sorted_draw)
 {
   const unsigned long long total = prefix[nitems];
   Rng rng;
@@ -2098,27 +2124,9 @@ __global__ void __launch_bounds__(256) batch_presort_count
     rng.i_hi = (uint32_t)(id >> 32);
     const U32x4 r0 = rng.get(0u, RNG_PRIMARY);
     const int k = sample_prim(scenes[item], r0);
-    keys[j] = (uint32_t)k;
-    draws[j] = make_uint4(r0.v[0], r0.v[1], r0.v[2], r0.v[3]);
-    atomicAdd(&hist[bin_base[item] + (uint32_t)k], 1u);
-  }
-}
-
-/* Each realisation to the next free place of its (item, primitive) range,
- * with its offset in the item */
-static __global__ void __launch_bounds__(256) batch_presort_scatter
-  (const unsigned long long* prefix, int nitems, const uint32_t* bin_base,
-   const uint32_t* keys, const uint4* draws, uint32_t* bin_off,
-   uint32_t* sorted_off, uint4* sorted_draw)
-{
-  const unsigned long long total = prefix[nitems];
-  int item = 0;
-  for(unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-      j < total; j += (unsigned long long)gridDim.x * blockDim.x) {
-    item = batch_item_of(prefix, nitems, j, item);
-    const uint32_t pos = atomicAdd(&bin_off[bin_base[item] + keys[j]], 1u);
+    const uint32_t pos = atomicAdd(&bin_off[bin_base[item] + (uint32_t)k], 1u);
     sorted_off[pos] = (uint32_t)(j - prefix[item]);
-    sorted_draw[pos] = draws[j];
+    sorted_draw[pos] = make_uint4(r0.v[0], r0.v[1], r0.v[2], r0.v[3]);
   }
 }
 
@@ -2293,12 +2301,11 @@ static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg
     const unsigned sort_blocks = (unsigned)nsm * 8u;
     cudaMemsetAsync(o.hist, 0, (size_t)o.nbins * sizeof(uint32_t), st);
     batch_presort_count<R><<<sort_blocks, 256, 0, st>>>
-      (b.scenes, b.prefix, b.firsts, b.nitems, b.seed, o.bin_base, o.keys,
-       reinterpret_cast<uint4*>(o.draws), o.hist);
+      (b.scenes, b.prefix, b.firsts, b.nitems, b.seed, o.bin_base, o.hist);
     presort_scan<<<1, 1024, 0, st>>>(o.hist, o.bin_off, (int)o.nbins);
-    batch_presort_scatter<<<sort_blocks, 256, 0, st>>>
-      (b.prefix, b.nitems, o.bin_base, o.keys, reinterpret_cast<const uint4*>(o.draws),
-       o.bin_off, o.sorted_off, reinterpret_cast<uint4*>(o.sorted_draw));
+    batch_presort_scatter<R><<<sort_blocks, 256, 0, st>>>
+      (b.scenes, b.prefix, b.firsts, b.nitems, b.seed, o.bin_base, o.bin_off,
+       o.sorted_off, reinterpret_cast<uint4*>(o.sorted_draw));
   }
   cudaMemsetAsync(b.next_items, 0, (size_t)b.nitems * sizeof(unsigned long long), st);
   batch_kernel<R, MINB, FEAT><<<(unsigned)blocks, block, smem, st>>>

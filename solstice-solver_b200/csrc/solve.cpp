@@ -88,7 +88,7 @@ struct MemCache {
   std::vector<std::pair<void*, size_t>> pinned; /* page-locked host blocks */
 };
 constexpr size_t CACHE_BLOCKS = 8;
-constexpr size_t CACHE_BYTES = size_t(4) << 30;
+constexpr size_t CACHE_BYTES = size_t(16) << 30;
 constexpr size_t PINNED_BLOCKS = 4;
 constexpr size_t PINNED_BYTES = size_t(2) << 30;
 }
@@ -157,7 +157,16 @@ static cudaError_t dev_alloc(ssol_device* dev, void** p, size_t bytes)
       return cudaSuccess;
     }
   }
-  return cudaMalloc(p, bytes);
+  cudaError_t e = cudaMalloc(p, bytes);
+  if(e != cudaSuccess && c) {
+    /* Out of memory: give the cached blocks back and try once more */
+    cudaGetLastError();
+    std::lock_guard<std::mutex> g(c->lock);
+    for(const auto& blk : c->blocks) cudaFree(blk.first);
+    c->blocks.clear();
+    e = cudaMalloc(p, bytes);
+  }
+  return e;
 }
 
 /* Work still queued on the block finishes first (a cudaFree would have
@@ -1225,7 +1234,7 @@ struct ssol_b200_batch {
   size_t scene_alloc = 0, tally_alloc = 0; /* bytes of d_scene, d_tally */
   /* Coherent order: sampled triangles per item, their histogram bins (all
    * items), per item its first bin and its segment stride (in d_tally), and
-   * the presort's scratch (40 B per realisation, grown on demand) */
+   * the presort's scratch (20 B per realisation, grown on demand) */
   std::vector<uint32_t> nsamp;
   uint32_t nbins = 0;
   uint32_t* d_bin_base = nullptr;
@@ -1750,10 +1759,8 @@ static BatchOrder batch_order(const ssol_b200_batch* b, bool sorted)
   if(!sorted) return o;
   const unsigned long long cap = b->sort_cap;
   unsigned char* p = (unsigned char*)b->d_sort;
-  o.keys = (uint32_t*)p;
-  o.sorted_off = (uint32_t*)(p + cap * 4);
-  o.draws = (uint32_t*)(p + cap * 8);
-  o.sorted_draw = (uint32_t*)(p + cap * 24);
+  o.sorted_draw = (uint32_t*)p;
+  o.sorted_off = (uint32_t*)(p + cap * 16);
   o.hist = b->d_hist;
   o.bin_off = b->d_bin_off;
   o.bin_base = b->d_bin_base;
@@ -1793,7 +1800,7 @@ static res_T batch_graph(ssol_b200_batch* b, const ssp_rng* rng, cudaStream_t s,
 }
 
 /* Launches of at least BATCH_SORT_MIN realisations run in the coherent order
- * (up to BATCH_SORT_MAX: the scratch takes 40 B per realisation, and the
+ * (up to BATCH_SORT_MAX: the scratch takes 20 B per realisation, and the
  * sorted offsets are 32-bit) */
 constexpr unsigned long long BATCH_SORT_MIN = 1ull << 22;
 constexpr unsigned long long BATCH_SORT_MAX = 1ull << 29;
@@ -1808,14 +1815,14 @@ static bool batch_prepare_order(ssol_b200_batch* b, unsigned long long total)
     /* one allocation for several launches: a quarter more than asked */
     unsigned long long cap = total + total / 4;
     if(cap > BATCH_SORT_MAX) cap = BATCH_SORT_MAX;
-    /* a multiple of 256 keeps every array of the scratch 16-byte aligned */
+    /* a multiple of 256: the offsets after the draws start on 256 bytes */
     cap = (cap + 255) & ~255ull;
     void* p = nullptr;
-    if(dev_alloc(b->dev, &p, (size_t)cap * 40) != cudaSuccess) return false;
+    if(dev_alloc(b->dev, &p, (size_t)cap * 20) != cudaSuccess) return false;
     if(b->graph_exec) { cudaGraphExecDestroy(b->graph_exec); b->graph_exec = nullptr; }
     dev_free(b->dev, b->d_sort, b->sort_alloc);
     b->d_sort = p;
-    b->sort_alloc = (size_t)cap * 40;
+    b->sort_alloc = (size_t)cap * 20;
     b->sort_cap = cap;
   }
   /* Per item, the stride of its full segments' order: near n / golden
