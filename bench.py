@@ -57,7 +57,7 @@ def launches_per_plain_launch(n):
 # Both passes of the adjoint kernel on the field, from a capture of 4e6 paths
 ADJOINT_DRAM_BYTES_PER_PATH = (2.76e6 + 26.97e6 + 5.95e6 + 52.99e6) / 4e6
 # Same for the batched kernel, from a capture of 32 suns (32245124 paths)
-BATCH_DRAM_BYTES_PER_PATH = (4249.9e6 + 22363.6e6) / 32245124
+BATCH_DRAM_BYTES_PER_PATH = (3918.3e6 + 18098.4e6) / 32245124
 
 
 def flops_per_run(st):
