@@ -505,11 +505,61 @@ def run_b200(args):
                     "plain_fp32_ssol_solve_loop: one ssol_solve per sun (wall clock); "
                     "from_scratch: pilot of 1e5 per sun, read-back, then the rest, "
                     "set-up included (wall clock)"}
+    if (args.config == "field" and args.heliostats == 1000 and not args.no_suns
+            and not args.no_others and world == 1 and rank == 0):
+        line["other_configs"] = other_configs()
     if rank == 0:
         print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# The other workloads of the repo, measured by the default line too (each in
+# a child process of its own, as `bench.py --config X` would run it, with
+# 3 warm-up and 3 timed steps)
+OTHER_CONFIGS = (
+    ("beamdown", ["--config", "beamdown", "--steps", "3", "--warmup", "3", "--no-cpu"]),
+    ("adjoint", ["--config", "adjoint", "--steps", "3", "--warmup", "3", "--no-cpu"]),
+    ("draft", ["--config", "draft", "--steps", "3", "--warmup", "3", "--no-cpu"]),
+    ("pt", ["--config", "pt", "--steps", "3", "--warmup", "3", "--no-cpu"]),
+)
+
+
+def other_configs():
+    """Run OTHER_CONFIGS one after the other; per config the key figures of
+    its JSON line (or why it has none)."""
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "LOCAL_WORLD_SIZE",
+                        "MASTER_ADDR", "MASTER_PORT", "GROUP_RANK")
+           and not k.startswith("TORCHELASTIC")}
+    out = {}
+    for name, flags in OTHER_CONFIGS:
+        try:
+            proc = subprocess.run([sys.executable, os.path.abspath(__file__)] + flags,
+                                  capture_output=True, text=True, timeout=900, env=env)
+            lines = [ln for ln in proc.stdout.splitlines() if ln.startswith("{")]
+            if proc.returncode != 0 or not lines:
+                out[name] = {"failed": "exit %d: %s" % (proc.returncode,
+                                                        proc.stderr.strip()[-300:])}
+                continue
+            d = json.loads(lines[-1])
+            r = {"workload": (d.get("config") or {}).get("workload"),
+                 "value": d.get("value"), "unit": d.get("unit"),
+                 "ms_per_step": d.get("ms_per_step"), "steps": d.get("steps"),
+                 "warmup": d.get("warmup"), "dtype": d.get("dtype"),
+                 "e2e": (d.get("e2e") or {}).get("value"),
+                 "roofline_frac": (d.get("roofline") or {}).get("frac"),
+                 "clocks": d.get("clocks")}
+            if d.get("precision_vs_fp64"):
+                r["precision_vs_fp64_max_rel_diff"] = d["precision_vs_fp64"].get(
+                    "max_abs_rel_diff")
+            if d.get("fd_check"):
+                r["fd_check"] = d["fd_check"]
+            out[name] = r
+        except Exception as exc:
+            out[name] = {"failed": str(exc)}
+    return out
 
 
 SUNS = ("256 suns (16 elevations 5-85 deg x 16 azimuths, DNI U[300,1000]) over the "
@@ -1170,7 +1220,10 @@ def main():
                    help="skip the FP32 vs all-FP64 comparison of the field configs")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-suns", action="store_true",
-                   help="field config: skip the 256-sun time-to-SE comparison")
+                   help="field config: skip the 256-sun time-to-SE comparison (and the "
+                        "other configs)")
+    p.add_argument("--no-others", action="store_true",
+                   help="field config: skip the short runs of the other configs")
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--ref-step-seconds", type=float, default=10.0)
     args = p.parse_args()
