@@ -1345,11 +1345,11 @@ constexpr unsigned long long BATCH_LARGE_ITEM = 400000;
 /* Coherent order (see presort_count) */
 constexpr int SORT_MAX_BINS = 12288; /* shared-memory histogram of primitives */
 constexpr uint64_t SORT_CHUNK = 1ull << 24; /* realisations per sorted chunk */
-/* Smaller launches keep the id order: below a full chunk the warps get too
- * few segments each (the last ones leave lanes idle) and the presort does not
- * pay (4e6 paths: 442 sorted against 451 Mpaths/s; a loop of 256 per-sun
- * launches of ~1e6 paths took 0.75 s instead of 0.62) */
-constexpr uint64_t SORT_MIN = 1ull << 24;
+/* Smaller launches keep the id order: there the warps get few segments each
+ * (the last ones leave lanes idle) and the presort does not pay. On the field
+ * (Mpaths/s, sorted against id order): 1e6 paths 596 / 597, 4e6 615 / 632,
+ * 8e6 652 / 637, 1.6e7 675 / 640 */
+constexpr uint64_t SORT_MIN = 6000000;
 constexpr uint32_t SORT_SEG = SORT_SEGMENT; /* sorted realisations per warp segment */
 
 /* Append one vertex of a tracked path (src/ssol_solver.c:909-922, 1014-1019,
@@ -1967,12 +1967,11 @@ batch_kernel
  * does not draw it again.
  ******************************************************************************/
 
-/* Primary draw and sampled primitive of realisation first + j; histogram of
- * the primitives, per block in shared memory */
+/* Sampled primitive of realisation first + j, counted per block in shared
+ * memory */
 template<class R>
 __global__ void __launch_bounds__(256) presort_count
-  (const DScene<R> S, uint64_t seed, uint64_t first, uint32_t n, uint32_t* keys,
-   uint4* draws, uint32_t* hist)
+  (const DScene<R> S, uint64_t seed, uint64_t first, uint32_t n, uint32_t* hist)
 {
   __shared__ uint32_t h[SORT_MAX_BINS];
   for(int i = threadIdx.x; i < S.nsamp; i += blockDim.x) h[i] = 0;
@@ -1985,11 +1984,7 @@ __global__ void __launch_bounds__(256) presort_count
     const uint64_t id = first + j;
     rng.i_lo = (uint32_t)id;
     rng.i_hi = (uint32_t)(id >> 32);
-    const U32x4 r0 = rng.get(0u, RNG_PRIMARY);
-    const int k = sample_prim(S, r0);
-    keys[j] = (uint32_t)k;
-    draws[j] = make_uint4(r0.v[0], r0.v[1], r0.v[2], r0.v[3]);
-    atomicAdd(&h[k], 1u);
+    atomicAdd(&h[sample_prim(S, rng.get(0u, RNG_PRIMARY))], 1u);
   }
   __syncthreads();
   for(int i = threadIdx.x; i < S.nsamp; i += blockDim.x)
@@ -2028,12 +2023,17 @@ static __global__ void __launch_bounds__(1024) presort_scan
  * realisation */
 constexpr int SCATTER_PER = 16;
 
-static __global__ void __launch_bounds__(256) presort_scatter
-  (const uint32_t* keys, const uint4* draws, uint32_t n, uint32_t* off,
-   uint4* out_draws, uint32_t* out_off, int nb)
+template<class R>
+__global__ void __launch_bounds__(256) presort_scatter
+  (const DScene<R> S, uint64_t seed, uint64_t first, uint32_t n, uint32_t* off,
+   uint4* out_draws, uint32_t* out_off)
 {
   __shared__ uint32_t cnt[SORT_MAX_BINS];
+  const int nb = S.nsamp;
   const uint32_t tile = 256u * SCATTER_PER;
+  Rng rng;
+  rng.k0 = (uint32_t)seed;
+  rng.k1 = (uint32_t)(seed >> 32);
   for(uint32_t t0 = blockIdx.x * tile; t0 < n; t0 += gridDim.x * tile) {
     for(int i = threadIdx.x; i < nb; i += 256) cnt[i] = 0;
     __syncthreads();
@@ -2041,19 +2041,32 @@ static __global__ void __launch_bounds__(256) presort_scatter
 #pragma unroll
     for(int e = 0; e < SCATTER_PER; ++e) {
       const uint32_t j = t0 + e * 256u + threadIdx.x;
-      k[e] = j < n ? keys[j] : 0u;
-      rank[e] = j < n ? atomicAdd(&cnt[k[e]], 1u) : 0u;
+      k[e] = 0u;
+      rank[e] = 0u;
+      if(j < n) {
+        const uint64_t id = first + j;
+        rng.i_lo = (uint32_t)id;
+        rng.i_hi = (uint32_t)(id >> 32);
+        k[e] = (uint32_t)sample_prim(S, rng.get(0u, RNG_PRIMARY));
+        rank[e] = atomicAdd(&cnt[k[e]], 1u);
+      }
     }
     __syncthreads();
     for(int i = threadIdx.x; i < nb; i += 256)
       if(cnt[i]) cnt[i] = atomicAdd(&off[i], cnt[i]);
     __syncthreads();
+    /* The draws again rather than kept: 16 more registers per realisation
+     * of the tile, or 20 B of scratch per realisation */
 #pragma unroll
     for(int e = 0; e < SCATTER_PER; ++e) {
       const uint32_t j = t0 + e * 256u + threadIdx.x;
       if(j < n) {
         const uint32_t pos = cnt[k[e]] + rank[e];
-        out_draws[pos] = draws[j];
+        const uint64_t id = first + j;
+        rng.i_lo = (uint32_t)id;
+        rng.i_hi = (uint32_t)(id >> 32);
+        const U32x4 r0 = rng.get(0u, RNG_PRIMARY);
+        out_draws[pos] = make_uint4(r0.v[0], r0.v[1], r0.v[2], r0.v[3]);
         out_off[pos] = j;
       }
     }
@@ -2197,9 +2210,7 @@ static int launch_variant
     return (int)cudaGetLastError();
   }
   const uint64_t chunk = count < SORT_CHUNK ? count : SORT_CHUNK;
-  const size_t o_keys = 0;
-  const size_t o_draws = o_keys + align256(chunk * sizeof(uint32_t));
-  const size_t o_sdraws = o_draws + align256(chunk * sizeof(uint4));
+  const size_t o_sdraws = 0;
   const size_t o_soff = o_sdraws + align256(chunk * sizeof(uint4));
   const size_t o_hist = o_soff + align256(chunk * sizeof(uint32_t));
   const size_t o_off = o_hist + align256((size_t)S.nsamp * sizeof(uint32_t));
@@ -2208,8 +2219,6 @@ static int launch_variant
   unsigned char* buf = nullptr;
   if(!pool || cudaMallocFromPoolAsync((void**)&buf, bytes, pool, st) != cudaSuccess)
     return (int)cudaErrorMemoryAllocation;
-  uint32_t* keys = (uint32_t*)(buf + o_keys);
-  uint4* draws = (uint4*)(buf + o_draws);
   uint4* sdraws = (uint4*)(buf + o_sdraws);
   uint32_t* soff = (uint32_t*)(buf + o_soff);
   uint32_t* hist = (uint32_t*)(buf + o_hist);
@@ -2218,10 +2227,10 @@ static int launch_variant
   for(uint64_t c0 = 0; c0 < count; c0 += chunk) {
     const uint32_t n = (uint32_t)(count - c0 < chunk ? count - c0 : chunk);
     cudaMemsetAsync(hist, 0, (size_t)S.nsamp * sizeof(uint32_t), st);
-    presort_count<R><<<sort_blocks, 256, 0, st>>>(S, seed, first + c0, n, keys, draws, hist);
+    presort_count<R><<<sort_blocks, 256, 0, st>>>(S, seed, first + c0, n, hist);
     presort_scan<<<1, 1024, 0, st>>>(hist, off, S.nsamp);
-    presort_scatter<<<sort_blocks, 256, 0, st>>>(keys, draws, n, off, sdraws, soff,
-                                                 S.nsamp);
+    presort_scatter<R><<<sort_blocks, 256, 0, st>>>(S, seed, first + c0, n, off, sdraws,
+                                                    soff);
     uint64_t nb = (n + block - 1) / block;
     if(nb > blocks) nb = blocks;
     /* Segment s of the launch is segment (s x mul) mod nseg of the sorted

@@ -1,8 +1,9 @@
-"""Coherent order: a plain launch of at least 2^24 realisations is presorted
-by sampled primitive and handed to warps in strided segments. It must trace
-exactly the realisations of the launch, each once with its own stream, so the
-estimates equal those of the same range launched in id order (launches below
-2^24), up to the rounding of the FP64 sums in another order."""
+"""Coherent order: a plain launch of at least 6e6 realisations is presorted
+by sampled primitive (in chunks of 2^24) and handed to warps in strided
+segments. It must trace exactly the realisations of the launch, each once with
+its own stream, so the estimates equal those of the same range launched in id
+order (launches below 6e6), up to the rounding of the FP64 sums in another
+order."""
 import ctypes as C
 
 import pytest
