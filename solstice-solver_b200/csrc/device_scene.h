@@ -98,7 +98,7 @@ struct DMedium {
 
 /* Per material constants; shader callbacks are tabulated per sun wavelength
  * node (`nodes` entries starting at `table`) */
-struct DMaterial {
+struct alignas(16) DMaterial {
   int32_t type;
   int32_t distrib;
   int32_t in_medium; /* index into media */
@@ -109,7 +109,7 @@ struct DMaterial {
 };
 
 /* Instance x shaded shape record: what a hit resolves to */
-struct DShadedInst {
+struct alignas(16) DShadedInst {
   int32_t instance; /* index of the instance in attach order */
   int32_t mtl[2]; /* [0] front, [1] back */
   int32_t receiver_mask; /* SSOL_FRONT | SSOL_BACK bits */
@@ -119,6 +119,7 @@ struct DShadedInst {
   int32_t is_punched;
   int32_t quadric; /* quadric patch index when punched */
   int32_t virtual_mask; /* bit0: front material virtual, bit1: back */
+  int32_t pad[3];
 };
 
 /* World-space triangle, stored as its three vertices (the watertight test

@@ -421,7 +421,7 @@ __device__ __forceinline__ bool side_passes
   (const DScene<R>& S, int sinst, int side, const SelfInfo& self)
 {
   if(self.reversed) side = side == 1 ? 2 : 1;
-  const DShadedInst& si = S.sinsts[sinst];
+  const DShadedInst si = ldg_record(S.sinsts + sinst);
   if(si.virtual_mask & (side == 1 ? 1 : 2)) {
     if(self.discard_virtual) return false;
     if(!(si.receiver_mask & side)) return false;
@@ -475,6 +475,50 @@ __device__ __forceinline__ R shear_row(V3<R> r, V3<R> a)
   return fma(r.z, a.z, fma(r.y, a.y, mul_rn(r.x, a.x)));
 }
 
+/* A 16-byte aligned record through the read-only data path, 16 bytes at a
+ * time */
+template<class T>
+__device__ __forceinline__ T ldg_record(const T* p)
+{
+  static_assert(sizeof(T) % 16 == 0 && alignof(T) >= 16, "16-byte records only");
+  union { T t; int4 w[sizeof(T) / 16]; } u;
+#pragma unroll
+  for(int i = 0; i < (int)(sizeof(T) / 16); ++i)
+    u.w[i] = __ldg(reinterpret_cast<const int4*>(p) + i);
+  return u.t;
+}
+
+/* A triangle through the read-only data path: three 16-byte loads in FP32 */
+__device__ __forceinline__ DTri<float> load_tri(const DTri<float>* p)
+{
+  const float4* q = reinterpret_cast<const float4*>(p);
+  const float4 a = __ldg(q), b = __ldg(q + 1);
+  const int4 c = __ldg(reinterpret_cast<const int4*>(q + 2));
+  DTri<float> t;
+  t.v0[0] = a.x; t.v0[1] = a.y; t.v0[2] = a.z;
+  t.v1[0] = a.w; t.v1[1] = b.x; t.v1[2] = b.y;
+  t.v2[0] = b.z; t.v2[1] = b.w; t.v2[2] = __int_as_float(c.x);
+  t.sinst = c.y; t.prim = c.z; t.gid = c.w;
+  return t;
+}
+__device__ __forceinline__ DTri<double> load_tri(const DTri<double>* p) { return *p; }
+
+/* A BVH node through the read-only data path: four 16-byte loads in FP32 */
+__device__ __forceinline__ DNode<float> load_node(const DNode<float>* p)
+{
+  const float4* q = reinterpret_cast<const float4*>(p);
+  const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+  const int4 d = __ldg(reinterpret_cast<const int4*>(q + 3));
+  DNode<float> n;
+  n.lo[0][0] = a.x; n.lo[0][1] = a.y; n.lo[0][2] = a.z;
+  n.lo[1][0] = a.w; n.lo[1][1] = b.x; n.lo[1][2] = b.y;
+  n.hi[0][0] = b.z; n.hi[0][1] = b.w; n.hi[0][2] = c.x;
+  n.hi[1][0] = c.y; n.hi[1][1] = c.z; n.hi[1][2] = c.w;
+  n.child[0] = d.x; n.child[1] = d.y; n.count[0] = d.z; n.count[1] = d.w;
+  return n;
+}
+__device__ __forceinline__ DNode<double> load_node(const DNode<double>* p) { return *p; }
+
 /* Mesh rule: reject t <= eps, t <= tmin and the starting triangle.
  * Inclusion by the watertight edge functions, so that no ray is lost between
  * two triangles; distance from the triangle's plane, dot(Ng, v0 - o) /
@@ -486,7 +530,7 @@ __device__ __forceinline__ void test_triangle
   (const DScene<R>& S, int idx, V3<R> o, V3<R> d, const Shear<R>& sh, R tmin,
    R eps, const SelfInfo& self, Hit<R>& best, bool& found)
 {
-  const DTri<R>& T = S.tris[idx];
+  const DTri<R> T = load_tri(S.tris + idx);
   const V3<R> p0 = ld3(T.v0), p1 = ld3(T.v1), p2 = ld3(T.v2);
   const V3<R> a = p0 - o, b = p1 - o, c = p2 - o;
   const R ax = shear_row(sh.rx, a), ay = shear_row(sh.ry, a);
@@ -628,7 +672,7 @@ __device__ bool trace_ray
   int sp = 0;
   int node = 0;
   for(;;) {
-    const DNode<R> N = S.nodes[node];
+    const DNode<R> N = load_node(S.nodes + node);
     ++cnt.nodes;
     R te[2];
     bool h[2];
