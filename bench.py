@@ -42,8 +42,8 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 # of the same scenes (field: one sorted chunk of 2^24 paths at 3 blocks per SM;
 # beam-down: 4e6 paths) (dram__bytes_read.sum + dram__bytes_write.sum);
 # the traffic scales with the paths traced (per-thread frames written back)
-DRAM_BYTES_PER_PATH = {"field": (2160.9e6 + 15301.9e6) / 16777216,
-                       "beamdown": (73.9e6 + 387.0e6) / 4e6}  # beam-down: id order
+DRAM_BYTES_PER_PATH = {"field": (2708.9e6 + 16358.4e6) / 16777216,
+                       "beamdown": (1104.4e6 + 3924.0e6) / 4e6}  # beam-down: id order
 
 # Kernels of one plain launch of n realisations: below 2^24 the realisation
 # kernel alone; from 2^24 on, per chunk of 2^24 realisations, the coherent
@@ -57,7 +57,7 @@ def launches_per_plain_launch(n):
 # Both passes of the adjoint kernel on the field, from a capture of 4e6 paths
 ADJOINT_DRAM_BYTES_PER_PATH = (2.76e6 + 26.97e6 + 5.95e6 + 52.99e6) / 4e6
 # Same for the batched kernel, from a capture of 32 suns (32245124 paths)
-BATCH_DRAM_BYTES_PER_PATH = (3918.3e6 + 18098.4e6) / 32245124
+BATCH_DRAM_BYTES_PER_PATH = (4571.5e6 + 19782.1e6) / 32245124
 
 
 def flops_per_run(st):
@@ -444,7 +444,7 @@ def run_b200(args):
                                        "realisation kernel, scaled to paths_per_step "
                                        "(bytes per step: its chunks' launches together)",
                      "timing": "CUDA events around each step: the realisation kernel and "
-                               "the coherent order's presort (2.5 % of the step)",
+                               "the coherent order's presort (2.3 % of the step)",
                      "peak_source": "SMs x 128 FP32 lanes x 2 x measured max SM clock "
                                     "(MEASURED_PEAKS.json sm_max_mhz)",
                      "work_model": "20/slab x2 per node + 55/triangle + 90/quadric + "
