@@ -415,6 +415,10 @@ def run_b200(args):
                 "same seed and realisation ids, every global and receiver estimate"}
         del e32, e64
 
+    bvh = None
+    if rank == 0 and not args.no_bvh_compare and args.config in ("field", "beamdown", "mirror"):
+        bvh = bvh_builders(lib, s, opt, n, stream, sp, flush if args.flush_mib else None)
+
     peaks = measured_peaks()
     nsm = torch.cuda.get_device_properties(local).multi_processor_count
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
@@ -455,6 +459,7 @@ def run_b200(args):
                      "kernel_ms": kernel_ms},
         "clocks": clk,
         "precision_vs_fp64": prec,
+        "bvh_builders": bvh,
         "estimate": {"absorbed_by_receivers_W": g["absorbed_by_receivers"][0],
                      "rel_se": g["absorbed_by_receivers"][2] / max(1e-30,
                                                                   g["absorbed_by_receivers"][0]),
@@ -515,6 +520,67 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def bvh_builders(lib, s, opt, n, stream, sp, flush):
+    """The two BVH builders on this scene, outside the timed region: plan
+    creation wall time (snapshot, tree, upload; median of 3), device
+    Mpaths/s of 2 launches of n paths after 1 warm-up (CUDA events, L2
+    flushed between launches), node visits per path and tree depth, and an
+    ssol_solve_ex of 1e6 paths end to end (median of 5), where the build is a
+    large part of the call."""
+    import torch
+    import pyssol as P
+    out = {}
+    for name, b in (("sah_host", P.BVH_SAH), ("lbvh_device", P.BVH_LBVH)):
+        o = P.options(opt.precision, block_size=opt.block_size, waves=opt.waves,
+                      leaf=opt.bvh_leaf_size, min_blocks=opt.min_blocks_per_sm, bvh=b)
+        create = []
+        for k in range(3):
+            plan = P.C.c_void_p()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            lib.call("ssol_b200_plan_create", s.scn, P.C.byref(o), P.C.byref(plan))
+            torch.cuda.synchronize()
+            create.append((time.perf_counter() - t0) * 1e3)
+            if k < 2:
+                lib.raw("ssol_b200_plan_ref_put", plan)
+        rng = s.rng(seed=123)
+        lib.call("ssol_b200_plan_launch", plan, rng, 0, n, sp)
+        lib.call("ssol_b200_plan_reset", plan, sp)
+        if flush is not None:
+            flush.zero_()
+        ms = 0.0
+        for k in range(2):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lib.call("ssol_b200_plan_launch", plan, rng, (1 + k) * n, n, sp)
+            e1.record(stream)
+            if flush is not None:
+                flush.zero_()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        est = P.C.c_void_p()
+        res = lib.raw("ssol_b200_plan_finish", plan, rng, 2 * n, 0, sp, P.C.byref(est))
+        e = P.Estimator(s, est, res)
+        st = e.stats()
+        del e
+        lib.raw("ssol_b200_plan_ref_put", plan)
+        solve = []
+        for k in range(5):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ek = s.solve(1_000_000, seed=k, options=o)
+            solve.append((time.perf_counter() - t0) * 1e3)
+            del ek
+        out[name] = {"plan_create_ms": sorted(create)[1],
+                     "mpaths_s": 2 * n / (ms * 1e-3) / 1e6,
+                     "node_visits_per_path": st["node_visits"] / max(1, st["paths"]),
+                     "depth": st["bvh_depth"], "nodes": st["bvh_nodes"],
+                     "built_on_device": bool(st["bvh_device"]),
+                     "ssol_solve_ex_1e6_ms": sorted(solve)[2]}
+    return out
+
+
 # The other workloads of the repo, measured by the default line too (each in
 # a child process of its own, as `bench.py --config X` would run it, with
 # 3 warm-up and 3 timed steps)
@@ -556,6 +622,8 @@ def other_configs():
                     "max_abs_rel_diff")
             if d.get("fd_check"):
                 r["fd_check"] = d["fd_check"]
+            if d.get("bvh_builders"):
+                r["bvh_builders"] = d["bvh_builders"]
             out[name] = r
         except Exception as exc:
             out[name] = {"failed": str(exc)}
@@ -1219,6 +1287,8 @@ def main():
     p.add_argument("--no-fp64-check", action="store_true",
                    help="skip the FP32 vs all-FP64 comparison of the field configs")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-bvh-compare", action="store_true",
+                   help="skip the host SAH against device LBVH builder comparison")
     p.add_argument("--no-suns", action="store_true",
                    help="field config: skip the 256-sun time-to-SE comparison (and the "
                         "other configs)")

@@ -26,6 +26,23 @@ enum ssol_b200_precision {
   SSOL_B200_FP64 = 1 /* everything in FP64 on identical random numbers */
 };
 
+/* Who builds the ray-tracing BVH of a plan's snapshot (the reference builds
+ * its Star-3D view on every solve, src/ssol_scene.c:347-433):
+ *  - SSOL_B200_BVH_SAH: binned-SAH tree on the host threads, uploaded with
+ *    the snapshot; leaves of bvh_leaf_size primitives;
+ *  - SSOL_B200_BVH_LBVH: linear BVH built on the device from the uploaded
+ *    primitive boxes (Morton codes, radix sort, Karras' hierarchy, bottom-up
+ *    boxes), one primitive per leaf (bvh_leaf_size is ignored). A tree deeper
+ *    than the traversal stack allows (more than 30 levels, only for
+ *    contrived layouts) is rebuilt on the host with the SAH builder, with a
+ *    warning. Both trees find the same closest hits; only the time to build
+ *    them and to traverse them differs. Batches and the renderers always use
+ *    the SAH builder. */
+enum ssol_b200_bvh_builder {
+  SSOL_B200_BVH_SAH = 0,
+  SSOL_B200_BVH_LBVH = 1
+};
+
 struct ssol_b200_options {
   enum ssol_b200_precision precision;
   int block_size; /* threads per block, <= 256; 0 => 256 */
@@ -35,8 +52,9 @@ struct ssol_b200_options {
   unsigned long long max_segments; /* path segment budget; 0 => 1e6 */
   int min_blocks_per_sm; /* register budget of the kernel variant: 1, 2, 3;
                           * 0 => 3 in FP32, 2 in FP64 */
+  enum ssol_b200_bvh_builder bvh_builder; /* plans and ssol_solve_ex */
 };
-#define SSOL_B200_OPTIONS_DEFAULT__ { SSOL_B200_FP32, 256, 0, 1, 0, 0, 0 }
+#define SSOL_B200_OPTIONS_DEFAULT__ { SSOL_B200_FP32, 256, 0, 1, 0, 0, 0, SSOL_B200_BVH_SAH }
 static const struct ssol_b200_options SSOL_B200_OPTIONS_DEFAULT =
   SSOL_B200_OPTIONS_DEFAULT__;
 
@@ -52,6 +70,9 @@ struct ssol_b200_stats {
   unsigned long long killed; /* paths ended by the Russian roulette */
   unsigned long long scene_bytes; /* host -> device bytes of the snapshot */
   unsigned long long tally_bytes; /* device -> host bytes of the tallies */
+  unsigned long long bvh_nodes; /* BVH nodes of the plan's snapshot */
+  unsigned long long bvh_depth; /* levels of internal nodes */
+  unsigned long long bvh_device; /* 1 if the BVH was built on the device */
 };
 
 /* ssol_solve with explicit options (NULL => defaults) */

@@ -392,6 +392,16 @@ template<class R> std::vector<DNode<R>> bvh_nodes(const BvhResult& b)
   return nodes;
 }
 
+template<class R> void round_box_outward(const PrimBox& b, R out[6])
+{
+  for(int c = 0; c < 3; ++c) {
+    out[c] = round_down<R>(b.lo[c]);
+    out[3 + c] = round_up<R>(b.hi[c]);
+  }
+}
+
+template void round_box_outward<float>(const PrimBox&, float*);
+template void round_box_outward<double>(const PrimBox&, double*);
 template std::vector<DNode<float>> bvh_nodes<float>(const BvhResult&);
 template std::vector<DNode<double>> bvh_nodes<double>(const BvhResult&);
 

@@ -23,6 +23,9 @@ struct BvhBuildParams {
   int bins = 16; /* SAH bins per axis */
   int max_depth = 30; /* the device traversal stack holds 32 entries */
   int threads = 1; /* host threads for the subtrees of large scenes */
+  /* Leave the tree to the device builder (lbvh.cu): the snapshot keeps the
+   * primitive boxes instead (scenes of at least 2 primitives) */
+  bool device = false;
 };
 
 struct BvhResult {
@@ -34,6 +37,9 @@ struct BvhResult {
 
 void build_bvh(std::vector<PrimBox> prims, const BvhBuildParams& params,
                BvhResult& out);
+
+/* A primitive's box in precision R, rounded outward: lo xyz, hi xyz */
+template<class R> void round_box_outward(const PrimBox& b, R out[6]);
 
 /* Convert to device nodes of precision R, rounding boxes outward */
 template<class R> std::vector<DNode<R>> bvh_nodes(const BvhResult& b);

@@ -966,6 +966,19 @@ static res_T flatten_impl
       out.meta.aabb_lo[c] = std::min(out.meta.aabb_lo[c], b.lo[c]);
       out.meta.aabb_hi[c] = std::max(out.meta.aabb_hi[c], b.hi[c]);
     }
+  if(bvh_params.device && boxes.size() >= 2) {
+    const size_t n = boxes.size();
+    out.device_bvh = true;
+    out.prim_box.resize(6 * n);
+    out.prim_ref.resize(n);
+    for(size_t i = 0; i < n; ++i) {
+      round_box_outward<R>(boxes[i], out.prim_box.data() + 6 * i);
+      out.prim_ref[i] = boxes[i].ref;
+    }
+    out.bvh = BvhResult();
+    out.nodes.assign(n - 1, DNode<R>());
+    return RES_OK;
+  }
   build_bvh(boxes, bvh_params, out.bvh);
   out.nodes = bvh_nodes<R>(out.bvh);
   return RES_OK;

@@ -58,6 +58,13 @@ template<class R> struct FlatScene {
   FlatMeta meta;
   BvhResult bvh;
   std::vector<DNode<R>> nodes;
+  /* Device-built BVH (BvhBuildParams::device): the primitives' boxes rounded
+   * outward (6 per primitive) and their references; `nodes` then holds the
+   * n - 1 zeroed nodes the device builder fills, and bvh.depth is unknown
+   * (0) until it has run */
+  bool device_bvh = false;
+  std::vector<R> prim_box;
+  std::vector<uint32_t> prim_ref;
   std::vector<DTri<R>> tris;
   std::vector<DQuadric<R>> quads;
   std::vector<DCarving> carvings;

@@ -134,6 +134,29 @@ struct TrackArgs {
 int launch_track_f32(const TrackArgs& A, void* stream);
 int launch_track_f64(const TrackArgs& A, void* stream);
 
+/* Device-built linear BVH (lbvh.cu) over n >= 2 primitive boxes (device
+ * array of 6 R per primitive: lo xyz, hi xyz, already rounded outward) and
+ * their references; writes the n - 1 nodes of DNode<R> (root 0, one
+ * primitive per leaf) and the tree depth (device int). The scratch pointers
+ * come from lbvh_bind_scratch over lbvh_scratch_bytes(n) bytes. */
+struct LbvhArgs {
+  int n;
+  const void* box;
+  const uint32_t* ref;
+  void* nodes;
+  void* cbounds;
+  int32_t* depth;
+  uint32_t* keys;
+  uint32_t* vals;
+  int32_t* parent;
+  uint32_t* flags;
+  int32_t* height;
+};
+size_t lbvh_scratch_bytes(int n);
+void lbvh_bind_scratch(LbvhArgs& A, void* scratch);
+int launch_lbvh_f32(const LbvhArgs& A, void* stream);
+int launch_lbvh_f64(const LbvhArgs& A, void* stream);
+
 /* Arguments of the adjoint passes (adjoint.cuh). Device pointers: inst_slot
  * (parameter slot per instance, -1 if none), axes (per slot: centre, e_x,
  * e_y), map (nx * ny cell sums of pass 0, read by pass 1), sums (sum w,

@@ -1,0 +1,340 @@
+/*
+ * lbvh.cu - device-built linear BVH over a snapshot's primitive boxes
+ * (Karras, "Maximizing Parallelism in the Construction of BVHs, Octrees,
+ * and k-d Trees", HPG 2012), emitted in the DNode layout the traversal reads.
+ *
+ * It replaces, on the device, the per-solve Star-3D view build of the
+ * reference (src/ssol_scene.c:347-433, s3d_scene_view_create at :410-413).
+ * Four steps on one stream, no host round trip between them:
+ *   1. centroid bounds of the primitive boxes (one block);
+ *   2. 30-bit Morton code of each centroid in those bounds (10 bits per axis);
+ *   3. stable LSD radix sort of (code, primitive) pairs, 4 passes of 8 bits,
+ *      in one block of 1024 threads: per 1024-element tile each warp ranks
+ *      its lanes by digit with __match_any_sync, the tile's digit offsets
+ *      come from a prefix over the warps, so equal codes keep their input
+ *      order and the tree is the same on every run;
+ *   4. one thread per internal node finds its key range and split from the
+ *      sorted codes (longest common prefix, with the sorted position breaking
+ *      ties between equal codes); internal node 0 is the root, so the layout
+ *      needs no renumbering; leaves are single primitives (count 1, the
+ *      child field holds the primitive reference itself);
+ *   5. one thread per leaf walks toward the root writing each child box into
+ *      its parent's slot; the second thread to reach a node (an atomic
+ *      arrival count) merges the node's two slots and goes on, the first
+ *      stops, so no thread waits on another. The same walk computes each
+ *      node's height; the root's is the tree depth, which the host reads back
+ *      to check the traversal stack bound.
+ */
+#include "kernels.h"
+
+#include <cuda_runtime.h>
+
+namespace ssolb {
+
+namespace {
+
+constexpr int SORT_THREADS = 1024;
+constexpr int SORT_WARPS = SORT_THREADS / 32;
+
+/* Spread the low 10 bits of v to every third bit */
+__device__ __forceinline__ uint32_t spread3(uint32_t v)
+{
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+template<class R>
+__device__ __forceinline__ R centroid(const R* box, int i, int c)
+{
+  return (R)0.5 * (box[6 * i + c] + box[6 * i + 3 + c]);
+}
+
+/* Step 1: bounds of the centroids, one block */
+template<class R>
+__global__ void __launch_bounds__(SORT_THREADS) lbvh_bounds(const R* box, int n, R* cb)
+{
+  __shared__ R red[6][SORT_WARPS];
+  R lo[3], hi[3];
+  for(int c = 0; c < 3; ++c) {
+    lo[c] = centroid(box, 0, c);
+    hi[c] = lo[c];
+  }
+  for(int i = threadIdx.x; i < n; i += blockDim.x)
+    for(int c = 0; c < 3; ++c) {
+      const R x = centroid(box, i, c);
+      lo[c] = fmin(lo[c], x);
+      hi[c] = fmax(hi[c], x);
+    }
+  for(int o = 16; o > 0; o >>= 1)
+    for(int c = 0; c < 3; ++c) {
+      lo[c] = fmin(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+      hi[c] = fmax(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+    }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if(lane == 0)
+    for(int c = 0; c < 3; ++c) {
+      red[c][w] = lo[c];
+      red[3 + c][w] = hi[c];
+    }
+  __syncthreads();
+  if(threadIdx.x < 6) {
+    const int q = threadIdx.x;
+    R v = red[q][0];
+    for(int k = 1; k < (int)(blockDim.x >> 5); ++k)
+      v = q < 3 ? fmin(v, red[q][k]) : fmax(v, red[q][k]);
+    cb[q] = v;
+  }
+}
+
+/* Step 2: Morton codes; vals are the primitives' input positions */
+template<class R>
+__global__ void lbvh_morton(const R* box, int n, const R* cb, uint32_t* keys, uint32_t* vals)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n) return;
+  uint32_t q[3];
+  for(int c = 0; c < 3; ++c) {
+    const R ext = cb[3 + c] - cb[c];
+    const R t = ext > (R)0 ? (centroid(box, i, c) - cb[c]) / ext : (R)0;
+    const R s = t * (R)1024;
+    q[c] = s <= (R)0 ? 0u : s >= (R)1023 ? 1023u : (uint32_t)s;
+  }
+  keys[i] = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+  vals[i] = (uint32_t)i;
+}
+
+/* Step 3: stable radix sort in one block; (k0, v0) in and out, (k1, v1)
+ * scratch */
+__global__ void __launch_bounds__(SORT_THREADS) lbvh_sort
+  (uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, int n)
+{
+  __shared__ uint32_t wcnt[SORT_WARPS][256];
+  __shared__ uint32_t base[256];
+  __shared__ uint32_t tile_total[256];
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  for(int pass = 0; pass < 4; ++pass) {
+    const int shift = 8 * pass;
+    const uint32_t* sk = pass & 1 ? k1 : k0;
+    const uint32_t* sv = pass & 1 ? v1 : v0;
+    uint32_t* dk = pass & 1 ? k0 : k1;
+    uint32_t* dv = pass & 1 ? v0 : v1;
+    if(tid < 256) tile_total[tid] = 0;
+    __syncthreads();
+    for(int i = tid; i < n; i += SORT_THREADS) atomicAdd(&tile_total[(sk[i] >> shift) & 255u], 1u);
+    __syncthreads();
+    if(tid < 32) {
+      /* exclusive scan of the 256 digit counts by one warp, 8 per lane */
+      uint32_t c[8], s = 0;
+      for(int k = 0; k < 8; ++k) { c[k] = tile_total[8 * lane + k]; s += c[k]; }
+      uint32_t inc = s;
+      for(int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if(lane >= o) inc += y;
+      }
+      uint32_t run = inc - s;
+      for(int k = 0; k < 8; ++k) { base[8 * lane + k] = run; run += c[k]; }
+    }
+    __syncthreads();
+    for(int t0 = 0; t0 < n; t0 += SORT_THREADS) {
+      const int i = t0 + tid;
+      const bool valid = i < n;
+      const uint32_t key = valid ? sk[i] : 0u, val = valid ? sv[i] : 0u;
+      const uint32_t d = (key >> shift) & 255u;
+      uint32_t* flat = &wcnt[0][0];
+      for(int k = tid; k < SORT_WARPS * 256; k += SORT_THREADS) flat[k] = 0;
+      __syncthreads();
+      /* invalid lanes group under 256, which no digit takes */
+      const unsigned peers = __match_any_sync(0xffffffffu, valid ? d : 256u);
+      const uint32_t rank = __popc(peers & lt);
+      if(valid && rank == 0) wcnt[w][d] = __popc(peers);
+      __syncthreads();
+      if(tid < 256) {
+        uint32_t s = 0;
+        for(int k = 0; k < SORT_WARPS; ++k) {
+          const uint32_t c = wcnt[k][tid];
+          wcnt[k][tid] = s;
+          s += c;
+        }
+        tile_total[tid] = s;
+      }
+      __syncthreads();
+      if(valid) {
+        const uint32_t pos = base[d] + wcnt[w][d] + rank;
+        dk[pos] = key;
+        dv[pos] = val;
+      }
+      __syncthreads();
+      if(tid < 256) base[tid] += tile_total[tid];
+      __syncthreads();
+    }
+  }
+}
+
+/* Longest common prefix of sorted keys i and j (-1 outside [0, n)); equal
+ * keys compare their positions, as if each key carried its position in its
+ * low 32 bits */
+__device__ __forceinline__ int lcp(const uint32_t* k, int n, int i, int j)
+{
+  if(j < 0 || j >= n) return -1;
+  const uint32_t a = k[i], b = k[j];
+  return a == b ? 32 + __clz(i ^ j) : __clz(a ^ b);
+}
+
+/* Step 4: internal node i of n - 1. parent[] holds (parent << 1) | slot:
+ * entries [0, n - 1) for internal nodes, [n - 1, 2n - 1) for leaves. */
+template<class R>
+__global__ void lbvh_nodes(const uint32_t* keys, const uint32_t* vals, const uint32_t* ref,
+                           int n, DNode<R>* nodes, int32_t* parent)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n - 1) return;
+  const int d = lcp(keys, n, i, i + 1) - lcp(keys, n, i, i - 1) > 0 ? 1 : -1;
+  const int dmin = lcp(keys, n, i, i - d);
+  int lmax = 2;
+  while(lcp(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for(int t = lmax >> 1; t >= 1; t >>= 1)
+    if(lcp(keys, n, i, i + (l + t) * d) > dmin) l += t;
+  const int j = i + l * d;
+  const int dnode = lcp(keys, n, i, j);
+  int s = 0;
+  for(int t = l;;) {
+    t = (t + 1) >> 1;
+    if(lcp(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    if(t == 1) break;
+  }
+  const int g = i + s * d + (d < 0 ? -1 : 0);
+  const int lo = min(i, j), hi = max(i, j);
+  DNode<R>& N = nodes[i];
+  const int c[2] = {g, g + 1};
+  const bool leaf[2] = {lo == g, hi == g + 1};
+  for(int k = 0; k < 2; ++k) {
+    if(leaf[k]) {
+      N.child[k] = (int32_t)ref[vals[c[k]]];
+      N.count[k] = 1;
+      parent[(n - 1) + c[k]] = (i << 1) | k;
+    } else {
+      N.child[k] = c[k];
+      N.count[k] = 0;
+      parent[c[k]] = (i << 1) | k;
+    }
+  }
+  if(i == 0) parent[0] = -1;
+}
+
+template<class R>
+__device__ __forceinline__ void put_slot(DNode<R>& N, int k, const R lo[3], const R hi[3])
+{
+  for(int c = 0; c < 3; ++c) {
+    N.lo[k][c] = lo[c];
+    N.hi[k][c] = hi[c];
+  }
+}
+
+/* Step 5: boxes and heights, one thread per leaf; flags start at zero */
+template<class R>
+__global__ void lbvh_boxes(const R* box, const uint32_t* vals, int n, DNode<R>* nodes,
+                           const int32_t* parent, uint32_t* flags, int32_t* height,
+                           int32_t* depth)
+{
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if(j >= n) return;
+  const int src = (int)vals[j];
+  R lo[3], hi[3];
+  for(int c = 0; c < 3; ++c) {
+    lo[c] = box[6 * src + c];
+    hi[c] = box[6 * src + 3 + c];
+  }
+  int p = parent[(n - 1) + j];
+  int node = p >> 1, slot = p & 1, h = 0;
+  put_slot(nodes[node], slot, lo, hi);
+  for(;;) {
+    /* publish this slot (and the height below it) before arriving */
+    __threadfence();
+    if(atomicAdd(&flags[node], 1u) == 0u) return;
+    __threadfence();
+    /* both slots are final: the sibling's box and height were written by
+     * the thread that arrived first, read past L1 */
+    DNode<R>& N = nodes[node];
+    const int o = 1 - slot;
+    for(int c = 0; c < 3; ++c) {
+      lo[c] = fmin(lo[c], __ldcg(&N.lo[o][c]));
+      hi[c] = fmax(hi[c], __ldcg(&N.hi[o][c]));
+    }
+    const int hs = N.count[o] == 0 ? __ldcg(&height[N.child[o]]) : 0;
+    h = 1 + max(h, hs);
+    height[node] = h;
+    if(node == 0) {
+      *depth = h;
+      return;
+    }
+    p = parent[node];
+    node = p >> 1;
+    slot = p & 1;
+    put_slot(nodes[node], slot, lo, hi);
+  }
+}
+
+template<class R>
+int launch_lbvh(const LbvhArgs& A, void* stream)
+{
+  const cudaStream_t s = (cudaStream_t)stream;
+  const int n = A.n;
+  if(n < 2) return (int)cudaErrorInvalidValue;
+  const R* box = (const R*)A.box;
+  R* cb = (R*)A.cbounds;
+  DNode<R>* nodes = (DNode<R>*)A.nodes;
+  uint32_t* k0 = A.keys;
+  uint32_t* k1 = A.keys + n;
+  uint32_t* v0 = A.vals;
+  uint32_t* v1 = A.vals + n;
+  if(cudaMemsetAsync(A.flags, 0, sizeof(uint32_t) * (size_t)(n - 1), s) != cudaSuccess)
+    return (int)cudaGetLastError();
+  lbvh_bounds<R><<<1, SORT_THREADS, 0, s>>>(box, n, cb);
+  const unsigned g = (unsigned)((n + 255) / 256);
+  lbvh_morton<R><<<g, 256, 0, s>>>(box, n, cb, k0, v0);
+  lbvh_sort<<<1, SORT_THREADS, 0, s>>>(k0, v0, k1, v1, n);
+  lbvh_nodes<R><<<g, 256, 0, s>>>(k0, v0, A.ref, n, nodes, A.parent);
+  lbvh_boxes<R><<<g, 256, 0, s>>>(box, v0, n, nodes, A.parent, A.flags, A.height, A.depth);
+  return (int)cudaGetLastError();
+}
+
+} /* namespace */
+
+size_t lbvh_scratch_bytes(int n)
+{
+  const size_t m = n > 0 ? (size_t)n : 0;
+  /* keys and vals (2n each), parent (2n), flags and heights (n each),
+   * centroid bounds (6 doubles), depth (one int, padded) */
+  return sizeof(uint32_t) * (2 * m + 2 * m + 2 * m + m + m) + 6 * sizeof(double) + 16;
+}
+
+void lbvh_bind_scratch(LbvhArgs& A, void* scratch)
+{
+  const size_t m = A.n > 0 ? (size_t)A.n : 0;
+  /* the doubles first, so that they are 8-byte aligned */
+  unsigned char* p = (unsigned char*)scratch;
+  A.cbounds = p;
+  p += 6 * sizeof(double);
+  A.depth = (int32_t*)p;
+  p += 16;
+  A.keys = (uint32_t*)p;
+  p += sizeof(uint32_t) * 2 * m;
+  A.vals = (uint32_t*)p;
+  p += sizeof(uint32_t) * 2 * m;
+  A.parent = (int32_t*)p;
+  p += sizeof(int32_t) * 2 * m;
+  A.flags = (uint32_t*)p;
+  p += sizeof(uint32_t) * m;
+  A.height = (int32_t*)p;
+}
+
+int launch_lbvh_f32(const LbvhArgs& A, void* stream) { return launch_lbvh<float>(A, stream); }
+int launch_lbvh_f64(const LbvhArgs& A, void* stream) { return launch_lbvh<double>(A, stream); }
+
+} /* namespace ssolb */

@@ -205,6 +205,7 @@ struct ssol_estimator {
   unsigned long long stats[6] = {};
   unsigned long long killed = 0;
   unsigned long long scene_bytes = 0, tally_bytes = 0;
+  unsigned long long bvh_nodes = 0, bvh_depth = 0, bvh_device = 0;
 };
 
 /* Shared helpers (objects.cpp) */

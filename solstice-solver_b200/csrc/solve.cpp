@@ -241,6 +241,9 @@ struct ssol_b200_plan {
   void* d_tally = nullptr;
   size_t scene_bytes = 0;
   size_t scene_alloc = 0;
+  int bvh_depth = 0; /* levels of internal nodes of the BVH */
+  bool bvh_device = false; /* built on the device */
+  unsigned long long bvh_nodes = 0;
   TallyLayout tl{};
   DScene<float> s32{};
   DScene<double> s64{};
@@ -448,9 +451,22 @@ static bool validate(const FlatScene<R>& f, bool need_samp = true)
   const int64_t nnodes = (int64_t)f.nodes.size();
   const int64_t nrefs = (int64_t)f.bvh.primrefs.size();
   if(nnodes < 1) return false;
+  /* A device-built tree's nodes are written on the device from the
+   * primitive references checked here, its depth is checked once built */
+  if(f.device_bvh) {
+    if(f.prim_ref.size() < 2 || (size_t)nnodes != f.prim_ref.size() - 1
+    || f.prim_box.size() != 6 * f.prim_ref.size() || f.prim_ref.size() > (1u << 28))
+      return false;
+    for(uint32_t ref : f.prim_ref) {
+      const uint32_t i = primref_index(ref);
+      if(primref_kind(ref) == PRIM_TRIANGLE ? i >= f.tris.size() : i >= f.quads.size())
+        return false;
+    }
+  }
   /* the traversal defers at most depth - 1 nodes on its 32-entry stack */
-  if(f.bvh.depth > 30) return false;
+  if(!f.device_bvh && f.bvh.depth > 30) return false;
   for(const DNode<R>& n : f.nodes) {
+    if(f.device_bvh) break;
     for(int k = 0; k < 2; ++k) {
       if(n.count[k] == 0) {
         if(n.child[k] <= 0 || n.child[k] >= nnodes) return false;
@@ -555,20 +571,49 @@ static void add_scene(Blob& b, const FlatScene<R>& f)
   b.add(f.bake_tab);
 }
 
+static int launch_lbvh_r(const LbvhArgs& A, void* s, float) { return launch_lbvh_f32(A, s); }
+static int launch_lbvh_r(const LbvhArgs& A, void* s, double) { return launch_lbvh_f64(A, s); }
+
+/* Snapshot upload; a device-built BVH is built here, after the copy, on the
+ * device's stream, and its depth read back. RES_BAD_OP: the tree is deeper
+ * than the traversal stack allows (the caller rebuilds on the host). */
 template<class R>
 static res_T upload(ssol_b200_plan* p, const FlatScene<R>& f, DScene<R>& S)
 {
   Blob b;
   add_scene(b, f);
-  const size_t bytes = b.host.size() + 256;
+  size_t o_box = 0, o_ref = 0, o_scratch = 0, bytes = b.host.size() + 256;
+  const int nprims = (int)f.prim_ref.size();
+  if(f.device_bvh) {
+    o_box = b.add(f.prim_box);
+    o_ref = b.add(f.prim_ref);
+    o_scratch = (b.host.size() + 255) & ~size_t(255);
+    bytes = o_scratch + lbvh_scratch_bytes(nprims) + 256;
+  }
+  const cudaStream_t st = (cudaStream_t)p->dev->stream;
   if(dev_alloc(p->dev, &p->d_scene, bytes) != cudaSuccess) return RES_MEM_ERR;
   p->scene_alloc = bytes;
   if(cudaMemcpyAsync(p->d_scene, b.host.data(), b.host.size(),
-                     cudaMemcpyHostToDevice,
-                     (cudaStream_t)p->dev->stream) != cudaSuccess)
+                     cudaMemcpyHostToDevice, st) != cudaSuccess)
     return RES_UNKNOWN_ERR;
   p->scene_bytes = b.host.size();
   bind_scene(S, f, b, (unsigned char*)p->d_scene);
+  if(f.device_bvh) {
+    unsigned char* base = (unsigned char*)p->d_scene;
+    LbvhArgs A = {};
+    A.n = nprims;
+    A.box = base + o_box;
+    A.ref = (const uint32_t*)(base + o_ref);
+    A.nodes = base + b.offsets[0];
+    lbvh_bind_scratch(A, base + o_scratch);
+    if(launch_lbvh_r(A, st, R()) != 0) return RES_UNKNOWN_ERR;
+    int32_t depth = 0;
+    if(cudaMemcpyAsync(&depth, A.depth, sizeof(depth), cudaMemcpyDeviceToHost, st)
+       != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+      return RES_UNKNOWN_ERR;
+    p->bvh_depth = depth;
+    if(depth < 1 || depth > 30) return RES_BAD_OP;
+  }
   return RES_OK;
 }
 
@@ -684,10 +729,14 @@ extern "C" res_T ssol_b200_plan_create
   if(opt.max_segments == 0) opt.max_segments = 1000000ull;
   if(opt.min_blocks_per_sm < 0 || opt.min_blocks_per_sm > 3) return RES_BAD_ARG;
   if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = default_min_blocks(opt.precision);
+  if(opt.bvh_builder != SSOL_B200_BVH_SAH && opt.bvh_builder != SSOL_B200_BVH_LBVH)
+    return RES_BAD_ARG;
+  if(opt.bvh_builder == SSOL_B200_BVH_LBVH) opt.bvh_leaf_size = 1;
 
   BvhBuildParams bp;
   bp.max_leaf = opt.bvh_leaf_size;
   bp.threads = host_threads();
+  bp.device = opt.bvh_builder == SSOL_B200_BVH_LBVH;
 
   /* Snapshot on the host first: argument errors need no GPU */
   std::unique_ptr<FlatScene<float>> f32;
@@ -716,12 +765,23 @@ extern "C" res_T ssol_b200_plan_create
   ssol_scene_ref_get(scn);
   p->scn = scn;
   p->opt = opt;
+  p->bvh_device = f32 ? f32->device_bvh : f64->device_bvh;
+  p->bvh_depth = f32 ? f32->bvh.depth : f64->bvh.depth;
+  p->bvh_nodes = f32 ? f32->nodes.size() : f64->nodes.size();
   if(f32) {
     p->meta = f32->meta;
     res = upload(p, *f32, p->s32);
   } else {
     p->meta = f64->meta;
     res = upload(p, *f64, p->s64);
+  }
+  if(res == RES_BAD_OP) {
+    /* A device-built tree too deep for the traversal stack: the host SAH
+     * builder bounds its depth */
+    plan_release(p);
+    scn->dev->log_warning("device BVH deeper than 30 levels; built on the host instead.\n");
+    opt.bvh_builder = SSOL_B200_BVH_SAH;
+    return ssol_b200_plan_create(scn, &opt, out);
   }
   if(res != RES_OK) { plan_release(p); return res; }
   p->nrcv = (int)p->meta.rcv.size();
@@ -880,6 +940,11 @@ extern "C" res_T ssol_b200_plan_finish
   const uint64_t ran = std::min<uint64_t>(nreal, st->paths);
   res_T res = make_estimator(p->dev, p->scn, p->meta, p->tl, h.data(), ran, rng,
                              nreal, st, p->kernel_ms, p->scene_bytes, max_failed, out);
+  if(*out) {
+    (*out)->bvh_nodes = p->bvh_nodes;
+    (*out)->bvh_depth = (unsigned long long)p->bvh_depth;
+    (*out)->bvh_device = p->bvh_device ? 1ull : 0ull;
+  }
   const unsigned long long* cnt = (const unsigned long long*)(h.data() + p->tl.counters);
   if(res == RES_OK && cnt[5]) {
     p->dev->log_error("the solve was aborted: %llu of %llu realisations ran.\n",
@@ -902,6 +967,8 @@ extern "C" res_T ssol_b200_autotune
   ssol_b200_options best_opt = base;
   double best = DBL_MAX;
   for(const int leaf : leaves) {
+    /* a device-built tree has one primitive per leaf */
+    if(base.bvh_builder == SSOL_B200_BVH_LBVH && leaf != 1) continue;
     ssol_b200_options o = base;
     o.bvh_leaf_size = leaf;
     o.grid_blocks = 0;
@@ -1115,6 +1182,9 @@ extern "C" res_T ssol_b200_plan_get_stats
   s->kernel_ms = p->kernel_ms;
   s->scene_bytes = p->scene_bytes;
   s->tally_bytes = p->tl.total;
+  s->bvh_nodes = p->bvh_nodes;
+  s->bvh_depth = (unsigned long long)p->bvh_depth;
+  s->bvh_device = p->bvh_device ? 1ull : 0ull;
   return RES_OK;
 }
 
@@ -2134,5 +2204,8 @@ extern "C" res_T ssol_estimator_get_b200_stats
   s->killed = e->killed;
   s->scene_bytes = e->scene_bytes;
   s->tally_bytes = e->tally_bytes;
+  s->bvh_nodes = e->bvh_nodes;
+  s->bvh_depth = e->bvh_depth;
+  s->bvh_device = e->bvh_device;
   return RES_OK;
 }

@@ -155,7 +155,11 @@ class PunchedSurface(C.Structure):
 class B200Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("block_size", C.c_int), ("grid_blocks", C.c_int),
                 ("waves", C.c_int), ("bvh_leaf_size", C.c_int),
-                ("max_segments", C.c_ulonglong), ("min_blocks_per_sm", C.c_int)]
+                ("max_segments", C.c_ulonglong), ("min_blocks_per_sm", C.c_int),
+                ("bvh_builder", C.c_int)]
+
+
+BVH_SAH, BVH_LBVH = 0, 1
 
 
 class SunPosition(C.Structure):
@@ -165,7 +169,7 @@ class SunPosition(C.Structure):
 class B200Stats(C.Structure):
     _fields_ = [("kernel_ms", C.c_double)] + [(n, C.c_ulonglong) for n in (
         "rays", "node_visits", "triangle_tests", "quadric_tests", "bounces", "paths",
-        "killed", "scene_bytes", "tally_bytes")]
+        "killed", "scene_bytes", "tally_bytes", "bvh_nodes", "bvh_depth", "bvh_device")]
 
 
 class ImageLayout(C.Structure):
@@ -929,7 +933,7 @@ def estimator_from_tallies(scene, rng, n, sums, counts, max_failed=0):
 
 
 def options(precision=FP32, block_size=256, grid_blocks=0, waves=1, leaf=0,
-            max_segments=0, min_blocks=0):
+            max_segments=0, min_blocks=0, bvh=BVH_SAH):
     o = B200Options()
     o.precision = precision
     o.block_size = block_size
@@ -938,6 +942,7 @@ def options(precision=FP32, block_size=256, grid_blocks=0, waves=1, leaf=0,
     o.bvh_leaf_size = leaf
     o.max_segments = max_segments
     o.min_blocks_per_sm = min_blocks
+    o.bvh_builder = bvh
     return o
 
 

@@ -90,6 +90,16 @@ def test_solve_argument_checks(lib):
     s.close()
 
 
+def test_plan_option_checks(product):
+    """Options are checked before any snapshot or GPU work: an unknown BVH
+    builder, a negative leaf size and an unknown precision are RES_BAD_ARG."""
+    s = P.Scene(product)
+    plan = C.c_void_p()
+    for o in (P.options(bvh=7), P.options(bvh=-1), P.options(leaf=-1), P.options(precision=5)):
+        assert product.raw("ssol_b200_plan_create", s.scn, C.byref(o), C.byref(plan)) == P.RES_BAD_ARG
+    s.close()
+
+
 def test_areas_and_tessellation(lib):
     """Areas of meshes and punched surfaces (src/test_ssol_solver3.c:138-163:
     a 20x20 punched plane has area 400)."""

@@ -1,0 +1,114 @@
+"""The device-built linear BVH (ssol_b200_options.bvh_builder = LBVH) against
+the host binned-SAH tree.
+
+Both trees hold the same primitive boxes and the traversal reports the
+closest accepted hit whatever the tree, so a solve traces the same paths with
+either: on the same seed every estimate agrees to the order of the FP64
+reductions (1e-10 relative). This is the device replacement of the
+reference's per-solve Star-3D view build (src/ssol_scene.c:347-433), checked
+through the estimates the reference's own tests read. A layout whose linear
+BVH is deeper than the traversal stack allows is rebuilt on the host (the
+stats say which builder ran)."""
+import pytest
+
+import pyssol as P
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(a, b, what, rel=1e-10):
+    for k in b:
+        assert a[k][0] == pytest.approx(b[k][0], rel=rel, abs=1e-9), (what, k)
+        assert a[k][2] == pytest.approx(b[k][2], rel=1e-6, abs=1e-9), (what, k)
+
+
+def _solve_pair(s, n, seed, precision=P.FP32):
+    sah = s.solve(n, seed=seed, options=P.options(precision=precision, bvh=P.BVH_SAH))
+    lbvh = s.solve(n, seed=seed, options=P.options(precision=precision, bvh=P.BVH_LBVH))
+    return sah, lbvh
+
+
+def test_lbvh_full_field_equals_sah(product):
+    """1000-heliostat field with its 64x64 receiver map (10,192 triangles),
+    4e6 paths: globals, receiver and all 8192 per-primitive estimates."""
+    s, h = W.heliostat_field(product)
+    sah, lbvh = _solve_pair(s, 4_000_000, seed=5)
+    st, sl = sah.stats(), lbvh.stats()
+    assert st["bvh_device"] == 0 and sl["bvh_device"] == 1
+    assert sl["bvh_nodes"] == 2 * 1000 + 2 * 64 * 64 - 1
+    assert 1 <= sl["bvh_depth"] <= 30
+    assert sl["rays"] == st["rays"] and sl["bounces"] == st["bounces"]
+    assert sl["triangle_tests"] > 0 and sl["node_visits"] > 0
+    _same(lbvh.globals(), sah.globals(), "globals")
+    _same(lbvh.receiver(h["receiver"]), sah.receiver(h["receiver"]), "receiver")
+    pl = lbvh.primitives(h["receiver"], h["receiver_shape"])
+    ps = sah.primitives(h["receiver"], h["receiver_shape"])
+    assert len(pl) == len(ps) == 2 * 64 * 64
+    for i, (a, b) in enumerate(zip(pl, ps)):
+        _same(a, b, ("primitive", i))
+    s.close()
+
+
+def test_lbvh_beam_down_equals_sah(product):
+    """Beam-down scene: 5000 punched paraboloids, a hyperboloid, the glass
+    window and the receiver grid (quadric patches in the device build), 1e6
+    paths with the roulette."""
+    s, h = W.beam_down(product)
+    sah, lbvh = _solve_pair(s, 1_000_000, seed=9)
+    assert lbvh.stats()["bvh_device"] == 1
+    assert lbvh.stats()["killed"] == sah.stats()["killed"]
+    _same(lbvh.globals(), sah.globals(), "globals")
+    _same(lbvh.receiver(h["receiver"]), sah.receiver(h["receiver"]), "receiver")
+    s.close()
+
+
+def test_lbvh_fp64_and_single_mirror(product):
+    """The FP64 build of a reduced field, and the single-mirror scene (four
+    triangles), with either builder."""
+    s, h = W.heliostat_field(product, n_helio=200, receiver_cells=16)
+    sah, lbvh = _solve_pair(s, 1_000_000, seed=3, precision=P.FP64)
+    assert lbvh.stats()["bvh_device"] == 1
+    _same(lbvh.globals(), sah.globals(), "fp64 globals")
+    _same(lbvh.receiver(h["receiver"]), sah.receiver(h["receiver"]), "fp64 receiver")
+    s.close()
+    s, h = W.single_mirror(product)
+    sah, lbvh = _solve_pair(s, 1_000_000, seed=0)
+    assert lbvh.stats()["bvh_nodes"] == 3
+    _same(lbvh.globals(), sah.globals(), "mirror globals")
+    _same(lbvh.receiver(h["receiver"]), sah.receiver(h["receiver"]), "mirror receiver")
+    s.close()
+
+
+def _deep_layout(lib):
+    """36 small horizontal matte triangles whose Morton codes are 0 (five of
+    them), each single bit of the 30 (one triangle per axis and bit) and all
+    ones: the linear BVH peels one triangle off per level, 33 levels deep."""
+    s = P.Scene(lib)
+    centres = [(0.1 * k, 0.0, 0.0) for k in range(5)]
+    for lvl in range(10):
+        v = 2.0 ** lvl + 0.5
+        centres += [(v, 0.0, 0.0), (0.0, v, 0.0), (0.0, 0.0, v)]
+    centres.append((1024.0, 1024.0, 1024.0))
+    a = 0.04
+    verts, ids = [], []
+    for (x, y, z) in centres:
+        b = len(verts)
+        verts += [(x - a, y - a, z), (x + a, y - a, z), (x, y + a, z)]
+        ids.append((b, b + 1, b + 2))
+    mesh = s.mesh(verts, ids)
+    m = s.matte(0.5)
+    inst = s.instance(s.object([(mesh, m, m)]), receiver=P.SSOL_FRONT | P.SSOL_BACK)
+    s.set_sun("directional", (0.1, 0.2, -1.0), 1000.0)
+    return s, inst
+
+
+def test_lbvh_too_deep_falls_back_to_sah(product):
+    s, inst = _deep_layout(product)
+    sah, lbvh = _solve_pair(s, 200_000, seed=1)
+    st, sl = sah.stats(), lbvh.stats()
+    assert sl["bvh_device"] == 0
+    assert sl["bvh_depth"] == st["bvh_depth"] <= 30
+    _same(lbvh.globals(), sah.globals(), "globals")
+    _same(lbvh.receiver(inst, P.SSOL_FRONT), sah.receiver(inst, P.SSOL_FRONT), "front")
+    s.close()
