@@ -497,6 +497,8 @@ def run_b200(args):
             "speedup_vs_ssol_solve_loop": r["speedup_batched_vs_ssol_solve_loop"],
             "from_scratch_s": r["time_to_0.1pct_se_from_scratch_s"],
             "speedup_from_scratch_vs_plan_loop": r["speedup_from_scratch_vs_plain_plan_loop"],
+            "speedup_from_scratch_vs_plan_loop_device_bvh":
+                r["speedup_from_scratch_vs_plain_plan_loop_device_bvh"],
             "speedup_from_scratch_vs_ssol_solve_loop":
                 r["speedup_from_scratch_vs_ssol_solve_loop"],
             "suns_reaching_0.1pct_se": r["reached"],
@@ -795,23 +797,31 @@ def suns_comparison(args, lib, opt, stream, sp, flush, dist, local, rank, world,
     scratch_batched = time.perf_counter() - t0
     del es
     bt.close()
-    t0 = time.perf_counter()
-    for sc, b in zip(scenes, budgets):
-        pl = P.C.c_void_p()
-        lib.call("ssol_b200_plan_create", sc.scn, P.C.byref(opt), P.C.byref(pl))
-        lib.call("ssol_b200_plan_launch", pl, rng, 0, b, sp)
-        est = P.C.c_void_p()
-        lib.raw("ssol_b200_plan_finish", pl, rng, b, 0, sp, P.C.byref(est))
-        e = P.Estimator(sc, est, 0)
-        tot = needed(e, b)
-        del e
-        if tot > b:
-            lib.call("ssol_b200_plan_launch", pl, rng, b, tot - b, sp)
+    def plain_from_scratch(o):
+        t0 = time.perf_counter()
+        for sc, b in zip(scenes, budgets):
+            pl = P.C.c_void_p()
+            lib.call("ssol_b200_plan_create", sc.scn, P.C.byref(o), P.C.byref(pl))
+            lib.call("ssol_b200_plan_launch", pl, rng, 0, b, sp)
             est = P.C.c_void_p()
-            lib.raw("ssol_b200_plan_finish", pl, rng, tot, 0, sp, P.C.byref(est))
-            lib.raw("ssol_estimator_ref_put", est)
-        lib.raw("ssol_b200_plan_ref_put", pl)
-    scratch_plain = time.perf_counter() - t0
+            lib.raw("ssol_b200_plan_finish", pl, rng, b, 0, sp, P.C.byref(est))
+            e = P.Estimator(sc, est, 0)
+            tot = needed(e, b)
+            del e
+            if tot > b:
+                lib.call("ssol_b200_plan_launch", pl, rng, b, tot - b, sp)
+                est = P.C.c_void_p()
+                lib.raw("ssol_b200_plan_finish", pl, rng, tot, 0, sp, P.C.byref(est))
+                lib.raw("ssol_estimator_ref_put", est)
+            lib.raw("ssol_b200_plan_ref_put", pl)
+        return time.perf_counter() - t0
+
+    scratch_plain = plain_from_scratch(opt)
+    # the same loop with each sun's tree built on the device
+    opt_lbvh = P.options(opt.precision, block_size=opt.block_size, waves=opt.waves,
+                         leaf=opt.bvh_leaf_size, min_blocks=opt.min_blocks_per_sm,
+                         bvh=P.BVH_LBVH)
+    scratch_plain_lbvh = plain_from_scratch(opt_lbvh)
     t0 = time.perf_counter()
     for sc, b in zip(scenes, budgets):
         r1 = sc.rng(seed=args.seed + 5)
@@ -844,12 +854,15 @@ def suns_comparison(args, lib, opt, stream, sp, flush, dist, local, rank, world,
                                 "batch_api_end_to_end": e2e_s},
         "time_to_0.1pct_se_from_scratch_s": {
             "batched": scratch_batched, "plain_plan_loop_per_sun": scratch_plain,
+            "plain_plan_loop_per_sun_device_bvh": scratch_plain_lbvh,
             "ssol_solve_loop_per_sun": scratch_solve,
             "what": "pilot of 1e5 per sun + read-back + the rest, per approach, "
                     "scene snapshots included (batched: one snapshot, re-aimed per "
                     "sun on the device; the loops: one snapshot per sun); the "
                     "per-sun loops synchronise once per pilot"},
         "speedup_from_scratch_vs_plain_plan_loop": scratch_plain / scratch_batched,
+        "speedup_from_scratch_vs_plain_plan_loop_device_bvh":
+            scratch_plain_lbvh / scratch_batched,
         "speedup_from_scratch_vs_ssol_solve_loop": scratch_solve / scratch_batched,
         "speedup_batched_vs_plain_plan_loop": per_step_p / per_step_b,
         "speedup_batched_vs_ssol_solve_loop": solve_loop_s / (per_step_b * 1e-3),
@@ -920,6 +933,7 @@ def run_suns(args):
     }
     for k in ("time_to_0.1pct_se_s", "time_to_0.1pct_se_from_scratch_s",
               "speedup_from_scratch_vs_plain_plan_loop",
+              "speedup_from_scratch_vs_plain_plan_loop_device_bvh",
               "speedup_from_scratch_vs_ssol_solve_loop",
               "speedup_batched_vs_plain_plan_loop", "speedup_batched_vs_ssol_solve_loop"):
         line[k] = r[k]

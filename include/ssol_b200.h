@@ -4,7 +4,8 @@
  * None of these entry points has a counterpart in the reference; they expose
  * what a GPU solver adds around `ssol_solve` (src/ssol.h:1216-1223):
  *  - solve options: arithmetic precision of geometry/sampling/BSDFs (FP32 or
- *    all-FP64; tallies are FP64 in both), launch shape, BVH leaf size;
+ *    all-FP64; tallies are FP64 in both), launch shape, BVH leaf size, and
+ *    whether the BVH is built on the host or the device;
  *  - plans: a scene snapshot resident in device memory that can be launched
  *    many times on a caller's CUDA stream and read back once, which is how
  *    `ssol_solve` itself is built (create, reset, launch, finish);
