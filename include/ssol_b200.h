@@ -33,12 +33,12 @@ enum ssol_b200_precision {
  *    the snapshot; leaves of bvh_leaf_size primitives;
  *  - SSOL_B200_BVH_LBVH: linear BVH built on the device from the uploaded
  *    primitive boxes (Morton codes, radix sort, Karras' hierarchy, bottom-up
- *    boxes), one primitive per leaf (bvh_leaf_size is ignored). A tree deeper
- *    than the traversal stack allows (more than 30 levels, only for
- *    contrived layouts) is rebuilt on the host with the SAH builder, with a
- *    warning. Both trees find the same closest hits; only the time to build
- *    them and to traverse them differs. Batches and the renderers always use
- *    the SAH builder. */
+ *    boxes, treelet restructuring for a lower SAH cost, depth-first node
+ *    order), one primitive per leaf (bvh_leaf_size is ignored). A tree
+ *    deeper than the traversal stack allows (more than 30 levels) is rebuilt
+ *    on the host with the SAH builder, with a warning. Both trees find the
+ *    same closest hits; only the time to build them and to traverse them
+ *    differs. Batches and the renderers always use the SAH builder. */
 enum ssol_b200_bvh_builder {
   SSOL_B200_BVH_SAH = 0,
   SSOL_B200_BVH_LBVH = 1

@@ -151,6 +151,11 @@ struct LbvhArgs {
   int32_t* parent;
   uint32_t* flags;
   int32_t* height;
+  float* cost;
+  int32_t* ninner;
+  int32_t* newidx;
+  void* tmp_nodes;
+  int optimize; /* treelet restructuring of every node's subtree */
 };
 size_t lbvh_scratch_bytes(int n);
 void lbvh_bind_scratch(LbvhArgs& A, void* scratch);

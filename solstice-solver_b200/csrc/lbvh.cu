@@ -5,7 +5,7 @@
  *
  * It replaces, on the device, the per-solve Star-3D view build of the
  * reference (src/ssol_scene.c:347-433, s3d_scene_view_create at :410-413).
- * Four steps on one stream, no host round trip between them:
+ * Six steps on one stream, no host round trip between them:
  *   1. centroid bounds of the primitive boxes (one block);
  *   2. 30-bit Morton code of each centroid in those bounds (10 bits per axis);
  *   3. stable LSD radix sort of (code, primitive) pairs, 4 passes of 8 bits,
@@ -15,23 +15,33 @@
  *      order and the tree is the same on every run;
  *   4. one thread per internal node finds its key range and split from the
  *      sorted codes (longest common prefix, with the sorted position breaking
- *      ties between equal codes); internal node 0 is the root, so the layout
- *      needs no renumbering; leaves are single primitives (count 1, the
- *      child field holds the primitive reference itself);
+ *      ties between equal codes); internal node 0 is the root; leaves are
+ *      single primitives (count 1, the child field holds the primitive
+ *      reference itself);
  *   5. one thread per leaf walks toward the root writing each child box into
  *      its parent's slot; the second thread to reach a node (an atomic
  *      arrival count) merges the node's two slots and goes on, the first
  *      stops, so no thread waits on another. The same walk computes each
- *      node's height; the root's is the tree depth, which the host reads back
- *      to check the traversal stack bound.
+ *      node's SAH cost, height and internal-node count, and restructures the
+ *      node's treelet for a lower SAH cost (Karras and Aila, HPG 2013) once
+ *      its subtree is final; the root's height is the tree depth, which the
+ *      host reads back to check the traversal stack bound;
+ *   6. the internal nodes are renumbered depth first, slot 0 first, so that
+ *      a node's first child follows it in memory.
  */
 #include "kernels.h"
 
 #include <cuda_runtime.h>
 
+#include <cfloat>
+
 namespace ssolb {
 
 namespace {
+
+template<class R> __device__ __forceinline__ R rmax();
+template<> __device__ __forceinline__ float rmax<float>() { return FLT_MAX; }
+template<> __device__ __forceinline__ double rmax<double>() { return DBL_MAX; }
 
 constexpr int SORT_THREADS = 1024;
 constexpr int SORT_WARPS = SORT_THREADS / 32;
@@ -236,11 +246,190 @@ __device__ __forceinline__ void put_slot(DNode<R>& N, int k, const R lo[3], cons
   }
 }
 
-/* Step 5: boxes and heights, one thread per leaf; flags start at zero */
+/* Surface-area heuristic: a node costs C_NODE x its surface area (a ray
+ * that reaches it tests both child boxes), a primitive C_PRIM x its box's
+ * (Karras and Aila's constants; areas are half surface areas, the factor
+ * cancels) */
+constexpr float C_NODE = 1.2f, C_PRIM = 1.0f;
+constexpr int TREELET = 6; /* leaves of a restructured treelet (7 gave a 0.2 % lower SAH
+                              * cost on the field for 3x the work) */
+
+template<class R>
+__device__ __forceinline__ float half_area(const R lo[3], const R hi[3])
+{
+  const float dx = (float)(hi[0] - lo[0]), dy = (float)(hi[1] - lo[1]),
+              dz = (float)(hi[2] - lo[2]);
+  return dx * dy + dy * dz + dz * dx;
+}
+
+/* Per internal node: SAH cost, height, internal nodes in its subtree
+ * (itself included) and parent link ((parent << 1) | slot; entries
+ * [n - 1, 2n - 1) are the leaves') */
+struct Aux {
+  float* cost;
+  int32_t* height;
+  int32_t* ninner;
+  int32_t* parent;
+};
+
+/* A treelet leaf: a slot's box, what it holds (a primitive, count 1, or a
+ * subtree, count 0), and the subtree's cost, height and internal nodes */
+template<class R> struct TLeaf {
+  R lo[3], hi[3];
+  int32_t child, count;
+  float cost;
+  int height, ninner;
+};
+
+/* Slot k of node N as written by other threads of this launch: read past L1 */
+template<class R>
+__device__ __forceinline__ void read_slot(const DNode<R>& N, int k, const Aux& A, TLeaf<R>& L)
+{
+  for(int c = 0; c < 3; ++c) {
+    L.lo[c] = __ldcg(&N.lo[k][c]);
+    L.hi[c] = __ldcg(&N.hi[k][c]);
+  }
+  L.child = __ldcg(&N.child[k]);
+  L.count = __ldcg(&N.count[k]);
+  if(L.count == 0) {
+    L.cost = __ldcg(&A.cost[L.child]);
+    L.height = __ldcg(&A.height[L.child]);
+    L.ninner = __ldcg(&A.ninner[L.child]);
+  } else {
+    L.cost = C_PRIM * half_area(L.lo, L.hi);
+    L.height = 0;
+    L.ninner = 0;
+  }
+}
+
+template<class R>
+__device__ __forceinline__ void union_of(const TLeaf<R>* L, int S, R lo[3], R hi[3])
+{
+  for(int c = 0; c < 3; ++c) { lo[c] = rmax<R>(); hi[c] = -rmax<R>(); }
+  for(int i = 0; S; ++i, S >>= 1)
+    if(S & 1)
+      for(int c = 0; c < 3; ++c) {
+        lo[c] = fmin(lo[c], L[i].lo[c]);
+        hi[c] = fmax(hi[c], L[i].hi[c]);
+      }
+}
+
+/* Treelet restructuring (Karras and Aila, "Fast Parallel Construction of
+ * High-Quality Bounding Volume Hierarchies", HPG 2013) at `root`, whose
+ * subtree is final: grow a treelet of up to TREELET leaves by opening the leaf of
+ * largest area that is a subtree, find the binary tree over those leaves of
+ * lowest SAH cost by dynamic programming over their subsets, and rebuild the
+ * treelet's internal nodes to it if that is cheaper than `cur`. The root
+ * keeps its index and box; the leaves' subtrees are untouched. Returns the
+ * root's cost and sets its height `h` and internal node count `ni`. */
+template<class R>
+__device__ float optimize_treelet(DNode<R>* nodes, int root, const Aux& A, float cur,
+                                  int& h, int& nin)
+{
+  TLeaf<R> L[TREELET];
+  int inner[TREELET - 1];
+  int nl = 2, ni = 1;
+  inner[0] = root;
+  read_slot(nodes[root], 0, A, L[0]);
+  read_slot(nodes[root], 1, A, L[1]);
+  while(nl < TREELET) {
+    int best = -1;
+    float ba = -1.f;
+    for(int i = 0; i < nl; ++i)
+      if(L[i].count == 0) {
+        const float a = half_area(L[i].lo, L[i].hi);
+        if(a > ba) { ba = a; best = i; }
+      }
+    if(best < 0) break;
+    const int nd = L[best].child;
+    inner[ni++] = nd;
+    read_slot(nodes[nd], 1, A, L[nl]);
+    read_slot(nodes[nd], 0, A, L[best]);
+    ++nl;
+  }
+  if(nl < 3) return cur;
+  const int full = (1 << nl) - 1;
+  float c[1 << TREELET];
+  uint8_t part[1 << TREELET];
+  for(int S = 1; S <= full; ++S) {
+    if(__popc(S) == 1) {
+      c[S] = L[__ffs(S) - 1].cost;
+      continue;
+    }
+    R lo[3], hi[3];
+    union_of(L, S, lo, hi);
+    /* each partition once: the part holding S's lowest leaf */
+    const int low = S & -S;
+    float bc = 3.4e38f;
+    int bp = low;
+    for(int P = (S - 1) & S; P; P = (P - 1) & S) {
+      if(!(P & low)) continue;
+      const float v = c[P] + c[S ^ P];
+      if(v < bc) { bc = v; bp = P; }
+    }
+    c[S] = C_NODE * half_area(lo, hi) + bc;
+    part[S] = (uint8_t)bp;
+  }
+  if(!(c[full] < cur * (1.f - 1e-5f))) return cur;
+  /* Rebuild, parents before children: entry q is internal node nidx[q]
+   * over leaf set nset[q]; kid[q][k] >= 0 is another entry, else the leaf
+   * -1 - kid */
+  int nset[TREELET - 1], nidx[TREELET - 1], kid[TREELET - 1][2];
+  int hh[TREELET - 1], nn[TREELET - 1];
+  int cnt = 1, next = 1;
+  nset[0] = full;
+  nidx[0] = root;
+  for(int q = 0; q < cnt; ++q) {
+    const int nd = nidx[q];
+    DNode<R>& N = nodes[nd];
+    const int S = nset[q];
+    const int T[2] = {part[S], S ^ part[S]};
+    for(int k = 0; k < 2; ++k) {
+      R lo[3], hi[3];
+      if(__popc(T[k]) == 1) {
+        const int i = __ffs(T[k]) - 1;
+        put_slot(N, k, L[i].lo, L[i].hi);
+        N.child[k] = L[i].child;
+        N.count[k] = L[i].count;
+        if(L[i].count == 0) A.parent[L[i].child] = (nd << 1) | k;
+        kid[q][k] = -1 - i;
+      } else {
+        const int m = inner[next++];
+        union_of(L, T[k], lo, hi);
+        put_slot(N, k, lo, hi);
+        N.child[k] = m;
+        N.count[k] = 0;
+        A.parent[m] = (nd << 1) | k;
+        nset[cnt] = T[k];
+        nidx[cnt] = m;
+        kid[q][k] = cnt++;
+      }
+    }
+  }
+  for(int q = cnt - 1; q >= 0; --q) {
+    int hm = 0, sum = 1;
+    for(int k = 0; k < 2; ++k) {
+      const int e = kid[q][k];
+      hm = max(hm, e >= 0 ? hh[e] : L[-1 - e].height);
+      sum += e >= 0 ? nn[e] : L[-1 - e].ninner;
+    }
+    hh[q] = 1 + hm;
+    nn[q] = sum;
+    A.cost[nidx[q]] = c[nset[q]];
+    A.height[nidx[q]] = hh[q];
+    A.ninner[nidx[q]] = nn[q];
+  }
+  h = hh[0];
+  nin = nn[0];
+  return c[full];
+}
+
+/* Step 5: boxes, SAH costs, heights and internal node counts, one thread
+ * per leaf; flags start at zero. With `optimize`, each node's treelet is
+ * restructured once its subtree is final, by the thread that completes it. */
 template<class R>
 __global__ void lbvh_boxes(const R* box, const uint32_t* vals, int n, DNode<R>* nodes,
-                           const int32_t* parent, uint32_t* flags, int32_t* height,
-                           int32_t* depth)
+                           const Aux A, uint32_t* flags, int32_t* depth, bool optimize)
 {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if(j >= n) return;
@@ -250,34 +439,76 @@ __global__ void lbvh_boxes(const R* box, const uint32_t* vals, int n, DNode<R>* 
     lo[c] = box[6 * src + c];
     hi[c] = box[6 * src + 3 + c];
   }
-  int p = parent[(n - 1) + j];
-  int node = p >> 1, slot = p & 1, h = 0;
+  int p = A.parent[(n - 1) + j];
+  int node = p >> 1, slot = p & 1, h = 0, nin = 0;
+  float my_cost = C_PRIM * half_area(lo, hi);
   put_slot(nodes[node], slot, lo, hi);
   for(;;) {
-    /* publish this slot (and the height below it) before arriving */
+    /* publish this slot (and what is known below it) before arriving */
     __threadfence();
     if(atomicAdd(&flags[node], 1u) == 0u) return;
     __threadfence();
-    /* both slots are final: the sibling's box and height were written by
-     * the thread that arrived first, read past L1 */
+    /* both slots are final: the sibling's box, cost and height were written
+     * by the thread that arrived first, read past L1 */
     DNode<R>& N = nodes[node];
-    const int o = 1 - slot;
+    TLeaf<R> sib;
+    read_slot(N, 1 - slot, A, sib);
     for(int c = 0; c < 3; ++c) {
-      lo[c] = fmin(lo[c], __ldcg(&N.lo[o][c]));
-      hi[c] = fmax(hi[c], __ldcg(&N.hi[o][c]));
+      lo[c] = fmin(lo[c], sib.lo[c]);
+      hi[c] = fmax(hi[c], sib.hi[c]);
     }
-    const int hs = N.count[o] == 0 ? __ldcg(&height[N.child[o]]) : 0;
-    h = 1 + max(h, hs);
-    height[node] = h;
+    h = 1 + max(h, sib.height);
+    nin = 1 + nin + sib.ninner;
+    my_cost = C_NODE * half_area(lo, hi) + my_cost + sib.cost;
+    if(optimize) my_cost = optimize_treelet(nodes, node, A, my_cost, h, nin);
+    A.cost[node] = my_cost;
+    A.height[node] = h;
+    A.ninner[node] = nin;
     if(node == 0) {
       *depth = h;
       return;
     }
-    p = parent[node];
+    p = A.parent[node];
     node = p >> 1;
     slot = p & 1;
     put_slot(nodes[node], slot, lo, hi);
   }
+}
+
+/* Step 6: depth-first order of the internal nodes (slot 0 first), as the
+ * host builder numbers them, so that a node's first child follows it in
+ * memory: a node's index is the sum, over the path from the root, of one
+ * per step plus, where the path takes slot 1, the internal nodes of the
+ * slot-0 subtree it passes by */
+template<class R>
+__global__ void lbvh_order(const DNode<R>* nodes, const int32_t* parent, const int32_t* ninner,
+                           int n, int32_t* newidx)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n - 1) return;
+  int x = 0, node = i;
+  while(node != 0) {
+    const int p = parent[node];
+    const int par = p >> 1;
+    x += 1;
+    if(p & 1) {
+      const DNode<R>& P = nodes[par];
+      if(P.count[0] == 0) x += ninner[P.child[0]];
+    }
+    node = par;
+  }
+  newidx[i] = x;
+}
+
+template<class R>
+__global__ void lbvh_permute(const DNode<R>* src, DNode<R>* dst, const int32_t* newidx, int n)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n - 1) return;
+  DNode<R> N = src[i];
+  for(int k = 0; k < 2; ++k)
+    if(N.count[k] == 0) N.child[k] = newidx[N.child[k]];
+  dst[newidx[i]] = N;
 }
 
 template<class R>
@@ -300,7 +531,14 @@ int launch_lbvh(const LbvhArgs& A, void* stream)
   lbvh_morton<R><<<g, 256, 0, s>>>(box, n, cb, k0, v0);
   lbvh_sort<<<1, SORT_THREADS, 0, s>>>(k0, v0, k1, v1, n);
   lbvh_nodes<R><<<g, 256, 0, s>>>(k0, v0, A.ref, n, nodes, A.parent);
-  lbvh_boxes<R><<<g, 256, 0, s>>>(box, v0, n, nodes, A.parent, A.flags, A.height, A.depth);
+  const Aux aux = {A.cost, A.height, A.ninner, A.parent};
+  lbvh_boxes<R><<<g, 256, 0, s>>>(box, v0, n, nodes, aux, A.flags, A.depth, A.optimize != 0);
+  DNode<R>* tmp = (DNode<R>*)A.tmp_nodes;
+  lbvh_order<R><<<g, 256, 0, s>>>(nodes, A.parent, A.ninner, n, A.newidx);
+  lbvh_permute<R><<<g, 256, 0, s>>>(nodes, tmp, A.newidx, n);
+  if(cudaMemcpyAsync(nodes, tmp, sizeof(DNode<R>) * (size_t)(n - 1), cudaMemcpyDeviceToDevice,
+                     s) != cudaSuccess)
+    return (int)cudaGetLastError();
   return (int)cudaGetLastError();
 }
 
@@ -309,9 +547,11 @@ int launch_lbvh(const LbvhArgs& A, void* stream)
 size_t lbvh_scratch_bytes(int n)
 {
   const size_t m = n > 0 ? (size_t)n : 0;
-  /* keys and vals (2n each), parent (2n), flags and heights (n each),
-   * centroid bounds (6 doubles), depth (one int, padded) */
-  return sizeof(uint32_t) * (2 * m + 2 * m + 2 * m + m + m) + 6 * sizeof(double) + 16;
+  /* centroid bounds (6 doubles), depth (one int, padded), a copy of the
+   * nodes (sized for FP64), keys and vals (2n each), parent (2n), flags,
+   * heights, costs, internal node counts and new indices (n each) */
+  return 6 * sizeof(double) + 16 + sizeof(DNode<double>) * m
+    + sizeof(uint32_t) * (2 * m + 2 * m + 2 * m + 5 * m);
 }
 
 void lbvh_bind_scratch(LbvhArgs& A, void* scratch)
@@ -323,6 +563,8 @@ void lbvh_bind_scratch(LbvhArgs& A, void* scratch)
   p += 6 * sizeof(double);
   A.depth = (int32_t*)p;
   p += 16;
+  A.tmp_nodes = p;
+  p += sizeof(DNode<double>) * m;
   A.keys = (uint32_t*)p;
   p += sizeof(uint32_t) * 2 * m;
   A.vals = (uint32_t*)p;
@@ -332,6 +574,12 @@ void lbvh_bind_scratch(LbvhArgs& A, void* scratch)
   A.flags = (uint32_t*)p;
   p += sizeof(uint32_t) * m;
   A.height = (int32_t*)p;
+  p += sizeof(int32_t) * m;
+  A.cost = (float*)p;
+  p += sizeof(float) * m;
+  A.ninner = (int32_t*)p;
+  p += sizeof(int32_t) * m;
+  A.newidx = (int32_t*)p;
 }
 
 int launch_lbvh_f32(const LbvhArgs& A, void* stream) { return launch_lbvh<float>(A, stream); }

@@ -605,6 +605,7 @@ static res_T upload(ssol_b200_plan* p, const FlatScene<R>& f, DScene<R>& S)
     A.box = base + o_box;
     A.ref = (const uint32_t*)(base + o_ref);
     A.nodes = base + b.offsets[0];
+    A.optimize = 1;
     lbvh_bind_scratch(A, base + o_scratch);
     if(launch_lbvh_r(A, st, R()) != 0) return RES_UNKNOWN_ERR;
     int32_t depth = 0;

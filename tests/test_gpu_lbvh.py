@@ -6,9 +6,8 @@ closest accepted hit whatever the tree, so a solve traces the same paths with
 either: on the same seed every estimate agrees to the order of the FP64
 reductions (1e-10 relative). This is the device replacement of the
 reference's per-solve Star-3D view build (src/ssol_scene.c:347-433), checked
-through the estimates the reference's own tests read. A layout whose linear
-BVH is deeper than the traversal stack allows is rebuilt on the host (the
-stats say which builder ran)."""
+through the estimates the reference's own tests read. The stats say which
+builder ran and how deep its tree is."""
 import pytest
 
 import pyssol as P
@@ -83,7 +82,8 @@ def test_lbvh_fp64_and_single_mirror(product):
 def _deep_layout(lib):
     """36 small horizontal matte triangles whose Morton codes are 0 (five of
     them), each single bit of the 30 (one triangle per axis and bit) and all
-    ones: the linear BVH peels one triangle off per level, 33 levels deep."""
+    ones: the linear hierarchy peels one triangle off per level, 33 levels
+    deep, more than the traversal stack holds."""
     s = P.Scene(lib)
     centres = [(0.1 * k, 0.0, 0.0) for k in range(5)]
     for lvl in range(10):
@@ -103,12 +103,16 @@ def _deep_layout(lib):
     return s, inst
 
 
-def test_lbvh_too_deep_falls_back_to_sah(product):
+def test_lbvh_chain_layout_is_restructured(product):
+    """The treelet restructuring balances the 33-level chain of the linear
+    hierarchy to about half that depth, so the tree is built on the device and
+    traced as is, with the SAH tree's results."""
     s, inst = _deep_layout(product)
     sah, lbvh = _solve_pair(s, 200_000, seed=1)
     st, sl = sah.stats(), lbvh.stats()
-    assert sl["bvh_device"] == 0
-    assert sl["bvh_depth"] == st["bvh_depth"] <= 30
+    assert sl["bvh_device"] == 1 and st["bvh_device"] == 0
+    assert 1 <= sl["bvh_depth"] <= 20
+    assert sl["bvh_nodes"] == 35
     _same(lbvh.globals(), sah.globals(), "globals")
     _same(lbvh.receiver(inst, P.SSOL_FRONT), sah.receiver(inst, P.SSOL_FRONT), "front")
     s.close()
