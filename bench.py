@@ -292,13 +292,14 @@ def run_b200(args):
     lib = P.load_product()
     s, h, desc = build_workload(lib, args)
     opt = P.options(P.FP64 if args.fp64 else P.FP32, block_size=args.block,
-                    waves=args.waves, leaf=args.leaf, min_blocks=args.minb)
+                    waves=args.waves, leaf=args.leaf, min_blocks=args.minb,
+                    bvh=BVH_CHOICES[args.bvh])
     tuned_ms = None
     if args.autotune:
         opt, tuned_ms = P.autotune(s, args.autotune_paths, opt, seed=args.seed + 77)
     launch_shape = {"block": opt.block_size, "blocks_per_sm_budget": opt.min_blocks_per_sm,
                     "waves": opt.waves, "bvh_leaf": opt.bvh_leaf_size,
-                    "autotuned": bool(args.autotune)}
+                    "bvh_builder": args.bvh, "autotuned": bool(args.autotune)}
     plan = P.C.c_void_p()
     lib.call("ssol_b200_plan_create", s.scn, P.C.byref(opt), P.C.byref(plan))
     rng = s.rng(seed=args.seed)
@@ -520,6 +521,9 @@ def run_b200(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+BVH_CHOICES = {"auto": 0, "sah": 1, "lbvh": 2}
 
 
 def bvh_builders(lib, s, opt, n, stream, sp, flush):
@@ -884,7 +888,8 @@ def run_suns(args):
                                 device_id=torch.device("cuda", local))
     lib = P.load_product()
     opt = P.options(P.FP64 if args.fp64 else P.FP32, block_size=args.block,
-                    waves=args.waves, leaf=args.leaf, min_blocks=args.minb)
+                    waves=args.waves, leaf=args.leaf, min_blocks=args.minb,
+                    bvh=BVH_CHOICES[args.bvh])
     if args.autotune:
         s, h = W.heliostat_field(lib, n_helio=args.heliostats, elevation=45.0)
         opt, _ = P.autotune(s, args.autotune_paths, opt, seed=args.seed + 77)
@@ -1301,6 +1306,9 @@ def main():
     p.add_argument("--no-fp64-check", action="store_true",
                    help="skip the FP32 vs all-FP64 comparison of the field configs")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--bvh", default="auto", choices=sorted(BVH_CHOICES),
+                   help="BVH builder of the solves (auto: by solve size for ssol_solve, "
+                        "host SAH for plans)")
     p.add_argument("--no-bvh-compare", action="store_true",
                    help="skip the host SAH against device LBVH builder comparison")
     p.add_argument("--no-suns", action="store_true",

@@ -30,19 +30,27 @@ enum ssol_b200_precision {
 /* Who builds the ray-tracing BVH of a plan's snapshot (the reference builds
  * its Star-3D view on every solve, src/ssol_scene.c:347-433):
  *  - SSOL_B200_BVH_SAH: binned-SAH tree on the host threads, uploaded with
- *    the snapshot; leaves of bvh_leaf_size primitives;
+ *    the snapshot; leaves of bvh_leaf_size primitives; the fastest to trace;
  *  - SSOL_B200_BVH_LBVH: linear BVH built on the device from the uploaded
  *    primitive boxes (Morton codes, radix sort, Karras' hierarchy, bottom-up
  *    boxes, treelet restructuring for a lower SAH cost, depth-first node
- *    order), one primitive per leaf (bvh_leaf_size is ignored). A tree
- *    deeper than the traversal stack allows (more than 30 levels) is rebuilt
- *    on the host with the SAH builder, with a warning. Both trees find the
- *    same closest hits; only the time to build them and to traverse them
- *    differs. Batches and the renderers always use the SAH builder. */
+ *    order), one primitive per leaf (bvh_leaf_size is ignored); the fastest
+ *    to build. A tree deeper than the traversal stack allows (more than 30
+ *    levels) is rebuilt on the host with the SAH builder, with a warning;
+ *  - SSOL_B200_BVH_AUTO (the default): ssol_solve and ssol_solve_ex use the
+ *    device builder for solves of at most SSOL_B200_BVH_AUTO_MAX_PATHS
+ *    realisations, where building is a large part of the call, and the SAH
+ *    builder above; plans, which do not know how many realisations they will
+ *    trace, use the SAH builder.
+ * Both trees find the same closest hits; only the time to build them and to
+ * traverse them differs. Batches and the renderers always use the SAH
+ * builder. */
 enum ssol_b200_bvh_builder {
-  SSOL_B200_BVH_SAH = 0,
-  SSOL_B200_BVH_LBVH = 1
+  SSOL_B200_BVH_AUTO = 0,
+  SSOL_B200_BVH_SAH = 1,
+  SSOL_B200_BVH_LBVH = 2
 };
+#define SSOL_B200_BVH_AUTO_MAX_PATHS (1ull << 24)
 
 struct ssol_b200_options {
   enum ssol_b200_precision precision;
@@ -55,7 +63,7 @@ struct ssol_b200_options {
                           * 0 => 3 in FP32, 2 in FP64 */
   enum ssol_b200_bvh_builder bvh_builder; /* plans and ssol_solve_ex */
 };
-#define SSOL_B200_OPTIONS_DEFAULT__ { SSOL_B200_FP32, 256, 0, 1, 0, 0, 0, SSOL_B200_BVH_SAH }
+#define SSOL_B200_OPTIONS_DEFAULT__ { SSOL_B200_FP32, 256, 0, 1, 0, 0, 0, SSOL_B200_BVH_AUTO }
 static const struct ssol_b200_options SSOL_B200_OPTIONS_DEFAULT =
   SSOL_B200_OPTIONS_DEFAULT__;
 

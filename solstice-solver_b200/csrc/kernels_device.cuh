@@ -1519,8 +1519,9 @@ realisation_kernel
       if(p.phase == PH_NONE && !done) {
         if(got) {
           start = true;
-          off = sorted_off[idx];
-          const uint4 d = sorted_draw[idx];
+          /* read once: streaming loads, evicted from L2 first */
+          off = __ldcs(&sorted_off[idx]);
+          const uint4 d = __ldcs(&sorted_draw[idx]);
           r0 = {{d.x, d.y, d.z, d.w}};
         } else if(exhausted) {
           done = true;
@@ -1845,8 +1846,8 @@ batch_kernel
                 ? (unsigned long long)((uint32_t)sg * seg_mul[it] % (uint32_t)nfull)
                 : sg * seg_mul[it] % nfull;
             const unsigned long long rec = prefix[it] + sg * SORT_SEG + g % SORT_SEG;
-            off = sorted_off[rec];
-            const uint4 d = sorted_draw[rec];
+            off = __ldcs(&sorted_off[rec]);
+            const uint4 d = __ldcs(&sorted_draw[rec]);
             r0 = {{d.x, d.y, d.z, d.w}};
           }
           const uint64_t id = firsts[it] + off;

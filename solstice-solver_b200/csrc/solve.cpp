@@ -730,8 +730,11 @@ extern "C" res_T ssol_b200_plan_create
   if(opt.max_segments == 0) opt.max_segments = 1000000ull;
   if(opt.min_blocks_per_sm < 0 || opt.min_blocks_per_sm > 3) return RES_BAD_ARG;
   if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = default_min_blocks(opt.precision);
-  if(opt.bvh_builder != SSOL_B200_BVH_SAH && opt.bvh_builder != SSOL_B200_BVH_LBVH)
+  if(opt.bvh_builder != SSOL_B200_BVH_AUTO && opt.bvh_builder != SSOL_B200_BVH_SAH
+  && opt.bvh_builder != SSOL_B200_BVH_LBVH)
     return RES_BAD_ARG;
+  /* a plan does not know how many realisations it will trace */
+  if(opt.bvh_builder == SSOL_B200_BVH_AUTO) opt.bvh_builder = SSOL_B200_BVH_SAH;
   if(opt.bvh_builder == SSOL_B200_BVH_LBVH) opt.bvh_leaf_size = 1;
 
   BvhBuildParams bp;
@@ -2098,8 +2101,15 @@ extern "C" res_T ssol_solve_ex
   *out = nullptr;
   if(n > (size_t)INT64_MAX || max_failed > (size_t)INT64_MAX)
     return RES_BAD_ARG;
+  /* The default builder by solve size: below the threshold, building the
+   * tree on the device saves more (2 ms on the 1000-heliostat field) than
+   * its slightly slower traversal costs */
+  ssol_b200_options opt = options ? *options : SSOL_B200_OPTIONS_DEFAULT;
+  if(opt.bvh_builder == SSOL_B200_BVH_AUTO)
+    opt.bvh_builder = (unsigned long long)n <= SSOL_B200_BVH_AUTO_MAX_PATHS
+      ? SSOL_B200_BVH_LBVH : SSOL_B200_BVH_SAH;
   ssol_b200_plan* plan = nullptr;
-  res_T res = ssol_b200_plan_create(scn, options, &plan);
+  res_T res = ssol_b200_plan_create(scn, &opt, &plan);
   if(res != RES_OK) return res;
   if(!tracker) {
     res = plan_launch(plan, rng, 0, n, nullptr, nullptr, (unsigned long long)max_failed);

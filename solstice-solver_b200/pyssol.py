@@ -159,7 +159,7 @@ class B200Options(C.Structure):
                 ("bvh_builder", C.c_int)]
 
 
-BVH_SAH, BVH_LBVH = 0, 1
+BVH_AUTO, BVH_SAH, BVH_LBVH = 0, 1, 2
 
 
 class SunPosition(C.Structure):
@@ -933,7 +933,7 @@ def estimator_from_tallies(scene, rng, n, sums, counts, max_failed=0):
 
 
 def options(precision=FP32, block_size=256, grid_blocks=0, waves=1, leaf=0,
-            max_segments=0, min_blocks=0, bvh=BVH_SAH):
+            max_segments=0, min_blocks=0, bvh=BVH_AUTO):
     o = B200Options()
     o.precision = precision
     o.block_size = block_size

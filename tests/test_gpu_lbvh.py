@@ -116,3 +116,21 @@ def test_lbvh_chain_layout_is_restructured(product):
     _same(lbvh.globals(), sah.globals(), "globals")
     _same(lbvh.receiver(inst, P.SSOL_FRONT), sah.receiver(inst, P.SSOL_FRONT), "front")
     s.close()
+
+
+def test_default_builder_by_solve_size(product):
+    """With the default options, ssol_solve builds the tree on the device for
+    solves of at most 2^24 realisations and on the host above; a plan, which
+    does not know its solve size, gets the host tree."""
+    import ctypes as C
+    s, h = W.single_mirror(product)
+    assert s.solve(100_000, seed=1).stats()["bvh_device"] == 1
+    assert s.solve((1 << 24) + 1, seed=1).stats()["bvh_device"] == 0
+    assert s.solve(100_000, seed=1, options=P.options()).stats()["bvh_device"] == 1
+    plan = C.c_void_p()
+    product.call("ssol_b200_plan_create", s.scn, None, C.byref(plan))
+    st = P.B200Stats()
+    product.call("ssol_b200_plan_get_stats", plan, C.byref(st))
+    assert st.bvh_device == 0 and st.bvh_nodes >= 1
+    product.call("ssol_b200_plan_ref_put", plan)
+    s.close()
