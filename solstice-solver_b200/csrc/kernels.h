@@ -154,6 +154,8 @@ struct LbvhArgs {
   float* cost;
   int32_t* ninner;
   int32_t* newidx;
+  int32_t* level_nodes;
+  int32_t* level_first; /* MAX_LEVELS + 1 offsets, then the largest height */
   void* tmp_nodes;
   int optimize; /* treelet restructuring of every node's subtree */
 };

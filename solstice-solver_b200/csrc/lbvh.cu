@@ -5,7 +5,8 @@
  *
  * It replaces, on the device, the per-solve Star-3D view build of the
  * reference (src/ssol_scene.c:347-433, s3d_scene_view_create at :410-413).
- * Six steps on one stream, no host round trip between them:
+ * Seven steps on one stream; the host reads the height histogram back once,
+ * to size the per-height launches:
  *   1. centroid bounds of the primitive boxes (one block);
  *   2. 30-bit Morton code of each centroid in those bounds (10 bits per axis);
  *   3. stable LSD radix sort of (code, primitive) pairs, 4 passes of 8 bits,
@@ -22,17 +23,20 @@
  *      its parent's slot; the second thread to reach a node (an atomic
  *      arrival count) merges the node's two slots and goes on, the first
  *      stops, so no thread waits on another. The same walk computes each
- *      node's SAH cost, height and internal-node count, and restructures the
- *      node's treelet for a lower SAH cost (Karras and Aila, HPG 2013) once
- *      its subtree is final; the root's height is the tree depth, which the
- *      host reads back to check the traversal stack bound;
- *   6. the internal nodes are renumbered depth first, slot 0 first, so that
+ *      node's SAH cost, height and internal-node count;
+ *   6. treelet restructuring for a lower SAH cost (Karras and Aila, HPG
+ *      2013): the nodes grouped by height, then one launch per height, lowest
+ *      first, one warp per node, whose lanes share the dynamic program over
+ *      the treelet's leaf subsets; the root's height is the tree depth, which
+ *      the host reads back to check the traversal stack bound;
+ *   7. the internal nodes are renumbered depth first, slot 0 first, so that
  *      a node's first child follows it in memory.
  */
 #include "kernels.h"
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 
 namespace ssolb {
@@ -314,71 +318,20 @@ __device__ __forceinline__ void union_of(const TLeaf<R>* L, int S, R lo[3], R hi
       }
 }
 
-/* Treelet restructuring (Karras and Aila, "Fast Parallel Construction of
- * High-Quality Bounding Volume Hierarchies", HPG 2013) at `root`, whose
- * subtree is final: grow a treelet of up to TREELET leaves by opening the leaf of
- * largest area that is a subtree, find the binary tree over those leaves of
- * lowest SAH cost by dynamic programming over their subsets, and rebuild the
- * treelet's internal nodes to it if that is cheaper than `cur`. The root
- * keeps its index and box; the leaves' subtrees are untouched. Returns the
- * root's cost and sets its height `h` and internal node count `ni`. */
+/* Rewrite the internal nodes of a treelet (root first, then inner[1..]) to
+ * the binary tree over its nl leaves that part[] describes (part[S]: the
+ * subset holding S's lowest leaf), and set their parent links, costs (c[]),
+ * heights and internal node counts. The root keeps its index and box; the
+ * leaves' subtrees are untouched. */
 template<class R>
-__device__ float optimize_treelet(DNode<R>* nodes, int root, const Aux& A, float cur,
-                                  int& h, int& nin)
+__device__ void rebuild_treelet(DNode<R>* nodes, const Aux& A, const TLeaf<R>* L, int nl,
+                                const int* inner, const float* c, const uint8_t* part)
 {
-  TLeaf<R> L[TREELET];
-  int inner[TREELET - 1];
-  int nl = 2, ni = 1;
-  inner[0] = root;
-  read_slot(nodes[root], 0, A, L[0]);
-  read_slot(nodes[root], 1, A, L[1]);
-  while(nl < TREELET) {
-    int best = -1;
-    float ba = -1.f;
-    for(int i = 0; i < nl; ++i)
-      if(L[i].count == 0) {
-        const float a = half_area(L[i].lo, L[i].hi);
-        if(a > ba) { ba = a; best = i; }
-      }
-    if(best < 0) break;
-    const int nd = L[best].child;
-    inner[ni++] = nd;
-    read_slot(nodes[nd], 1, A, L[nl]);
-    read_slot(nodes[nd], 0, A, L[best]);
-    ++nl;
-  }
-  if(nl < 3) return cur;
-  const int full = (1 << nl) - 1;
-  float c[1 << TREELET];
-  uint8_t part[1 << TREELET];
-  for(int S = 1; S <= full; ++S) {
-    if(__popc(S) == 1) {
-      c[S] = L[__ffs(S) - 1].cost;
-      continue;
-    }
-    R lo[3], hi[3];
-    union_of(L, S, lo, hi);
-    /* each partition once: the part holding S's lowest leaf */
-    const int low = S & -S;
-    float bc = 3.4e38f;
-    int bp = low;
-    for(int P = (S - 1) & S; P; P = (P - 1) & S) {
-      if(!(P & low)) continue;
-      const float v = c[P] + c[S ^ P];
-      if(v < bc) { bc = v; bp = P; }
-    }
-    c[S] = C_NODE * half_area(lo, hi) + bc;
-    part[S] = (uint8_t)bp;
-  }
-  if(!(c[full] < cur * (1.f - 1e-5f))) return cur;
-  /* Rebuild, parents before children: entry q is internal node nidx[q]
-   * over leaf set nset[q]; kid[q][k] >= 0 is another entry, else the leaf
-   * -1 - kid */
   int nset[TREELET - 1], nidx[TREELET - 1], kid[TREELET - 1][2];
   int hh[TREELET - 1], nn[TREELET - 1];
   int cnt = 1, next = 1;
-  nset[0] = full;
-  nidx[0] = root;
+  nset[0] = (1 << nl) - 1;
+  nidx[0] = inner[0];
   for(int q = 0; q < cnt; ++q) {
     const int nd = nidx[q];
     DNode<R>& N = nodes[nd];
@@ -419,17 +372,141 @@ __device__ float optimize_treelet(DNode<R>* nodes, int root, const Aux& A, float
     A.height[nidx[q]] = hh[q];
     A.ninner[nidx[q]] = nn[q];
   }
-  h = hh[0];
-  nin = nn[0];
-  return c[full];
+}
+
+constexpr int MAX_LEVELS = 128;
+
+/* Internal nodes grouped by height (one block): level_first[h] .. [h + 1]
+ * of level_nodes; *maxh the largest height present. Nodes of one height
+ * are never ancestors of one another, so their treelets are disjoint. */
+__global__ void __launch_bounds__(SORT_THREADS) lbvh_levels
+  (const int32_t* height, int m, int32_t* level_first, int32_t* level_nodes, int32_t* maxh)
+{
+  __shared__ uint32_t cnt[MAX_LEVELS], cur[MAX_LEVELS];
+  const int tid = threadIdx.x;
+  for(int h = tid; h < MAX_LEVELS; h += SORT_THREADS) cnt[h] = 0;
+  __syncthreads();
+  for(int i = tid; i < m; i += SORT_THREADS)
+    atomicAdd(&cnt[min(max(height[i], 0), MAX_LEVELS - 1)], 1u);
+  __syncthreads();
+  if(tid == 0) {
+    uint32_t run = 0;
+    int mh = 0;
+    for(int h = 0; h < MAX_LEVELS; ++h) {
+      level_first[h] = (int32_t)run;
+      cur[h] = run;
+      run += cnt[h];
+      if(cnt[h]) mh = h;
+    }
+    level_first[MAX_LEVELS] = (int32_t)run;
+    *maxh = mh;
+  }
+  __syncthreads();
+  for(int i = tid; i < m; i += SORT_THREADS)
+    level_nodes[atomicAdd(&cur[min(max(height[i], 0), MAX_LEVELS - 1)], 1u)] = i;
+}
+
+constexpr int TREELET_WARPS = 4;
+
+/* Treelet restructuring (Karras and Aila, "Fast Parallel Construction of
+ * High-Quality Bounding Volume Hierarchies", HPG 2013) of the nodes of one
+ * height, one warp per node, heights in increasing order (one launch each),
+ * so that a node's subtree is final when its treelet is formed. Lane 0
+ * refreshes the node's cost, height and node count from its slots (its
+ * descendants may have changed), then grows a treelet of up to TREELET
+ * leaves by opening the leaf of largest area that is a subtree; the lanes
+ * then find the binary tree over those leaves of lowest SAH cost by dynamic
+ * programming over their subsets, all subsets of one size at a time; lane 0
+ * rewrites the treelet's internal nodes to it if it is cheaper. */
+template<class R>
+__global__ void __launch_bounds__(32 * TREELET_WARPS) lbvh_treelets
+  (DNode<R>* nodes, const Aux A, const int32_t* level_first, const int32_t* level_nodes,
+   int level, int32_t* depth)
+{
+  __shared__ TLeaf<R> Ls[TREELET_WARPS][TREELET];
+  __shared__ float cs[TREELET_WARPS][1 << TREELET];
+  __shared__ uint8_t ps[TREELET_WARPS][1 << TREELET];
+  __shared__ int inner_s[TREELET_WARPS][TREELET - 1];
+  __shared__ int nl_s[TREELET_WARPS];
+  __shared__ float cur_s[TREELET_WARPS];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int first = level_first[level], count = level_first[level + 1] - first;
+  TLeaf<R>* L = Ls[w];
+  float* c = cs[w];
+  uint8_t* part = ps[w];
+  for(int t = blockIdx.x * TREELET_WARPS + w; t < count; t += gridDim.x * TREELET_WARPS) {
+    const int root = level_nodes[first + t];
+    if(lane == 0) {
+      read_slot(nodes[root], 0, A, L[0]);
+      read_slot(nodes[root], 1, A, L[1]);
+      R lo[3], hi[3];
+      union_of(L, 3, lo, hi);
+      const float cur = C_NODE * half_area(lo, hi) + L[0].cost + L[1].cost;
+      const int h = 1 + max(L[0].height, L[1].height);
+      A.cost[root] = cur;
+      A.height[root] = h;
+      A.ninner[root] = 1 + L[0].ninner + L[1].ninner;
+      if(root == 0) *depth = h;
+      int nl = 2, ni = 1;
+      inner_s[w][0] = root;
+      while(nl < TREELET) {
+        int best = -1;
+        float ba = -1.f;
+        for(int i = 0; i < nl; ++i)
+          if(L[i].count == 0) {
+            const float a = half_area(L[i].lo, L[i].hi);
+            if(a > ba) { ba = a; best = i; }
+          }
+        if(best < 0) break;
+        const int nd = L[best].child;
+        inner_s[w][ni++] = nd;
+        read_slot(nodes[nd], 1, A, L[nl]);
+        read_slot(nodes[nd], 0, A, L[best]);
+        ++nl;
+      }
+      nl_s[w] = nl;
+      cur_s[w] = cur;
+    }
+    __syncwarp();
+    const int nl = nl_s[w];
+    if(nl >= 3) {
+      const int full = (1 << nl) - 1;
+      for(int S = lane + 1; S <= full; S += 32)
+        if(__popc(S) == 1) c[S] = L[__ffs(S) - 1].cost;
+      __syncwarp();
+      for(int k = 2; k <= nl; ++k) {
+        for(int S = lane + 1; S <= full; S += 32) {
+          if(__popc(S) != k) continue;
+          R lo[3], hi[3];
+          union_of(L, S, lo, hi);
+          /* each partition once: the part holding S's lowest leaf */
+          const int low = S & -S;
+          float bc = 3.4e38f;
+          int bp = low;
+          for(int P = (S - 1) & S; P; P = (P - 1) & S) {
+            if(!(P & low)) continue;
+            const float v = c[P] + c[S ^ P];
+            if(v < bc) { bc = v; bp = P; }
+          }
+          c[S] = C_NODE * half_area(lo, hi) + bc;
+          part[S] = (uint8_t)bp;
+        }
+        __syncwarp();
+      }
+      if(lane == 0 && c[full] < cur_s[w] * (1.f - 1e-5f)) {
+        rebuild_treelet(nodes, A, L, nl, inner_s[w], c, part);
+        if(root == 0) *depth = A.height[0];
+      }
+    }
+    __syncwarp();
+  }
 }
 
 /* Step 5: boxes, SAH costs, heights and internal node counts, one thread
- * per leaf; flags start at zero. With `optimize`, each node's treelet is
- * restructured once its subtree is final, by the thread that completes it. */
+ * per leaf; flags start at zero */
 template<class R>
 __global__ void lbvh_boxes(const R* box, const uint32_t* vals, int n, DNode<R>* nodes,
-                           const Aux A, uint32_t* flags, int32_t* depth, bool optimize)
+                           const Aux A, uint32_t* flags, int32_t* depth)
 {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if(j >= n) return;
@@ -460,7 +537,6 @@ __global__ void lbvh_boxes(const R* box, const uint32_t* vals, int n, DNode<R>* 
     h = 1 + max(h, sib.height);
     nin = 1 + nin + sib.ninner;
     my_cost = C_NODE * half_area(lo, hi) + my_cost + sib.cost;
-    if(optimize) my_cost = optimize_treelet(nodes, node, A, my_cost, h, nin);
     A.cost[node] = my_cost;
     A.height[node] = h;
     A.ninner[node] = nin;
@@ -532,7 +608,26 @@ int launch_lbvh(const LbvhArgs& A, void* stream)
   lbvh_sort<<<1, SORT_THREADS, 0, s>>>(k0, v0, k1, v1, n);
   lbvh_nodes<R><<<g, 256, 0, s>>>(k0, v0, A.ref, n, nodes, A.parent);
   const Aux aux = {A.cost, A.height, A.ninner, A.parent};
-  lbvh_boxes<R><<<g, 256, 0, s>>>(box, v0, n, nodes, aux, A.flags, A.depth, A.optimize != 0);
+  lbvh_boxes<R><<<g, 256, 0, s>>>(box, v0, n, nodes, aux, A.flags, A.depth);
+  if(A.optimize && n >= 3) {
+    /* the heights decide how many levels to launch and how wide */
+    lbvh_levels<<<1, SORT_THREADS, 0, s>>>(A.height, n - 1, A.level_first, A.level_nodes,
+                                           A.level_first + MAX_LEVELS + 1);
+    int32_t lf[MAX_LEVELS + 2];
+    if(cudaMemcpyAsync(lf, A.level_first, sizeof(lf), cudaMemcpyDeviceToHost, s) != cudaSuccess
+    || cudaStreamSynchronize(s) != cudaSuccess)
+      return (int)cudaGetLastError();
+    const int maxh = lf[MAX_LEVELS + 1];
+    if(maxh < MAX_LEVELS - 1)
+      for(int h = 2; h <= maxh; ++h) {
+        const int cnt = lf[h + 1] - lf[h];
+        if(cnt <= 0) continue;
+        const unsigned blocks = (unsigned)std::min(
+          (cnt + TREELET_WARPS - 1) / TREELET_WARPS, 148 * 8);
+        lbvh_treelets<R><<<blocks, 32 * TREELET_WARPS, 0, s>>>(nodes, aux, A.level_first,
+                                                               A.level_nodes, h, A.depth);
+      }
+  }
   DNode<R>* tmp = (DNode<R>*)A.tmp_nodes;
   lbvh_order<R><<<g, 256, 0, s>>>(nodes, A.parent, A.ninner, n, A.newidx);
   lbvh_permute<R><<<g, 256, 0, s>>>(nodes, tmp, A.newidx, n);
@@ -549,9 +644,10 @@ size_t lbvh_scratch_bytes(int n)
   const size_t m = n > 0 ? (size_t)n : 0;
   /* centroid bounds (6 doubles), depth (one int, padded), a copy of the
    * nodes (sized for FP64), keys and vals (2n each), parent (2n), flags,
-   * heights, costs, internal node counts and new indices (n each) */
+   * heights, costs, internal node counts, new indices and nodes by level (n
+   * each), level offsets and the largest height */
   return 6 * sizeof(double) + 16 + sizeof(DNode<double>) * m
-    + sizeof(uint32_t) * (2 * m + 2 * m + 2 * m + 5 * m);
+    + sizeof(uint32_t) * (2 * m + 2 * m + 2 * m + 6 * m) + sizeof(int32_t) * (MAX_LEVELS + 2);
 }
 
 void lbvh_bind_scratch(LbvhArgs& A, void* scratch)
@@ -580,6 +676,10 @@ void lbvh_bind_scratch(LbvhArgs& A, void* scratch)
   A.ninner = (int32_t*)p;
   p += sizeof(int32_t) * m;
   A.newidx = (int32_t*)p;
+  p += sizeof(int32_t) * m;
+  A.level_nodes = (int32_t*)p;
+  p += sizeof(int32_t) * m;
+  A.level_first = (int32_t*)p;
 }
 
 int launch_lbvh_f32(const LbvhArgs& A, void* stream) { return launch_lbvh<float>(A, stream); }
