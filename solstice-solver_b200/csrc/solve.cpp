@@ -1003,8 +1003,11 @@ extern "C" res_T ssol_b200_autotune
         }
     ssol_b200_plan_ref_put(plan);
   }
+  /* the tuner picks the launch shape and the leaf size, not the builder (a
+   * plan resolves the default builder to the host one) */
   best_opt.precision = base.precision;
   best_opt.max_segments = base.max_segments;
+  best_opt.bvh_builder = base.bvh_builder;
   *options = best_opt;
   if(best_ms) *best_ms = best;
   return RES_OK;

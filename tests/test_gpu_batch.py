@@ -61,6 +61,8 @@ def test_autotune_picks_a_valid_shape(product):
     assert opt.min_blocks_per_sm in (1, 2, 3)
     assert opt.waves in (1, 2)
     assert opt.bvh_leaf_size in (1, 2, 4)
+    # the builder is the caller's choice, kept as given (default: by solve size)
+    assert opt.bvh_builder == P.BVH_AUTO
     a = s.solve(2000000, seed=4, options=opt).globals()
     b = s.solve(2000000, seed=4).globals()
     for k in b:
