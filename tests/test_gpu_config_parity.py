@@ -66,33 +66,39 @@ def test_config1_single_mirror_1e6(product, oracle):
 
 
 def test_config2_full_field_vs_oracle(product, oracle):
+    """Both BVH builders (the host SAH tree of this solve size's default, and
+    the device-built tree) against one oracle solve."""
     n = 17_000_000
     sg, hg = W.heliostat_field(product)
     sc, hc = W.heliostat_field(oracle)
-    eg, ec = sg.solve(n, seed=2), sc.solve(n, seed=2)
-    assert eg.count("realisation_count") == ec.count("realisation_count") == n
-    assert eg.count("failed_count") == ec.count("failed_count") == 0
-    assert eg.stats()["paths"] == n
-    assert_dict_close(eg.globals(), ec.globals(), "globals")
-    assert_dict_close(eg.receiver(hg["receiver"]), ec.receiver(hc["receiver"]), "receiver")
-    pg = eg.primitives(hg["receiver"], hg["receiver_shape"])
-    pc = ec.primitives(hc["receiver"], hc["receiver_shape"])
-    assert len(pg) == len(pc) == 64 * 64 * 2
-    bad = [(i, bad_keys(a, b)) for i, (a, b) in enumerate(zip(pg, pc)) if bad_keys(a, b)]
-    assert not bad, "primitives differ: %r" % bad[:5]
-    bad = []
-    for k, (xg, xc) in enumerate(zip(hg["heliostats"], hc["heliostats"])):
-        d = bad_keys(eg.sampled_x_receiver(xg, hg["receiver"]),
-                     ec.sampled_x_receiver(xc, hc["receiver"]))
-        a, b = eg.sampled(xg), ec.sampled(xc)
-        if a["nb_samples"] != b["nb_samples"]:
-            d["nb_samples"] = (a["nb_samples"], b["nb_samples"])
-        for q in ("cos_factor", "shadowed"):
-            if not close(a[q], b[q]):
-                d[q] = (a[q], b[q])
-        if d:
-            bad.append((k, d))
-    assert not bad, "heliostats differ: %r" % bad[:5]
+    ec = sc.solve(n, seed=2)
+    for bvh in (P.BVH_SAH, P.BVH_LBVH):
+        eg = sg.solve(n, seed=2, options=P.options(bvh=bvh))
+        assert eg.stats()["bvh_device"] == (1 if bvh == P.BVH_LBVH else 0)
+        assert eg.count("realisation_count") == ec.count("realisation_count") == n
+        assert eg.count("failed_count") == ec.count("failed_count") == 0
+        assert eg.stats()["paths"] == n
+        assert_dict_close(eg.globals(), ec.globals(), "globals")
+        assert_dict_close(eg.receiver(hg["receiver"]), ec.receiver(hc["receiver"]), "receiver")
+        pg = eg.primitives(hg["receiver"], hg["receiver_shape"])
+        pc = ec.primitives(hc["receiver"], hc["receiver_shape"])
+        assert len(pg) == len(pc) == 64 * 64 * 2
+        bad = [(i, bad_keys(a, b)) for i, (a, b) in enumerate(zip(pg, pc)) if bad_keys(a, b)]
+        assert not bad, "primitives differ (builder %d): %r" % (bvh, bad[:5])
+        bad = []
+        for k, (xg, xc) in enumerate(zip(hg["heliostats"], hc["heliostats"])):
+            d = bad_keys(eg.sampled_x_receiver(xg, hg["receiver"]),
+                         ec.sampled_x_receiver(xc, hc["receiver"]))
+            a, b = eg.sampled(xg), ec.sampled(xc)
+            if a["nb_samples"] != b["nb_samples"]:
+                d["nb_samples"] = (a["nb_samples"], b["nb_samples"])
+            for q in ("cos_factor", "shadowed"):
+                if not close(a[q], b[q]):
+                    d[q] = (a[q], b[q])
+            if d:
+                bad.append((k, d))
+        assert not bad, "heliostats differ (builder %d): %r" % (bvh, bad[:5])
+        del eg
     sg.close()
     sc.close()
 
