@@ -45,11 +45,11 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 DRAM_BYTES_PER_PATH = {"field": (2708.9e6 + 16358.4e6) / 16777216,
                        "beamdown": (1104.4e6 + 3924.0e6) / 4e6}  # beam-down: id order
 
-# Kernels of one plain launch of n realisations: below 2^24 the realisation
-# kernel alone; from 2^24 on, per chunk of 2^24 realisations, the coherent
-# order's presort (count, scan, scatter) and the realisation kernel (every
-# bench scene samples fewer than 12288 primitives)
-SORT_MIN, SORT_CHUNK = 1 << 24, 1 << 24
+# Kernels of one plain launch of n realisations: below 6e6 the realisation
+# kernel alone; from 6e6 on, per chunk of at most 2^24 realisations, the
+# coherent order's presort (count, scan, scatter) and the realisation kernel
+# (every bench scene samples more than one and fewer than 12288 primitives)
+SORT_MIN, SORT_CHUNK = 6_000_000, 1 << 24
 
 
 def launches_per_plain_launch(n):
