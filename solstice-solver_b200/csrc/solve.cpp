@@ -230,6 +230,12 @@ struct TallyLayout {
 
 } /* namespace */
 
+/* The BVH builder values ssol_b200_options accepts */
+static bool builder_ok(int b)
+{
+  return b == SSOL_B200_BVH_AUTO || b == SSOL_B200_BVH_SAH || b == SSOL_B200_BVH_LBVH;
+}
+
 struct ssol_b200_plan {
   RefCount ref;
   ssol_device* dev = nullptr;
@@ -653,7 +659,7 @@ res_T ssolb_snapshot_create
   const ssol_b200_options opt = options ? *options : SSOL_B200_OPTIONS_DEFAULT;
   if(opt.precision != SSOL_B200_FP32 && opt.precision != SSOL_B200_FP64)
     return RES_BAD_ARG;
-  if(opt.bvh_leaf_size < 0) return RES_BAD_ARG;
+  if(opt.bvh_leaf_size < 0 || !builder_ok(opt.bvh_builder)) return RES_BAD_ARG;
   BvhBuildParams bp;
   bp.max_leaf = opt.bvh_leaf_size ? opt.bvh_leaf_size : 1;
   bp.threads = host_threads();
@@ -730,9 +736,7 @@ extern "C" res_T ssol_b200_plan_create
   if(opt.max_segments == 0) opt.max_segments = 1000000ull;
   if(opt.min_blocks_per_sm < 0 || opt.min_blocks_per_sm > 3) return RES_BAD_ARG;
   if(opt.min_blocks_per_sm == 0) opt.min_blocks_per_sm = default_min_blocks(opt.precision);
-  if(opt.bvh_builder != SSOL_B200_BVH_AUTO && opt.bvh_builder != SSOL_B200_BVH_SAH
-  && opt.bvh_builder != SSOL_B200_BVH_LBVH)
-    return RES_BAD_ARG;
+  if(!builder_ok(opt.bvh_builder)) return RES_BAD_ARG;
   /* a plan does not know how many realisations it will trace */
   if(opt.bvh_builder == SSOL_B200_BVH_AUTO) opt.bvh_builder = SSOL_B200_BVH_SAH;
   if(opt.bvh_builder == SSOL_B200_BVH_LBVH) opt.bvh_leaf_size = 1;
@@ -1410,7 +1414,7 @@ extern "C" res_T ssol_b200_batch_create
     return RES_BAD_ARG;
   if(opt.block_size < 0 || opt.block_size > 256 || opt.grid_blocks < 0
   || opt.waves < 0 || opt.bvh_leaf_size < 0 || opt.min_blocks_per_sm < 0
-  || opt.min_blocks_per_sm > 3)
+  || opt.min_blocks_per_sm > 3 || !builder_ok(opt.bvh_builder))
     return RES_BAD_ARG;
   if(opt.block_size == 0) opt.block_size = 256;
   if(opt.block_size % 32) return RES_BAD_ARG;
@@ -1712,7 +1716,7 @@ extern "C" res_T ssol_b200_batch_create_tracking
     return RES_BAD_ARG;
   if(opt.block_size < 0 || opt.block_size > 256 || opt.grid_blocks < 0
   || opt.waves < 0 || opt.bvh_leaf_size < 0 || opt.min_blocks_per_sm < 0
-  || opt.min_blocks_per_sm > 3)
+  || opt.min_blocks_per_sm > 3 || !builder_ok(opt.bvh_builder))
     return RES_BAD_ARG;
   if(opt.block_size == 0) opt.block_size = 256;
   if(opt.block_size % 32) return RES_BAD_ARG;

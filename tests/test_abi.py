@@ -97,6 +97,10 @@ def test_plan_option_checks(product):
     plan = C.c_void_p()
     for o in (P.options(bvh=7), P.options(bvh=-1), P.options(leaf=-1), P.options(precision=5)):
         assert product.raw("ssol_b200_plan_create", s.scn, C.byref(o), C.byref(plan)) == P.RES_BAD_ARG
+    scenes = (C.c_void_p * 1)(s.scn.value)
+    batch = C.c_void_p()
+    assert product.raw("ssol_b200_batch_create", scenes, 1, C.byref(P.options(bvh=7)),
+                       C.byref(batch)) == P.RES_BAD_ARG
     s.close()
 
 
