@@ -365,11 +365,14 @@ def run_b200(args):
     est = P.C.c_void_p()
     res = lib.raw("ssol_b200_plan_finish", plan, rng, merged_n, 0, sp, P.C.byref(est))
     e = P.Estimator(s, est, res)
-    st = e.stats()
     g = e.globals()
     lib.raw("ssol_b200_plan_ref_put", plan)
     total_paths = args.steps * n * world
     value = total_paths / (ms * 1e-3) / 1e6
+    # The work per path for the roofline model: the timed launches leave the
+    # work counters out (the library's default), one counted launch of the
+    # same plan shape, outside the timed region, gives them
+    st = counted_stats(lib, s, opt, n, args.seed + 99, sp)
 
     # e2e through the public API
     e2e_value, h2d, d2h = None, 0, 0
@@ -424,7 +427,8 @@ def run_b200(args):
     nsm = torch.cuda.get_device_properties(local).multi_processor_count
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
     fp32_peak = nsm * 128 * 2 * sm_mhz * 1e6 / 1e12
-    achieved = flops_per_run(st) / (kernel_ms * 1e-3) / 1e12 if kernel_ms > 0 else 0.0
+    achieved = (flops_per_run(st) / max(1, st["paths"]) * args.steps * n
+                / (kernel_ms * 1e-3) / 1e12 if kernel_ms > 0 else 0.0)
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -454,6 +458,9 @@ def run_b200(args):
                                     "(MEASURED_PEAKS.json sm_max_mhz)",
                      "work_model": "20/slab x2 per node + 55/triangle + 90/quadric + "
                                    "150/bounce + 120/path (counted on device)",
+                     "counters_source": "one counted launch of paths_per_step paths "
+                                        "outside the timed region (the timed launches "
+                                        "run the kernel variant without work counters)",
                      "counters_per_path": {k: st[k] / max(1, st["paths"]) for k in
                                            ("rays", "node_visits", "triangle_tests",
                                             "quadric_tests", "bounces")},
@@ -526,19 +533,39 @@ def run_b200(args):
 BVH_CHOICES = {"auto": 0, "sah": 1, "lbvh": 2}
 
 
+def counted_stats(lib, s, opt, n, seed, sp):
+    """Stats of one launch of n paths with the work counters on, with the
+    launch shape and builder of `opt`."""
+    import pyssol as P
+    o = P.options(opt.precision, block_size=opt.block_size, waves=opt.waves,
+                  leaf=opt.bvh_leaf_size, min_blocks=opt.min_blocks_per_sm,
+                  bvh=opt.bvh_builder, count=1)
+    plan = P.C.c_void_p()
+    lib.call("ssol_b200_plan_create", s.scn, P.C.byref(o), P.C.byref(plan))
+    rng = s.rng(seed=seed)
+    lib.call("ssol_b200_plan_launch", plan, rng, 0, n, sp)
+    est = P.C.c_void_p()
+    res = lib.raw("ssol_b200_plan_finish", plan, rng, n, 0, sp, P.C.byref(est))
+    st = P.Estimator(s, est, res).stats()
+    lib.raw("ssol_b200_plan_ref_put", plan)
+    return st
+
+
 def bvh_builders(lib, s, opt, n, stream, sp, flush):
     """The two BVH builders on this scene, outside the timed region: plan
     creation wall time (snapshot, tree, upload; median of 3), device
     Mpaths/s of 2 launches of n paths after 1 warm-up (CUDA events, L2
-    flushed between launches), node visits per path and tree depth, and an
-    ssol_solve_ex of 1e6 paths end to end (median of 5), where the build is a
-    large part of the call."""
+    flushed between launches; the kernel variant with work counters, for the
+    node visits per path), the tree's depth, and an ssol_solve_ex of 1e6
+    paths end to end (median of 5), where the build is a large part of the
+    call."""
     import torch
     import pyssol as P
     out = {}
     for name, b in (("sah_host", P.BVH_SAH), ("lbvh_device", P.BVH_LBVH)):
         o = P.options(opt.precision, block_size=opt.block_size, waves=opt.waves,
-                      leaf=opt.bvh_leaf_size, min_blocks=opt.min_blocks_per_sm, bvh=b)
+                      leaf=opt.bvh_leaf_size, min_blocks=opt.min_blocks_per_sm, bvh=b,
+                      count=1)
         create = []
         for k in range(3):
             plan = P.C.c_void_p()

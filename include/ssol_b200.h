@@ -62,16 +62,24 @@ struct ssol_b200_options {
   int min_blocks_per_sm; /* register budget of the kernel variant: 1, 2, 3;
                           * 0 => 3 in FP32, 2 in FP64 */
   enum ssol_b200_bvh_builder bvh_builder; /* plans and ssol_solve_ex */
+  /* Nonzero: count rays, BVH node visits and primitive tests into the stats
+   * (ssol_b200_stats rays .. quadric_tests). 0 (the default): leave them out
+   * of the FP32 kernel, which is about 2 % faster without them; they then
+   * read 0. The FP64 build, path tracking, batches, the adjoint and the
+   * renderers always count. */
+  int count_work;
 };
-#define SSOL_B200_OPTIONS_DEFAULT__ { SSOL_B200_FP32, 256, 0, 1, 0, 0, 0, SSOL_B200_BVH_AUTO }
+#define SSOL_B200_OPTIONS_DEFAULT__ { SSOL_B200_FP32, 256, 0, 1, 0, 0, 0, SSOL_B200_BVH_AUTO, 0 }
 static const struct ssol_b200_options SSOL_B200_OPTIONS_DEFAULT =
   SSOL_B200_OPTIONS_DEFAULT__;
 
 /* Device work of the last solve (or of a plan's launches since its reset) */
 struct ssol_b200_stats {
   double kernel_ms; /* CUDA-event time of the realisation launches */
-  unsigned long long rays; /* rays cast (shadow + scattered) */
-  unsigned long long node_visits; /* BVH nodes fetched */
+  /* rays cast (shadow + scattered), BVH nodes fetched, triangle and quadric
+   * tests: counted when the options ask for it (count_work) */
+  unsigned long long rays;
+  unsigned long long node_visits;
   unsigned long long triangle_tests;
   unsigned long long quadric_tests;
   unsigned long long bounces; /* surface interactions that were shaded */

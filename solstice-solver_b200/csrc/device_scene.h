@@ -195,7 +195,10 @@ enum : int32_t {
   FEAT_QUADRIC = 1, /* punched quadric patches */
   FEAT_DIELECTRIC = 2, /* dielectric or thin-dielectric materials */
   FEAT_ATTRIBUTES = 4, /* per-triangle shading attributes (DScene::tshade) */
-  FEAT_ALL = 7
+  FEAT_ALL = 7,
+  /* Not a scene feature: the plain kernel variant that does not count rays,
+   * node visits and primitive tests (one instruction per node visit) */
+  FEAT_NOCOUNT = 8
 };
 
 /* Counters for the roofline model (see kernels_device.cuh) */

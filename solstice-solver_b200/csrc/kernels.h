@@ -31,6 +31,10 @@ struct LaunchConfig {
   /* FEAT_* bits the scene needs; the launch picks the smallest variant
    * that covers them */
   int features = FEAT_ALL;
+  /* Count rays, node visits and primitive tests into DTallies::stats (FP32
+   * plain launches without tracking can leave them out; the others always
+   * count) */
+  bool count_work = true;
 };
 
 /* Enqueue the realisations [first, first + count) of the stream keyed by
@@ -45,6 +49,11 @@ int launch_realisations_f64
   (const DScene<double>& S, const DTallies& T, uint64_t seed, uint64_t first,
    uint64_t count, const LaunchConfig& cfg, void* stream,
    const DTrack* track = nullptr);
+/* The FP32 variants without work counters (kernels_plain_nc.cu), which
+ * launch_realisations_f32 calls when cfg.count_work is false */
+int launch_realisations_nocount_f32
+  (const DScene<float>& S, const DTallies& T, uint64_t seed, uint64_t first,
+   uint64_t count, const LaunchConfig& cfg, void* stream);
 
 /* Batched launch: device arrays of per-item scenes and tallies, the item
  * budgets as an inclusive prefix (nitems + 1 entries; the last one is the

@@ -652,7 +652,7 @@ __device__ bool trace_ray
   (const DScene<R>& S, V3<R> o, V3<R> d, R tmin, const SelfInfo& self,
    bool any, Hit<R>& best, Counters& cnt, int* stack, int stride)
 {
-  ++cnt.rays;
+  if(!(FEAT & FEAT_NOCOUNT)) ++cnt.rays;
   /* A zero direction component would make lo * inv - o * inv an inf - inf
    * NaN for boxes the ray runs parallel to; clamp it to +-2^-64 so that the
    * FMA form of the slab test stays finite (Aila and Laine, HPG 2009) */
@@ -673,7 +673,7 @@ __device__ bool trace_ray
   int node = 0;
   for(;;) {
     const DNode<R> N = load_node(S.nodes + node);
-    ++cnt.nodes;
+    if(!(FEAT & FEAT_NOCOUNT)) ++cnt.nodes;
     R te[2];
     bool h[2];
     h[0] = slab(N.lo[0], N.hi[0], inv, oinv, tmin, best.t, te[0])
@@ -692,11 +692,11 @@ __device__ bool trace_ray
       for(int p = 0; p < lc; ++p) {
         const uint32_t ref = lc == 1 ? (uint32_t)first : S.primrefs[first + p];
         if(!(FEAT & FEAT_QUADRIC) || primref_kind(ref) == PRIM_TRIANGLE) {
-          ++cnt.tris;
+          if(!(FEAT & FEAT_NOCOUNT)) ++cnt.tris;
           test_triangle(S, (int)primref_index(ref), o, d, sh, tmin, eps,
                         self, best, found);
         } else {
-          ++cnt.quads;
+          if(!(FEAT & FEAT_NOCOUNT)) ++cnt.quads;
           test_quadric(S, (int)primref_index(ref), o, d, tmin, self,
                        best, found);
         }
@@ -2296,7 +2296,7 @@ static int launch_variant
 /* Feature variants of the FP32 kernel: meshes with mirror and matte
  * materials only, quadrics and dielectrics, or everything (vertex
  * attributes); the all-FP64 build, for precision checks, has the last one */
-template<class R, int MINB>
+template<class R, int MINB, int NC>
 static int launch_features
   (const DScene<R>& S, const DTallies& T, uint64_t seed, uint64_t first,
    uint64_t count, const LaunchConfig& cfg, void* stream)
@@ -2304,16 +2304,19 @@ static int launch_features
   const DTrack none = {};
   if constexpr(sizeof(R) == sizeof(float)) {
     if(cfg.features == 0)
-      return launch_variant<R, MINB, false, 0>(S, T, seed, first, count, cfg, stream, none);
+      return launch_variant<R, MINB, false, NC>(S, T, seed, first, count, cfg, stream, none);
     if(!(cfg.features & FEAT_ATTRIBUTES))
-      return launch_variant<R, MINB, false, FEAT_QUADRIC | FEAT_DIELECTRIC>
+      return launch_variant<R, MINB, false, FEAT_QUADRIC | FEAT_DIELECTRIC | NC>
         (S, T, seed, first, count, cfg, stream, none);
   }
-  return launch_variant<R, MINB, false, FEAT_ALL>(S, T, seed, first, count, cfg, stream, none);
+  return launch_variant<R, MINB, false, FEAT_ALL | NC>(S, T, seed, first, count, cfg, stream,
+                                                       none);
 }
 
-/* Register budget variants: at least MINB blocks of 256 threads per SM */
-template<class R>
+/* Register budget variants: at least MINB blocks of 256 threads per SM; NC
+ * is FEAT_NOCOUNT for the variants without work counters (path tracking
+ * always counts) */
+template<class R, int NC = 0>
 static int launch_impl
   (const DScene<R>& S, const DTallies& T, uint64_t seed, uint64_t first,
    uint64_t count, const LaunchConfig& cfg, void* stream, const DTrack* track)
@@ -2321,9 +2324,9 @@ static int launch_impl
   if(track)
     return launch_variant<R, 2, true, FEAT_ALL>(S, T, seed, first, count, cfg, stream, *track);
   switch(cfg.min_blocks) {
-    case 1: return launch_features<R, 1>(S, T, seed, first, count, cfg, stream);
-    case 3: return launch_features<R, 3>(S, T, seed, first, count, cfg, stream);
-    default: return launch_features<R, 2>(S, T, seed, first, count, cfg, stream);
+    case 1: return launch_features<R, 1, NC>(S, T, seed, first, count, cfg, stream);
+    case 3: return launch_features<R, 3, NC>(S, T, seed, first, count, cfg, stream);
+    default: return launch_features<R, 2, NC>(S, T, seed, first, count, cfg, stream);
   }
 }
 

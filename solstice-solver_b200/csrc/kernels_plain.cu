@@ -33,7 +33,11 @@ cudaMemPool_t sort_pool(int dev)
 int launch_realisations_f32
   (const DScene<float>& S, const DTallies& T, uint64_t seed, uint64_t first,
    uint64_t count, const LaunchConfig& cfg, void* stream, const DTrack* track)
-{ return launch_impl<float>(S, T, seed, first, count, cfg, stream, track); }
+{
+  if(!track && !cfg.count_work)
+    return launch_realisations_nocount_f32(S, T, seed, first, count, cfg, stream);
+  return launch_impl<float>(S, T, seed, first, count, cfg, stream, track);
+}
 
 
 } /* namespace ssolb */

@@ -893,6 +893,7 @@ static res_T plan_launch
   cfg.max_failed = max_failed;
   cfg.abortable = true;
   cfg.features = p->meta.features;
+  cfg.count_work = p->opt.count_work != 0;
   const uint64_t start = rng->position + first;
   cudaEventRecord(p->ev0, s);
   const int err = p->opt.precision == SSOL_B200_FP32

@@ -156,7 +156,7 @@ class B200Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("block_size", C.c_int), ("grid_blocks", C.c_int),
                 ("waves", C.c_int), ("bvh_leaf_size", C.c_int),
                 ("max_segments", C.c_ulonglong), ("min_blocks_per_sm", C.c_int),
-                ("bvh_builder", C.c_int)]
+                ("bvh_builder", C.c_int), ("count_work", C.c_int)]
 
 
 BVH_AUTO, BVH_SAH, BVH_LBVH = 0, 1, 2
@@ -933,7 +933,7 @@ def estimator_from_tallies(scene, rng, n, sums, counts, max_failed=0):
 
 
 def options(precision=FP32, block_size=256, grid_blocks=0, waves=1, leaf=0,
-            max_segments=0, min_blocks=0, bvh=BVH_AUTO):
+            max_segments=0, min_blocks=0, bvh=BVH_AUTO, count=0):
     o = B200Options()
     o.precision = precision
     o.block_size = block_size
@@ -943,6 +943,7 @@ def options(precision=FP32, block_size=256, grid_blocks=0, waves=1, leaf=0,
     o.max_segments = max_segments
     o.min_blocks_per_sm = min_blocks
     o.bvh_builder = bvh
+    o.count_work = count
     return o
 
 

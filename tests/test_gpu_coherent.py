@@ -17,7 +17,7 @@ CHUNK = 1 << 24
 
 
 def _run(lib, s, launches, nreal):
-    opt = P.options(P.FP32)
+    opt = P.options(P.FP32, count=1)
     plan = C.c_void_p()
     lib.call("ssol_b200_plan_create", s.scn, C.byref(opt), C.byref(plan))
     try:

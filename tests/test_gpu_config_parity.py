@@ -107,7 +107,7 @@ def test_config4_beam_down_vs_oracle(product, oracle):
     n = 4_000_000
     sg, hg = W.beam_down(product)
     sc, hc = W.beam_down(oracle)
-    eg, ec = sg.solve(n, seed=4), sc.solve(n, seed=4)
+    eg, ec = sg.solve(n, seed=4, options=P.options(count=1)), sc.solve(n, seed=4)
     assert eg.count("realisation_count") == ec.count("realisation_count") == n
     assert eg.count("failed_count") == ec.count("failed_count")
     assert_dict_close(eg.globals(), ec.globals(), "globals")

@@ -23,8 +23,9 @@ def _same(a, b, what, rel=1e-10):
 
 
 def _solve_pair(s, n, seed, precision=P.FP32):
-    sah = s.solve(n, seed=seed, options=P.options(precision=precision, bvh=P.BVH_SAH))
-    lbvh = s.solve(n, seed=seed, options=P.options(precision=precision, bvh=P.BVH_LBVH))
+    sah = s.solve(n, seed=seed, options=P.options(precision=precision, bvh=P.BVH_SAH, count=1))
+    lbvh = s.solve(n, seed=seed, options=P.options(precision=precision, bvh=P.BVH_LBVH,
+                                                   count=1))
     return sah, lbvh
 
 
@@ -133,4 +134,21 @@ def test_default_builder_by_solve_size(product):
     product.call("ssol_b200_plan_get_stats", plan, C.byref(st))
     assert st.bvh_device == 0 and st.bvh_nodes >= 1
     product.call("ssol_b200_plan_ref_put", plan)
+    s.close()
+
+
+def test_work_counters_are_optional(product):
+    """FP32 solves count rays, node visits and primitive tests only when the
+    options ask for it; the estimates are the same either way, and so are
+    the counters that are always kept (paths, bounces)."""
+    s, h = W.heliostat_field(product, n_helio=200, receiver_cells=16)
+    off = s.solve(2_000_000, seed=6)
+    on = s.solve(2_000_000, seed=6, options=P.options(count=1))
+    so, sn = off.stats(), on.stats()
+    for k in ("rays", "node_visits", "triangle_tests", "quadric_tests"):
+        assert so[k] == 0, k
+    assert sn["rays"] > 0 and sn["node_visits"] > sn["rays"] and sn["triangle_tests"] > 0
+    assert so["paths"] == sn["paths"] == 2_000_000 and so["bounces"] == sn["bounces"]
+    _same(off.globals(), on.globals(), "globals")
+    _same(off.receiver(h["receiver"]), on.receiver(h["receiver"]), "receiver")
     s.close()
