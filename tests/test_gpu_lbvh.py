@@ -53,13 +53,18 @@ def test_lbvh_full_field_equals_sah(product):
 def test_lbvh_beam_down_equals_sah(product):
     """Beam-down scene: 5000 punched paraboloids, a hyperboloid, the glass
     window and the receiver grid (quadric patches in the device build), 1e6
-    paths with the roulette."""
+    paths with the roulette in FP32, 2e5 in FP64."""
     s, h = W.beam_down(product)
     sah, lbvh = _solve_pair(s, 1_000_000, seed=9)
     assert lbvh.stats()["bvh_device"] == 1
     assert lbvh.stats()["killed"] == sah.stats()["killed"]
     _same(lbvh.globals(), sah.globals(), "globals")
     _same(lbvh.receiver(h["receiver"]), sah.receiver(h["receiver"]), "receiver")
+    # the FP64 build's device tree (boxes and Morton codes in FP64)
+    sah, lbvh = _solve_pair(s, 200_000, seed=10, precision=P.FP64)
+    assert lbvh.stats()["bvh_device"] == 1
+    _same(lbvh.globals(), sah.globals(), "fp64 globals")
+    _same(lbvh.receiver(h["receiver"]), sah.receiver(h["receiver"]), "fp64 receiver")
     s.close()
 
 
