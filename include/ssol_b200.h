@@ -64,9 +64,10 @@ struct ssol_b200_options {
   enum ssol_b200_bvh_builder bvh_builder; /* plans and ssol_solve_ex */
   /* Nonzero: count rays, BVH node visits and primitive tests into the stats
    * (ssol_b200_stats rays .. quadric_tests). 0 (the default): leave them out
-   * of the FP32 kernel, which is about 2 % faster without them; they then
-   * read 0. The FP64 build, path tracking, batches, the adjoint and the
-   * renderers always count. */
+   * of the FP32 plain and batched kernels, which are about 1-2 % faster
+   * without them; they then read 0. The FP64 build, path tracking, the
+   * no-allocation batched launch, the adjoint and the renderers always
+   * count. */
   int count_work;
 };
 #define SSOL_B200_OPTIONS_DEFAULT__ { SSOL_B200_FP32, 256, 0, 1, 0, 0, 0, SSOL_B200_BVH_AUTO, 0 }

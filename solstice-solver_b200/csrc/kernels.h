@@ -31,9 +31,9 @@ struct LaunchConfig {
   /* FEAT_* bits the scene needs; the launch picks the smallest variant
    * that covers them */
   int features = FEAT_ALL;
-  /* Count rays, node visits and primitive tests into DTallies::stats (FP32
-   * plain launches without tracking can leave them out; the others always
-   * count) */
+  /* Count rays, node visits and primitive tests into the launch's stats
+   * (FP32 plain launches without tracking and FP32 batched launches can
+   * leave them out; the others always count) */
   bool count_work = true;
 };
 
@@ -92,6 +92,10 @@ template<class R> struct BatchLaunch {
 
 int launch_batch_f32(const BatchLaunch<float>& b, const LaunchConfig& cfg,
                      void* stream);
+/* The FP32 batched variants without work counters (kernels_batch_nc.cu),
+ * which launch_batch_f32 calls when cfg.count_work is false */
+int launch_batch_nocount_f32(const BatchLaunch<float>& b, const LaunchConfig& cfg,
+                             void* stream);
 
 /* Largest item count of the no-allocation batched launch: its scratch is a
  * static device array sized for this many items */

@@ -8,7 +8,10 @@ namespace ssolb {
 
 int launch_batch_f32(const BatchLaunch<float>& b, const LaunchConfig& cfg,
                      void* stream)
-{ return launch_batch_impl<float>(b, cfg, stream); }
+{
+  if(!cfg.count_work) return launch_batch_nocount_f32(b, cfg, stream);
+  return launch_batch_impl<float>(b, cfg, stream);
+}
 
 int launch_batch_f64(const BatchLaunch<double>& b, const LaunchConfig& cfg,
                      void* stream)

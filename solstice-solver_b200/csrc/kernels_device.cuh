@@ -2372,7 +2372,8 @@ static int launch_batch_variant(const BatchLaunch<R>& b, const LaunchConfig& cfg
   return (int)cudaGetLastError();
 }
 
-template<class R>
+/* NC is FEAT_NOCOUNT for the variants without work counters */
+template<class R, int NC = 0>
 static int launch_batch_impl(const BatchLaunch<R>& b, const LaunchConfig& cfg,
                              void* stream)
 {
@@ -2380,15 +2381,15 @@ static int launch_batch_impl(const BatchLaunch<R>& b, const LaunchConfig& cfg,
    * smaller variant */
   if(sizeof(R) == sizeof(float) && cfg.features == 0) {
     switch(cfg.min_blocks) {
-      case 1: return launch_batch_variant<R, 1, 0>(b, cfg, stream);
-      case 3: return launch_batch_variant<R, 3, 0>(b, cfg, stream);
-      default: return launch_batch_variant<R, 2, 0>(b, cfg, stream);
+      case 1: return launch_batch_variant<R, 1, NC>(b, cfg, stream);
+      case 3: return launch_batch_variant<R, 3, NC>(b, cfg, stream);
+      default: return launch_batch_variant<R, 2, NC>(b, cfg, stream);
     }
   }
   switch(cfg.min_blocks) {
-    case 1: return launch_batch_variant<R, 1, FEAT_ALL>(b, cfg, stream);
-    case 3: return launch_batch_variant<R, 3, FEAT_ALL>(b, cfg, stream);
-    default: return launch_batch_variant<R, 2, FEAT_ALL>(b, cfg, stream);
+    case 1: return launch_batch_variant<R, 1, FEAT_ALL | NC>(b, cfg, stream);
+    case 3: return launch_batch_variant<R, 3, FEAT_ALL | NC>(b, cfg, stream);
+    default: return launch_batch_variant<R, 2, FEAT_ALL | NC>(b, cfg, stream);
   }
 }
 

@@ -1821,6 +1821,7 @@ static LaunchConfig batch_config(const ssol_b200_batch* b)
   cfg.waves = b->opt.waves;
   cfg.max_segments = b->opt.max_segments;
   cfg.min_blocks = b->opt.min_blocks_per_sm;
+  cfg.count_work = b->opt.count_work != 0;
   size_t nrcv = 0;
   cfg.features = 0;
   for(const FlatMeta& m : b->meta) {
