@@ -39,12 +39,12 @@ WORKLOAD = ("1000 flat 10x10 heliostats (radial staggered, r 100-600 m, Beckmann
 
 
 # DRAM bytes per path of the realisation kernel, from ncu captures of launches
-# of the same scenes (field: one sorted chunk of 2^24 paths at 3 blocks per SM,
-# the variant without work counters; beam-down: 4e6 paths, with counters)
+# of the same scenes, the variants without work counters (field: one sorted
+# chunk of 2^24 paths at 3 blocks per SM; beam-down: 4e6 paths)
 # (dram__bytes_read.sum + dram__bytes_write.sum);
 # the traffic scales with the paths traced (per-thread frames written back)
 DRAM_BYTES_PER_PATH = {"field": (2202.1e6 + 15599.4e6) / 16777216,
-                       "beamdown": (1104.4e6 + 3924.0e6) / 4e6}  # beam-down: id order
+                       "beamdown": (892.0e6 + 3562.1e6) / 4e6}  # beam-down: id order
 
 # Kernels of one plain launch of n realisations: below 6e6 the realisation
 # kernel alone; from 6e6 on, per chunk of at most 2^24 realisations, the
