@@ -1229,8 +1229,11 @@ extern "C" res_T ssol_b200_plan_get_tallies
  * primitive ranges): what gives a tally block its layout */
 static res_T scene_meta(ssol_scene* scn, FlatMeta& meta, TallyLayout& tl)
 {
+  /* the slots only: no tree is built (the device builder's snapshot keeps
+   * the primitive boxes and builds nothing on the host) */
   BvhBuildParams bp;
   bp.threads = host_threads();
+  bp.device = true;
   FlatScene<float> f;
   res_T res = flatten_scene(scn, bp, f);
   if(res != RES_OK) return res;
