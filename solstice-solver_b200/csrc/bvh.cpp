@@ -7,7 +7,6 @@
 
 #include <algorithm>
 #include <array>
-#include <atomic>
 #include <thread>
 #include <cmath>
 #include <limits>
@@ -220,19 +219,13 @@ struct Builder {
   }
 };
 
-/* Expands tasks top down. Ranges smaller than `defer_below` (when > 0) are
- * not expanded but returned in `deferred`, still to be built. */
+/* Expands tasks top down on the calling thread */
 void run_tasks(std::vector<PrimBox>& prims, std::vector<std::array<double, 3>>& cent,
-               const BvhBuildParams& prm, Builder& B, std::vector<Task> stack,
-               int defer_below, std::vector<Task>* deferred)
+               const BvhBuildParams& prm, Builder& B, std::vector<Task> stack)
 {
   while(!stack.empty()) {
     const Task t = stack.back();
     stack.pop_back();
-    if(defer_below > 0 && t.end - t.begin < defer_below) {
-      deferred->push_back(t);
-      continue;
-    }
     B.depth = std::max(B.depth, t.depth + 1);
     const Box b = bounds(prims, t.begin, t.end);
     const int s = split(prims, cent, t.begin, t.end, prm, t.depth);
@@ -247,6 +240,84 @@ void run_tasks(std::vector<PrimBox>& prims, std::vector<std::array<double, 3>>& 
       stack.push_back({s, t.end, id, 1, t.depth + 1});
     }
   }
+}
+
+/* Ranges below this many primitives are built by one thread */
+constexpr int PAR_MIN = 1024;
+
+/* Threads for the part of `nsub` primitives out of `n`: in proportion, at
+ * least 1, leaving at least 1 for the rest */
+int share(int threads, int nsub, int n)
+{
+  const int t = (int)((long long)threads * nsub / n);
+  return std::min(std::max(t, 1), threads - 1);
+}
+
+/* Append builder L's tree to B: L's node 0 stands for B's slot (node,
+ * slot), L's node j > 0 becomes a new node of B, and L's leaf references
+ * move by the references B already holds */
+void merge_into(Builder& B, const Builder& L, int node, int slot)
+{
+  const int base = (int)(B.child.size() / 2);
+  const int ref_base = (int)B.refs.size();
+  const size_t nl = L.child.size() / 2;
+  auto fix = [&](int c, int cnt) { return cnt == 0 ? c - 1 + base : cnt > 0 ? c + ref_base : c; };
+  /* L's nodes 1.. in bulk: boxes and counts as they are, children moved */
+  B.lo.insert(B.lo.end(), L.lo.begin() + 6, L.lo.end());
+  B.hi.insert(B.hi.end(), L.hi.begin() + 6, L.hi.end());
+  B.count.insert(B.count.end(), L.count.begin() + 2, L.count.end());
+  B.child.reserve(B.child.size() + 2 * (nl - 1));
+  for(size_t ls = 2; ls < 2 * nl; ++ls) B.child.push_back(fix(L.child[ls], L.count[ls]));
+  const size_t ps = (size_t)node * 2 + slot;
+  for(int c = 0; c < 3; ++c) {
+    B.lo[ps * 3 + c] = L.lo[c];
+    B.hi[ps * 3 + c] = L.hi[c];
+  }
+  B.count[ps] = L.count[0];
+  B.child[ps] = fix(L.child[0], L.count[0]);
+  B.refs.insert(B.refs.end(), L.refs.begin(), L.refs.end());
+  B.depth = std::max(B.depth, L.depth);
+}
+
+/* The tree of task t (absolute depth t.depth) in a builder of its own whose
+ * node 0 stands for the task's parent slot. A range of at least PAR_MIN
+ * primitives with 2 or more threads is split here, and its two halves are
+ * built at once on two threads that share `threads` in proportion to their
+ * sizes; the rest is built top down by one thread. Ranges are disjoint, so
+ * the threads partition the shared arrays without overlap. */
+Builder build_sub(std::vector<PrimBox>& prims, std::vector<std::array<double, 3>>& cent,
+                  const BvhBuildParams& prm, const Task& t, int threads)
+{
+  Builder L;
+  L.new_node();
+  Task tt = t;
+  tt.node = 0;
+  tt.slot = 0;
+  const int n = t.end - t.begin;
+  if(threads < 2 || n < PAR_MIN) {
+    run_tasks(prims, cent, prm, L, {tt});
+    return L;
+  }
+  L.depth = std::max(L.depth, t.depth + 1);
+  const Box b = bounds(prims, t.begin, t.end);
+  const int s = split(prims, cent, t.begin, t.end, prm, t.depth);
+  if(s < 0) {
+    const int first = (int)L.refs.size();
+    for(int i = t.begin; i < t.end; ++i) L.refs.push_back(prims[i].ref);
+    L.set_slot(0, b, first, n);
+    return L;
+  }
+  const int id = L.new_node();
+  L.set_slot(0, b, id, 0);
+  const Task tl = {t.begin, s, id, 0, t.depth + 1}, tr = {s, t.end, id, 1, t.depth + 1};
+  const int thl = share(threads, s - t.begin, n);
+  Builder right;
+  std::thread th([&] { right = build_sub(prims, cent, prm, tr, threads - thl); });
+  Builder left = build_sub(prims, cent, prm, tl, thl);
+  th.join();
+  merge_into(L, left, id, 0);
+  merge_into(L, right, id, 1);
+  return L;
 }
 
 } /* namespace */
@@ -284,64 +355,20 @@ void build_bvh(std::vector<PrimBox> prims, const BvhBuildParams& prm,
     B.set_slot(root * 2 + 1, empty, 0, -1);
     B.depth = 1;
   } else {
-    std::vector<Task> stack = {{0, m, root, 0, 1}, {m, n, root, 1, 1}};
+    const Task t0 = {0, m, root, 0, 1}, t1 = {m, n, root, 1, 1};
     const int threads = std::max(1, prm.threads);
-    if(threads == 1 || n < 4096) {
-      run_tasks(prims, cent, prm, B, stack, 0, nullptr);
+    if(threads == 1 || n < PAR_MIN) {
+      run_tasks(prims, cent, prm, B, {t0, t1});
     } else {
-      /* Top levels here, then the subtrees below n / (4 x threads)
-       * primitives on the threads, each into its own builder whose node 0
-       * stands for the parent slot; the splits are the same, so is the tree */
-      std::vector<Task> deferred;
-      run_tasks(prims, cent, prm, B, stack, std::max(512, n / (4 * threads)), &deferred);
-      std::vector<Builder> sub(deferred.size());
-      std::atomic<size_t> next{0};
-      auto work = [&]() {
-        for(size_t i = next.fetch_add(1); i < deferred.size(); i = next.fetch_add(1)) {
-          Builder& L = sub[i];
-          L.new_node();
-          Task t = deferred[i];
-          t.node = 0;
-          t.slot = 0;
-          run_tasks(prims, cent, prm, L, {t}, 0, nullptr);
-        }
-      };
-      std::vector<std::thread> pool;
-      const size_t nt = std::min<size_t>((size_t)threads, deferred.size());
-      for(size_t k = 1; k < nt; ++k) pool.emplace_back(work);
-      work();
-      for(std::thread& th : pool) th.join();
-      /* Merge in the order the tasks were deferred: local node j > 0 becomes
-       * base + j - 1, local leaf refs move by the refs already merged */
-      for(size_t i = 0; i < deferred.size(); ++i) {
-        const Builder& L = sub[i];
-        const int base = (int)(B.child.size() / 2);
-        const int ref_base = (int)B.refs.size();
-        const int nl = (int)(L.child.size() / 2);
-        auto fix = [&](int c, int cnt) { return cnt == 0 ? c - 1 + base : cnt > 0 ? c + ref_base : c; };
-        for(int j = 1; j < nl; ++j) {
-          const int id = B.new_node();
-          for(int k = 0; k < 2; ++k) {
-            const size_t ls = (size_t)j * 2 + k, gs = (size_t)id * 2 + k;
-            for(int c = 0; c < 3; ++c) {
-              B.lo[gs * 3 + c] = L.lo[ls * 3 + c];
-              B.hi[gs * 3 + c] = L.hi[ls * 3 + c];
-            }
-            B.count[gs] = L.count[ls];
-            B.child[gs] = fix(L.child[ls], L.count[ls]);
-          }
-        }
-        const Task& t = deferred[i];
-        const size_t ps = (size_t)t.node * 2 + t.slot;
-        for(int c = 0; c < 3; ++c) {
-          B.lo[ps * 3 + c] = L.lo[c];
-          B.hi[ps * 3 + c] = L.hi[c];
-        }
-        B.count[ps] = L.count[0];
-        B.child[ps] = fix(L.child[0], L.count[0]);
-        B.refs.insert(B.refs.end(), L.refs.begin(), L.refs.end());
-        B.depth = std::max(B.depth, L.depth);
-      }
+      /* The two halves on two threads, each splitting its thread share
+       * further (build_sub); the splits are the same, so is the tree */
+      const int th0 = share(threads, m, n);
+      Builder r1;
+      std::thread th([&] { r1 = build_sub(prims, cent, prm, t1, threads - th0); });
+      Builder r0 = build_sub(prims, cent, prm, t0, th0);
+      th.join();
+      merge_into(B, r0, root, 0);
+      merge_into(B, r1, root, 1);
     }
   }
   out.lo = std::move(B.lo);
