@@ -257,6 +257,12 @@ struct ssol_b200_plan {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double kernel_ms = 0;
   bool timing_valid = false;
+  /* The snapshot of a device-built tree, kept for a host SAH tree built
+   * while the first realisations run (plan_swap_sah), and that tree */
+  std::unique_ptr<FlatScene<float>> keep32;
+  std::unique_ptr<FlatScene<double>> keep64;
+  void* d_bvh2 = nullptr;
+  size_t bvh2_alloc = 0;
 };
 
 /* Default register budget: 3 blocks of 256 threads per SM (80 registers) in
@@ -698,6 +704,7 @@ static void plan_release(ssol_b200_plan* p)
 {
   dev_free(p->dev, p->d_scene, p->scene_alloc);
   dev_free(p->dev, p->d_tally, p->tl.total);
+  dev_free(p->dev, p->d_bvh2, p->bvh2_alloc);
   if(p->ev0) cudaEventDestroy(p->ev0);
   if(p->ev1) cudaEventDestroy(p->ev1);
   if(p->scn) ssol_scene_ref_put(p->scn);
@@ -720,8 +727,11 @@ extern "C" res_T ssol_b200_plan_ref_put(ssol_b200_plan* p)
   return RES_OK;
 }
 
-extern "C" res_T ssol_b200_plan_create
-  (ssol_scene* scn, const ssol_b200_options* options, ssol_b200_plan** out)
+/* keep_flat: with a device-built tree, the plan keeps its snapshot for
+ * plan_swap_sah */
+static res_T plan_create_impl
+  (ssol_scene* scn, const ssol_b200_options* options, ssol_b200_plan** out,
+   bool keep_flat)
 {
   if(!scn || !out) return RES_BAD_ARG;
   ssol_b200_options opt = options ? *options : SSOL_B200_OPTIONS_DEFAULT;
@@ -804,8 +814,18 @@ extern "C" res_T ssol_b200_plan_create
   p->t = bind_tallies(p->tl, (unsigned char*)p->d_tally);
   cudaEventCreate(&p->ev0);
   cudaEventCreate(&p->ev1);
+  if(keep_flat && p->bvh_device) {
+    p->keep32 = std::move(f32);
+    p->keep64 = std::move(f64);
+  }
   *out = p;
   return ssol_b200_plan_reset(p, nullptr);
+}
+
+extern "C" res_T ssol_b200_plan_create
+  (ssol_scene* scn, const ssol_b200_options* options, ssol_b200_plan** out)
+{
+  return plan_create_impl(scn, options, out, false);
 }
 
 static cudaStream_t plan_stream(ssol_b200_plan* p, void* stream)
@@ -876,10 +896,12 @@ extern "C" res_T ssol_b200_plan_reset(ssol_b200_plan* p, void* stream)
   return RES_OK;
 }
 
+/* keep_start: the launch continues the previous one in the kernel timing
+ * (the start event is not recorded again) */
 static res_T plan_launch
   (ssol_b200_plan* p, const ssp_rng* rng, const uint64_t first,
    const uint64_t count, void* stream, const DTrack* track,
-   const unsigned long long max_failed = ~0ull)
+   const unsigned long long max_failed = ~0ull, bool keep_start = false)
 {
   if(!p || !rng) return RES_BAD_ARG;
   if(!count) return RES_OK;
@@ -895,7 +917,7 @@ static res_T plan_launch
   cfg.features = p->meta.features;
   cfg.count_work = p->opt.count_work != 0;
   const uint64_t start = rng->position + first;
-  cudaEventRecord(p->ev0, s);
+  if(!keep_start || !p->timing_valid) cudaEventRecord(p->ev0, s);
   const int err = p->opt.precision == SSOL_B200_FP32
     ? launch_realisations_f32(p->s32, p->t, rng->seed, start, count, cfg, s, track)
     : launch_realisations_f64(p->s64, p->t, rng->seed, start, count, cfg, s, track);
@@ -914,6 +936,63 @@ extern "C" res_T ssol_b200_plan_launch
    const uint64_t count, void* stream)
 {
   return plan_launch(p, rng, first, count, stream, nullptr);
+}
+
+/* Replace a plan's device-built tree by the host SAH tree of the same
+ * primitive boxes, built on the calling thread while the plan's launches
+ * already queued run on the device's tree. Both trees give the same closest
+ * hits, so later launches only trace faster. The new nodes go to a buffer
+ * of their own; launches take the scene by value, so the queued ones keep
+ * the old tree. No-op for a plan without a kept snapshot, or when the host
+ * tree would be too deep. */
+template<class R>
+static res_T swap_sah(ssol_b200_plan* p, const FlatScene<R>& f, DScene<R>& S)
+{
+  const size_t n = f.prim_ref.size();
+  std::vector<PrimBox> boxes(n);
+  for(size_t i = 0; i < n; ++i) {
+    for(int c = 0; c < 3; ++c) {
+      boxes[i].lo[c] = (double)f.prim_box[6 * i + c];
+      boxes[i].hi[c] = (double)f.prim_box[6 * i + 3 + c];
+    }
+    boxes[i].ref = f.prim_ref[i];
+  }
+  BvhBuildParams bp;
+  bp.max_leaf = 1;
+  bp.threads = host_threads();
+  BvhResult r;
+  build_bvh(std::move(boxes), bp, r);
+  if(r.depth > 30) return RES_OK;
+  const std::vector<DNode<R>> nodes = bvh_nodes<R>(r);
+  Blob b;
+  const size_t o_nodes = b.add(nodes);
+  const size_t o_refs = b.add(r.primrefs);
+  const size_t bytes = b.host.size() + 256;
+  if(dev_alloc(p->dev, &p->d_bvh2, bytes) != cudaSuccess) {
+    p->d_bvh2 = nullptr;
+    return RES_OK; /* keep tracing on the device's tree */
+  }
+  p->bvh2_alloc = bytes;
+  if(cudaMemcpyAsync(p->d_bvh2, b.host.data(), b.host.size(), cudaMemcpyHostToDevice,
+                     (cudaStream_t)p->dev->stream) != cudaSuccess)
+    return RES_UNKNOWN_ERR;
+  unsigned char* base = (unsigned char*)p->d_bvh2;
+  S.nodes = (const DNode<R>*)(base + o_nodes);
+  S.primrefs = (const uint32_t*)(base + o_refs);
+  p->bvh_device = false;
+  p->bvh_depth = r.depth;
+  p->bvh_nodes = nodes.size();
+  return RES_OK;
+}
+
+static res_T plan_swap_sah(ssol_b200_plan* p)
+{
+  res_T res = RES_OK;
+  if(p->keep32) res = swap_sah(p, *p->keep32, p->s32);
+  else if(p->keep64) res = swap_sah(p, *p->keep64, p->s64);
+  p->keep32.reset();
+  p->keep64.reset();
+  return res;
 }
 
 static void fill_sums(double dst[10][2], const double* src)
@@ -2117,14 +2196,30 @@ extern "C" res_T ssol_solve_ex
    * tree on the device saves more (2 ms on the 1000-heliostat field) than
    * its slightly slower traversal costs */
   ssol_b200_options opt = options ? *options : SSOL_B200_OPTIONS_DEFAULT;
+  /* The default builder by solve size. Larger solves start on the device's
+   * tree and switch to the host SAH tree, built meanwhile on the host
+   * threads, after their first 6e6 realisations (the smallest launch that
+   * runs in the coherent order, 8.5 ms on the 1000-heliostat field): the
+   * host build (2-3 ms there) no longer delays the first launch, and only
+   * that first part traces on the slower tree */
+  const bool hybrid = opt.bvh_builder == SSOL_B200_BVH_AUTO && !tracker
+    && (unsigned long long)n > SSOL_B200_BVH_AUTO_MAX_PATHS;
   if(opt.bvh_builder == SSOL_B200_BVH_AUTO)
-    opt.bvh_builder = (unsigned long long)n <= SSOL_B200_BVH_AUTO_MAX_PATHS
+    opt.bvh_builder = (unsigned long long)n <= SSOL_B200_BVH_AUTO_MAX_PATHS || hybrid
       ? SSOL_B200_BVH_LBVH : SSOL_B200_BVH_SAH;
   ssol_b200_plan* plan = nullptr;
-  res_T res = ssol_b200_plan_create(scn, &opt, &plan);
+  res_T res = plan_create_impl(scn, &opt, &plan, hybrid);
   if(res != RES_OK) return res;
   if(!tracker) {
-    res = plan_launch(plan, rng, 0, n, nullptr, nullptr, (unsigned long long)max_failed);
+    const unsigned long long mf = (unsigned long long)max_failed;
+    if(hybrid && (plan->keep32 || plan->keep64)) {
+      const uint64_t n0 = 6000000;
+      res = plan_launch(plan, rng, 0, n0, nullptr, nullptr, mf);
+      if(res == RES_OK) res = plan_swap_sah(plan);
+      if(res == RES_OK) res = plan_launch(plan, rng, n0, n - n0, nullptr, nullptr, mf, true);
+    } else {
+      res = plan_launch(plan, rng, 0, n, nullptr, nullptr, mf);
+    }
     if(res == RES_OK)
       res = ssol_b200_plan_finish(plan, rng, n, max_failed, nullptr, out);
     ssol_b200_plan_ref_put(plan);

@@ -177,3 +177,22 @@ def test_work_counters_are_optional(product):
     _same(off.globals(), on.globals(), "globals")
     _same(off.receiver(h["receiver"]), on.receiver(h["receiver"]), "receiver")
     s.close()
+
+
+def test_large_default_solve_switches_trees(product):
+    """A default ssol_solve above 2^24 realisations traces its first 2^24 on
+    the device-built tree and the rest on the host SAH tree built meanwhile:
+    the same estimates as a solve on either tree alone, and the stats name
+    the tree it ended on."""
+    s, h = W.heliostat_field(product, n_helio=300, receiver_cells=16)
+    n = (1 << 24) + 3_000_000
+    both = s.solve(n, seed=21)
+    sah = s.solve(n, seed=21, options=P.options(bvh=P.BVH_SAH))
+    lbvh = s.solve(n, seed=21, options=P.options(bvh=P.BVH_LBVH))
+    sb = both.stats()
+    assert sb["bvh_device"] == 0 and sb["paths"] == n and sb["kernel_ms"] > 0
+    assert both.count("realisation_count") == n
+    for other in (sah, lbvh):
+        _same(both.globals(), other.globals(), "globals")
+        _same(both.receiver(h["receiver"]), other.receiver(h["receiver"]), "receiver")
+    s.close()
