@@ -39,9 +39,11 @@ enum ssol_b200_precision {
  *    levels) is rebuilt on the host with the SAH builder, with a warning;
  *  - SSOL_B200_BVH_AUTO (the default): ssol_solve and ssol_solve_ex use the
  *    device builder for solves of at most SSOL_B200_BVH_AUTO_MAX_PATHS
- *    realisations, where building is a large part of the call, and the SAH
- *    builder above; plans, which do not know how many realisations they will
- *    trace, use the SAH builder.
+ *    realisations, where building is a large part of the call. Larger solves
+ *    start on the device's tree and, after their first 6e6 realisations,
+ *    trace on the SAH tree that the host threads built meanwhile. Plans,
+ *    which do not know how many realisations they will trace, use the SAH
+ *    builder.
  * Both trees find the same closest hits; only the time to build them and to
  * traverse them differs. Batches and the renderers always use the SAH
  * builder. */
