@@ -101,3 +101,29 @@ def test_c_caller_on_b200(tmp_path, product, oracle):
         tol = 4 * (se_c ** 2 + se_o ** 2) ** 0.5 + 1e-5 * abs(e_o)
         assert abs(e_c - e_o) <= tol, (k, e_c, e_o, tol)
     assert c_out["incoming_flux"][0] > 0
+
+
+def test_struct_layouts_match_the_binding(tmp_path):
+    """The ctypes mirrors of ssol_b200_options and ssol_b200_stats have the C
+    structs' sizes and field offsets, and the binding's defaults and builder
+    values are the header's (no GPU: nothing is called)."""
+    import ctypes as C
+    exe = str(tmp_path / "struct_sizes")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-I",
+                    os.path.join(ROOT, "include"), "-o", exe,
+                    os.path.join(ROOT, "tests", "c_caller", "struct_sizes.c")],
+                   check=True, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    c = {k: int(v) for k, v in (line.split() for line in out.splitlines())}
+    o, st = P.B200Options, P.B200Stats
+    assert c["options.size"] == C.sizeof(o)
+    assert c["options.bvh_builder"] == o.bvh_builder.offset
+    assert c["options.count_work"] == o.count_work.offset
+    assert c["stats.size"] == C.sizeof(st)
+    assert c["stats.bvh_device"] == st.bvh_device.offset
+    d = P.options()
+    assert (c["default.precision"], c["default.block_size"], c["default.waves"],
+            c["default.bvh_builder"], c["default.count_work"]) == \
+        (d.precision, d.block_size, d.waves, d.bvh_builder, d.count_work)
+    assert (c["builder.auto"], c["builder.sah"], c["builder.lbvh"]) == \
+        (P.BVH_AUTO, P.BVH_SAH, P.BVH_LBVH)
